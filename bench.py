@@ -1,0 +1,427 @@
+#!/usr/bin/env python3
+"""Benchmark of the pimdal_b200 operators on one node (one process per GPU).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload sort_smj|select|...]
+
+Prints ONE JSON line (rank 0).  A "step" is one pass of the workload's
+operators over one batch of synthetic input already resident in HBM.  Every
+rank runs the same workload on its own GPU (independent replicas: the
+operators shard by rows with no data-path exchange), so `value` is the sum
+of the ranks' rows over the max over ranks of the device time.
+
+  value  = input rows / s over the timed steps (CUDA events per step on the
+           launching stream; L2 flushed between steps by writing 256 MiB)
+  e2e    = the same metric through the public API with host buffers: pinned
+           host inputs copied in and outputs copied back inside the region
+  roofline   = the dominant kernel's algorithmic bytes per launch / its mean
+               launch duration (CUDA events recorded by the library on the
+               launching stream), against MEASURED_PEAKS.json hbm_gbs
+  cpu_baseline = the reference's own CPU operators (oracle/_ref, all host
+               threads) on a bounded sample of the same workload, rank 0
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+L2_FLUSH_BYTES = 256 << 20
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+def hbm_peak() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks / throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def __enter__(self):
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        self.file.flush()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            for line in Path(self.file.name).read_text().splitlines():
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                    rows.append(f)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.unlink(self.file.name)
+            except Exception:
+                pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]),
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())
+                if any(r[3].replace(".", "").isdigit() for r in rows) else None}
+
+
+# ---------------------------------------------------------------------------
+# workloads
+# ---------------------------------------------------------------------------
+class Workload:
+    name = ""
+    config = {}
+    rows_per_step = 0
+    dominant = None            # kernel id for the roofline
+    dominant_name = ""
+    traffic_per_launch = None  # bytes, from the committed ncu summary
+
+    def setup(self, ctx, dev):  # device-resident inputs + pinned host copies
+        raise NotImplementedError
+
+    def step(self):             # inputs resident in HBM
+        raise NotImplementedError
+
+    def step_e2e(self, stream):  # host inputs -> device -> host outputs
+        raise NotImplementedError
+
+    def algorithmic_bytes_per_launch(self) -> float:
+        raise NotImplementedError
+
+    def cpu_sample(self, ref, threads, budget_s):  # -> (rows, seconds, description)
+        raise NotImplementedError
+
+
+class SelectWorkload(Workload):
+    """Selection over 2^24 int32 values U[0, 2^31), predicate v < 214748364."""
+    name = "select"
+    N = 1 << 24
+
+    def __init__(self):
+        from pimdal_b200 import _lib as L
+        from pimdal_b200 import gen
+        self.spec = gen.Spec(L.GEN_UNIFORM, L.I32, seed=0xB200, lo=0, hi=2**31 - 1)
+        self.config = {"workload": "selection 2^24 int32 U[0,2^31), v < 214748364 (~10%)",
+                       "rows": self.N, "l2": "flushed between steps (input 64 MiB < L2)"}
+        self.rows_per_step = self.N
+        self.dominant = L.KERNEL_SELECT
+        self.dominant_name = "k_select"
+
+    def setup(self, ctx, dev):
+        import torch
+        from pimdal_b200 import _lib as L
+        from pimdal_b200 import gen, ops
+        self.ctx, self.ops, self.L = ctx, ops, L
+        self.spec = gen.Spec(L.GEN_UNIFORM, L.I32, seed=0xB200, lo=0, hi=2**31 - 1)
+        self.keys = ops.gen_column(ctx, self.spec, self.N)
+        self.pred = ops.make_pred(L.PRED_LT, 214748364)
+        self.out = torch.empty_like(self.keys)
+        self.out_ptr = torch.empty_like(self.keys)
+        self.res = torch.empty(1, dtype=torch.int64, device=dev)
+        self.h_keys = torch.from_numpy(gen.generate_cpu(self.spec, self.N)).pin_memory()
+        self.h_out = torch.empty(self.N, dtype=torch.int32).pin_memory()
+        self.h_ptr = torch.empty(self.N, dtype=torch.int32).pin_memory()
+        self.h_cnt = torch.empty(1, dtype=torch.int64).pin_memory()
+        self.d_in2 = torch.empty_like(self.keys)
+        ops.sel_kernel(ctx, self.keys, self.pred, out=self.out, out_ptr=self.out_ptr, result=self.res)
+        ctx.sync()
+        self.count = int(self.res.item())
+
+    def step(self):
+        self.ops.sel_kernel(self.ctx, self.keys, self.pred, out=self.out, out_ptr=self.out_ptr,
+                            result=self.res)
+
+    def step_e2e(self, stream):
+        self.d_in2.copy_(self.h_keys, non_blocking=True)
+        self.ops.sel_kernel(self.ctx, self.d_in2, self.pred, out=self.out, out_ptr=self.out_ptr,
+                            result=self.res)
+        self.h_cnt.copy_(self.res, non_blocking=True)
+        k = self.count  # output size is known from setup (same input every step)
+        self.h_out[:k].copy_(self.out[:k], non_blocking=True)
+        self.h_ptr[:k].copy_(self.out_ptr[:k], non_blocking=True)
+        return 4 * self.N, 8 + 8 * k
+
+    def algorithmic_bytes_per_launch(self):
+        return 4 * self.N + 8 * self.count
+
+    def cpu_sample(self, ref, threads, budget_s):
+        from pimdal_b200 import gen
+        n = self.N
+        if not hasattr(self, "_cpu_keys"):
+            self._cpu_keys = gen.generate_cpu(self.spec, n)
+            ref.set_threads("select", threads)
+            ref.select(self._cpu_keys, -2**63, 214748364 - 1)
+        reps = 0
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < budget_s or reps < 1:
+            ref.select(self._cpu_keys, -2**63, 214748364 - 1)
+            reps += 1
+        dt = time.perf_counter() - t0
+        return n * reps, dt, f"reference select() body (select.cpp:77-100) on the full 2^24 column x{reps}"
+
+
+WORKLOADS = {"select": SelectWorkload}
+DEFAULT_WORKLOAD = "select"
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device(f"cuda:{local}"))
+    return world, rank, local
+
+
+def reduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def run_ours(args) -> None:
+    import torch
+    from pimdal_b200 import ops
+
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dev = f"cuda:{local}"
+    ctx = ops.Context(local)
+    wl = WORKLOADS[args.workload]()
+    wl.setup(ctx, dev)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+
+    for _ in range(args.warmup):
+        flush.fill_(1)
+        wl.step()
+    ctx.sync()
+
+    # ---- device-resident timing ----
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ctx.kernel_time(wl.dominant)  # reset
+    barrier(world)
+    torch.cuda.synchronize()
+    launches0 = ctx.launches
+    with ClockSampler(local) as clk:
+        ctx.set_profiling(True)
+        for i in range(args.steps):
+            flush.fill_(i)
+            starts[i].record(stream)
+            wl.step()
+            stops[i].record(stream)
+        torch.cuda.synchronize()
+        ctx.set_profiling(False)
+    barrier(world)
+    launches = ctx.launches - launches0
+    ctx.sync()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, stops)]
+    total_ms = reduce_max(sum(step_ms), world)
+    k_launches, k_ms = ctx.kernel_time(wl.dominant)
+    clocks = clk.summary()
+
+    # ---- end-to-end timing (public API, host buffers) ----
+    for _ in range(max(1, args.warmup // 2)):
+        wl.step_e2e(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    h2d = d2h = 0
+    for _ in range(args.steps):
+        h2d, d2h = wl.step_e2e(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    e2e_ms = reduce_max(e0.elapsed_time(e1), world)
+    ctx.sync()
+
+    rows_total = reduce_sum(float(wl.rows_per_step * args.steps), world)
+    value = rows_total / (total_ms / 1e3)
+    e2e_value = rows_total / (e2e_ms / 1e3)
+
+    peak, peak_kind = hbm_peak()
+    roof = None
+    if k_launches:
+        avg_s = k_ms / k_launches / 1e3
+        ach = wl.algorithmic_bytes_per_launch() / avg_s / 1e9
+        roof = {"bound": "hbm", "kernel": wl.dominant_name, "achieved": round(ach, 1),
+                "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
+                "peak_source": peak_kind,
+                "traffic": wl.traffic_per_launch,
+                "algorithmic_bytes_per_launch": wl.algorithmic_bytes_per_launch(),
+                "mean_launch_ms": round(k_ms / k_launches, 5), "launches": k_launches}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(wl)
+
+    if rank == 0:
+        line = {
+            "metric": "rows/s", "value": round(value, 1), "unit": "rows/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(total_ms / args.steps, 5), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int32/uint32 keys, int64 sums",
+            "data": "synthetic (seeded counter-based generator)",
+            "config": dict(wl.config, parallelism=f"replicas x{world}"),
+            "e2e": {"value": round(e2e_value, 1), "unit": "rows/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": round(e2e_ms / args.steps, 4)},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+            "gpu_launches": launches, "impl": "ours",
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_baseline(wl) -> dict | None:
+    import oracle
+    if not oracle.Ref.available("select"):
+        return {"value": None, "unavailable": "oracle/_ref not built"}
+    threads = host_threads()
+    rows, secs, desc = wl.cpu_sample(oracle.Ref(), threads, 15.0)
+    return {"value": round(rows / secs, 1), "unit": "rows/s", "cores": threads,
+            "kind": "reference", "sample": desc}
+
+
+def run_reference(args) -> None:
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    wl = WORKLOADS[args.workload]()
+    if not oracle.Ref.available("select"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref (the reference's CPU "
+                          "operators) was not built on this machine"}))
+        return
+    threads = host_threads()
+    ref = oracle.Ref()
+    budget = max(0.5, min(5.0, 150.0 / (args.steps + args.warmup)))
+    for _ in range(args.warmup):
+        wl.cpu_sample(ref, threads, 0.0)
+    rows = secs = 0.0
+    desc = ""
+    for _ in range(args.steps):
+        r, s, desc = wl.cpu_sample(ref, threads, budget)
+        rows += r
+        secs += s
+    value = rows / secs
+    print(json.dumps({
+        "metric": "rows/s", "value": round(value, 1), "unit": "rows/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(secs / args.steps * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "int32/uint32 keys, int64 sums", "data": "synthetic (seeded counter-based generator)",
+        "config": dict(wl.config, parallelism="host CPU"), "impl": "reference",
+        "cpu_baseline": {"value": round(value, 1), "unit": "rows/s", "cores": threads,
+                         "kind": "reference", "sample": desc},
+        "e2e": {"value": round(value, 1), "unit": "rows/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,203 @@
+/*
+ * pimdal_gpu.h -- C ABI of the B200 (sm_100a) implementation of PIMDAL's
+ * data-parallel operator layer: selection, stable radix sort, sort-merge join,
+ * radix-partitioned / L2-resident hash join, and hash / sort group-by.
+ *
+ * Every entry point mirrors one DPU library call of the reference.  The
+ * argument structs keep the reference's field meaning; what changes is:
+ *   - 32-bit MRAM addresses become 64-bit device pointers (columns resident
+ *     in HBM, caller-owned);
+ *   - function-pointer predicates / combiners become small descriptors;
+ *   - every call takes a context (workspace + device error word) and a
+ *     CUDA stream, and returns a status code instead of `return 0`;
+ *   - counts are uint64 and are written to DEVICE memory (results structs),
+ *     so calls never block the host.
+ *
+ * Threading: all work is stream-ordered.  A context may be used from one
+ * stream at a time (its workspace and lookback status words are shared by
+ * consecutive calls); use one context per concurrently-running stream.
+ *
+ * Device-side failures (a bounded spin that gave up, a hash table that ran
+ * out of slots, an output buffer that was too small) never trap: kernels set
+ * bits in the context's device error word; pimdal_ctx_sync_status() waits for
+ * the stream and turns the word into a status code.
+ */
+#ifndef PIMDAL_GPU_H_
+#define PIMDAL_GPU_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PIMDAL_ABI_VERSION 1
+
+/* ------------------------------------------------------------------------- */
+/* Status codes (replace the reference's unconditional `return 0` and the     */
+/* host-side DPU_ASSERT / dpu::DpuError).                                     */
+/* ------------------------------------------------------------------------- */
+typedef enum {
+  PIMDAL_OK = 0,
+  PIMDAL_ERR_ARG = 1,            /* bad argument (null pointer, size, enum)   */
+  PIMDAL_ERR_OOM = 2,            /* device allocation failed                 */
+  PIMDAL_ERR_WORKSPACE = 3,      /* caller-provided workspace too small      */
+  PIMDAL_ERR_TABLE_FULL = 4,     /* hash table has no free slot              */
+  PIMDAL_ERR_DEVICE_TIMEOUT = 5, /* a bounded device-side wait gave up       */
+  PIMDAL_ERR_CUDA = 6,           /* a CUDA runtime call or launch failed     */
+  PIMDAL_ERR_CAPACITY = 7,       /* output buffer smaller than the result    */
+  PIMDAL_ERR_BUDGET = 8,         /* admission rejected by the HBM byte budget*/
+  PIMDAL_ERR_NOT_SUPPORTED = 9
+} pimdal_status_t;
+
+typedef void *pimdal_stream_t; /* a cudaStream_t; NULL = legacy default stream */
+
+/* The reference's pair type: key_ptr32 {uint32 key; uint32 ptr;}
+ * (pimdal/main/select/shared/datatype.h:8-12, key_ptr_t alias at :35). */
+typedef struct {
+  uint32_t key;
+  uint32_t ptr;
+} pimdal_key_ptr32_t;
+
+/* Column element types accepted at the boundary. */
+typedef enum { PIMDAL_U32 = 0, PIMDAL_I32 = 1, PIMDAL_I64 = 2 } pimdal_dtype_t;
+
+/* Input/output layout: structure-of-arrays columns (key column + row-id
+ * column) or the reference's array of key_ptr32 pairs. */
+typedef enum { PIMDAL_LAYOUT_COLUMNS = 0, PIMDAL_LAYOUT_PAIRS = 1 } pimdal_layout_t;
+
+/* ------------------------------------------------------------------------- */
+/* Context                                                                    */
+/* ------------------------------------------------------------------------- */
+typedef struct pimdal_ctx pimdal_ctx_t;
+
+/* Creates a context on `device`.  Allocates only the device error word and
+ * the lookback status words (a few MB), zeroed. */
+int pimdal_ctx_create(pimdal_ctx_t **ctx, int device);
+int pimdal_ctx_destroy(pimdal_ctx_t *ctx);
+
+/* Hands the context a caller-owned scratch buffer (device memory, 256-byte
+ * aligned).  Without one, the context grows its own buffer with cudaMalloc
+ * when a call needs more (never during stream capture).  Each operator's
+ * *_workspace_size() query gives the bytes it needs. */
+int pimdal_ctx_set_workspace(pimdal_ctx_t *ctx, void *ptr, size_t bytes);
+
+/* Waits for `stream`, reads and clears the device error word, and returns the
+ * first error code it holds (PIMDAL_OK when none). */
+int pimdal_ctx_sync_status(pimdal_ctx_t *ctx, pimdal_stream_t stream);
+
+/* Number of kernels this context launched so far (for accounting). */
+uint64_t pimdal_ctx_launch_count(const pimdal_ctx_t *ctx);
+
+/* Per-kernel device timing.  While enabled, every launch of the library's
+ * kernels is bracketed by CUDA events recorded on the launching stream;
+ * pimdal_ctx_kernel_time() waits for them and returns, for one kernel id,
+ * the number of launches and their summed duration since the last read. */
+typedef enum {
+  PIMDAL_KERNEL_SELECT = 0,
+  PIMDAL_KERNEL_GEN = 1,
+  PIMDAL_KERNEL_SORT_HIST = 2,   /* radix sort: all-digit histogram pass   */
+  PIMDAL_KERNEL_SORT_PASS = 3,   /* radix sort: one onesweep digit pass    */
+  PIMDAL_KERNEL_SMJ_MERGE = 4,   /* merge-path join                        */
+  PIMDAL_KERNEL_PARTITION = 5,   /* hash radix partition                   */
+  PIMDAL_KERNEL_HJ_BUILD = 6,
+  PIMDAL_KERNEL_HJ_PROBE = 7,
+  PIMDAL_KERNEL_GROUP = 8,       /* hash group-by                          */
+  PIMDAL_KERNEL_SEGREDUCE = 9,   /* sort group-by segmented reduction      */
+  PIMDAL_KERNEL_OTHER = 10,
+  PIMDAL_KERNEL_COUNT = 11
+} pimdal_kernel_id_t;
+int pimdal_ctx_set_profiling(pimdal_ctx_t *ctx, int enable);
+int pimdal_ctx_kernel_time(pimdal_ctx_t *ctx, int kernel_id, uint64_t *launches,
+                           double *total_ms);
+
+const char *pimdal_status_string(int status);
+int pimdal_abi_version(void);
+
+/* ------------------------------------------------------------------------- */
+/* Seeded counter-based column generator (replaces the thread-count-dependent */
+/* std::default_random_engine generators of reference/db_operators/          */
+/* shared.cpp:10-60).  Value i depends only on (seed, stream_id, i), so CPU   */
+/* and GPU produce identical columns for any launch shape.                    */
+/* ------------------------------------------------------------------------- */
+typedef enum {
+  PIMDAL_GEN_UNIFORM = 0,      /* lo + floor(u * (hi-lo+1)), inclusive range    */
+  PIMDAL_GEN_PERM = 1,         /* perm_domain(row)  (distinct values)           */
+  PIMDAL_GEN_PERM_UNIFORM = 2, /* perm_domain(uniform index in [lo, hi])        */
+  PIMDAL_GEN_PERM_ZIPF = 3,    /* perm_domain(zipf index over cdf[0..cdf_n))    */
+  PIMDAL_GEN_PROBE = 4         /* join probe: Bernoulli(match_permille/1000)
+                                  picks perm_domain(idx) with idx < lo (a build
+                                  key) or perm_domain(lo + idx) (a non-key);
+                                  idx uniform over [0, lo) or zipf via cdf     */
+} pimdal_gen_kind_t;
+
+typedef struct {
+  int32_t kind;          /* pimdal_gen_kind_t */
+  int32_t out_dtype;     /* PIMDAL_U32 / PIMDAL_I32 (4 bytes) or PIMDAL_I64 */
+  uint64_t seed;
+  uint64_t stream_id;    /* independent sub-stream per column */
+  int64_t lo, hi;        /* uniform range (inclusive) / PROBE: build count */
+  uint64_t perm_domain;  /* permutation domain size (0 = 2^32) */
+  const double *cdf;     /* device pointer: zipf CDF (ascending), or NULL */
+  uint64_t cdf_n;
+  uint32_t match_permille; /* PROBE only */
+  uint32_t pad;
+} pimdal_gen_spec_t;
+
+/* dst[i] = value(row_offset + i) for i < n. */
+int pimdal_gen_column(pimdal_ctx_t *ctx, const pimdal_gen_spec_t *spec, void *dst,
+                      uint64_t n, uint64_t row_offset, pimdal_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
+/* Selection.  Replaces sel_kernel(sel_arguments_t*, sel_results_t*)          */
+/* (pimdal/select/sel.h:7-21, sel.c:81-150) together with the create_ptr /   */
+/* out_val glue of pimdal/main/select/dpu/kernel_select.c:31-42, and the CPU  */
+/* sel_cnt_kernel / sel_out_kernel of reference/db_operators/select.cpp:39-75.*/
+/* Output is stable: selected rows appear in ascending input order.           */
+/* ------------------------------------------------------------------------- */
+typedef enum {
+  PIMDAL_PRED_LT = 0,      /* v <  lo            */
+  PIMDAL_PRED_LE = 1,      /* v <= lo            */
+  PIMDAL_PRED_GT = 2,      /* v >  lo            */
+  PIMDAL_PRED_GE = 3,      /* v >= lo            */
+  PIMDAL_PRED_EQ = 4,      /* v == lo            */
+  PIMDAL_PRED_NE = 5,      /* v != lo            */
+  PIMDAL_PRED_BETWEEN = 6, /* lo <= v && v <= hi */
+  PIMDAL_PRED_RANGE = 7    /* lo <= v && v <  hi */
+} pimdal_pred_op_t;
+
+/* Replaces `bool (*pred)(const key_ptr_t)` (sel.h:11). */
+typedef struct {
+  int32_t op;    /* pimdal_pred_op_t */
+  int32_t pad;
+  int64_t lo;
+  int64_t hi;
+} pimdal_pred_t;
+
+typedef struct {
+  uint64_t size;          /* sel_arguments_t.size: number of elements          */
+  const void *in;         /* sel_arguments_t.in: key column (key_dtype) or pairs */
+  const uint32_t *in_ptr; /* row-id column; NULL = ptr_base + index (create_ptr) */
+  uint64_t ptr_base;
+  void *out;              /* sel_arguments_t.out: selected keys (or pairs)      */
+  uint32_t *out_ptr;      /* selected row ids (COLUMNS layout); may be NULL     */
+  pimdal_pred_t pred;     /* sel_arguments_t.pred                               */
+  int32_t key_dtype;      /* PIMDAL_I32 or PIMDAL_U32                            */
+  int32_t layout;         /* pimdal_layout_t                                    */
+} pimdal_sel_arguments_t;
+
+typedef struct {
+  uint64_t t_count; /* sel_results_t.t_count (sel.h:14-16) */
+} pimdal_sel_results_t;
+
+int pimdal_sel_workspace_size(const pimdal_sel_arguments_t *args, size_t *bytes);
+/* `d_result` is device memory. */
+int pimdal_sel_kernel(pimdal_ctx_t *ctx, const pimdal_sel_arguments_t *args,
+                      pimdal_sel_results_t *d_result, pimdal_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PIMDAL_GPU_H_ */

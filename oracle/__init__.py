@@ -1,0 +1,253 @@
+"""CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
+arm may import this package, and only as the checker or the timed CPU
+baseline.  The product (pimdal_b200) never imports it.
+
+Two layers:
+  * liboracle.so -- plain-C restatement of the reference algorithms
+    (oracle.c, built by `make -C oracle`);
+  * _ref/libref_*.so -- the reference's own CPU operators from
+    reference/db_operators, compiled where they lie through oracle/ref/*.cpp
+    (`make -C oracle ref`, needs the reference checkout at build time only).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF_DIR = HERE / "_ref"
+
+_P = C.c_void_p
+_U64 = C.c_uint64
+
+
+def build(ref: bool = False) -> None:
+    """Builds liboracle.so (and, with ref=True, the reference harnesses)."""
+    targets = ["oracle"] + (["ref"] if ref else [])
+    subprocess.run(["make", "-s", "-C", str(HERE), *targets], check=True)
+
+
+def _p(a: np.ndarray | None) -> int | None:
+    return None if a is None else a.ctypes.data
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        path = HERE / "liboracle.so"
+        if not path.exists():
+            build()
+        l = C.CDLL(str(path), mode=os.RTLD_LOCAL)
+        l.oracle_select.restype = _U64
+        l.oracle_select.argtypes = [_P, _U64, C.c_int, C.c_int64, C.c_int64, C.c_int, _P, _U64, _P, _P]
+        l.oracle_sort_pairs.restype = None
+        l.oracle_sort_pairs.argtypes = [_P, _P, _U64, C.c_int, _P, _P]
+        l.oracle_smj_merge.restype = _U64
+        l.oracle_smj_merge.argtypes = [_P, _P, _U64, _P, _P, _U64, C.c_int, _P, _P, _U64]
+        l.oracle_hash_join.restype = _U64
+        l.oracle_hash_join.argtypes = [_P, _P, _U64, _P, _P, _U64, C.c_uint32, _P, _P, _U64]
+        l.oracle_part_hash0.restype = None
+        l.oracle_part_hash0.argtypes = [_P, _P, _U64, C.c_uint32, C.c_uint32, _P, _P, _P]
+        for f in (l.oracle_group_by, l.oracle_sort_group_by):
+            f.restype = _U64
+            f.argtypes = [_P, _P, _U64, _P, _P, _P, _P, _P]
+        _lib = l
+    return _lib
+
+
+def _u32(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a).view(np.uint32) if np.asarray(a).dtype.itemsize == 4
+                                else np.asarray(a, dtype=np.uint32))
+
+
+# ----------------------------------------------------------------- select
+def select(keys: np.ndarray, lo: int, hi: int, invert: bool = False, is_signed: bool = True,
+           in_ptr: np.ndarray | None = None, ptr_base: int = 0):
+    """Returns (values, row ids) of the selected rows, ascending by row."""
+    k = _u32(keys)
+    n = k.size
+    out_k = np.empty(max(n, 1), np.uint32)
+    out_p = np.empty(max(n, 1), np.uint32)
+    ip = None if in_ptr is None else _u32(in_ptr)
+    c = lib().oracle_select(_p(k), n, int(is_signed), lo, hi, int(invert), _p(ip), ptr_base,
+                            _p(out_k), _p(out_p))
+    dt = np.int32 if is_signed else np.uint32
+    return out_k[:c].view(dt), out_p[:c]
+
+
+def sort_pairs(keys: np.ndarray, ptr: np.ndarray | None = None, is_signed: bool = False):
+    k = _u32(keys)
+    n = k.size
+    ok = np.empty(max(n, 1), np.uint32)
+    op = np.empty(max(n, 1), np.uint32)
+    pp = None if ptr is None else _u32(ptr)
+    lib().oracle_sort_pairs(_p(k), _p(pp), n, int(is_signed), _p(ok), _p(op))
+    return ok[:n], op[:n]
+
+
+def smj_merge(ikey, iptr, okey, optr, is_signed: bool = True):
+    ik, ip, ok, op = map(_u32, (ikey, iptr, okey, optr))
+    cnt = lib().oracle_smj_merge(_p(ik), _p(ip), ik.size, _p(ok), _p(op), ok.size, int(is_signed),
+                                 None, None, 0)
+    oo = np.empty(max(cnt, 1), np.uint32)
+    oi = np.empty(max(cnt, 1), np.uint32)
+    lib().oracle_smj_merge(_p(ik), _p(ip), ik.size, _p(ok), _p(op), ok.size, int(is_signed),
+                           _p(oo), _p(oi), cnt)
+    return oo[:cnt], oi[:cnt]
+
+
+def sort_merge_join(rkey, rpay, skey, spay, is_signed: bool = True):
+    """Sorts R and S stably by key and merges; returns (R payload, S payload)
+    per match, S-major (outer = S, inner = R)."""
+    rk, rp = sort_pairs(rkey, rpay, is_signed)
+    sk, sp = sort_pairs(skey, spay, is_signed)
+    s_pay, r_pay = smj_merge(rk, rp, sk, sp, is_signed)
+    return r_pay, s_pay
+
+
+def hash_join(bkey, bpay, pkey, prow=None, part_n: int = 16384):
+    bk, bp, pk = map(_u32, (bkey, bpay, pkey))
+    pr = None if prow is None else _u32(prow)
+    cnt = lib().oracle_hash_join(_p(bk), _p(bp), bk.size, _p(pk), _p(pr), pk.size, part_n,
+                                 None, None, 0)
+    op = np.empty(max(cnt, 1), np.uint32)
+    orow = np.empty(max(cnt, 1), np.uint32)
+    lib().oracle_hash_join(_p(bk), _p(bp), bk.size, _p(pk), _p(pr), pk.size, part_n,
+                           _p(op), _p(orow), cnt)
+    return op[:cnt], orow[:cnt]
+
+
+def part_hash0(keys, ptr=None, shift: int = 32, part_n: int = 32):
+    k = _u32(keys)
+    n = k.size
+    ok = np.empty(max(n, 1), np.uint32)
+    op = np.empty(max(n, 1), np.uint32)
+    sizes = np.empty(part_n + 1, np.uint64)
+    pp = None if ptr is None else _u32(ptr)
+    lib().oracle_part_hash0(_p(k), _p(pp), n, shift, part_n, _p(ok), _p(op), _p(sizes))
+    return ok[:n], op[:n], sizes
+
+
+def _group(fn, keys, vals):
+    k = np.ascontiguousarray(keys, dtype=np.int32)
+    v = None if vals is None else np.ascontiguousarray(vals, dtype=np.int64)
+    n = k.size
+    outs = [np.empty(max(n, 1), np.int32)] + [np.empty(max(n, 1), np.int64) for _ in range(4)]
+    g = fn(_p(k), _p(v), n, *map(_p, outs))
+    return tuple(o[:g] for o in outs)
+
+
+def group_by(keys, vals=None):
+    """(key, SUM, COUNT, MIN, MAX) per group, ascending by key."""
+    return _group(lib().oracle_group_by, keys, vals)
+
+
+def sort_group_by(keys, vals=None):
+    return _group(lib().oracle_sort_group_by, keys, vals)
+
+
+# ------------------------------------------------------------ reference libs
+class Ref:
+    """The reference's own CPU operators (oracle/_ref/libref_*.so)."""
+
+    def __init__(self):
+        self._libs: dict[str, C.CDLL] = {}
+
+    @staticmethod
+    def available(name: str = "select") -> bool:
+        return (REF_DIR / f"libref_{name}.so").exists()
+
+    def _get(self, name: str) -> C.CDLL:
+        if name not in self._libs:
+            path = REF_DIR / f"libref_{name}.so"
+            if not path.exists():
+                raise FileNotFoundError(f"{path} not built (make -C oracle ref)")
+            self._libs[name] = C.CDLL(str(path), mode=os.RTLD_LOCAL)
+        return self._libs[name]
+
+    def set_threads(self, name: str, t: int) -> None:
+        f = self._get(name).pimdal_ref_set_threads
+        f.argtypes = [C.c_int]
+        f(t)
+
+    def sel_count(self, keys: np.ndarray, lo: int, hi: int) -> int:
+        f = self._get("select").pimdal_ref_sel_count
+        f.restype = _U64
+        f.argtypes = [_P, _U64, C.c_int64, C.c_int64]
+        k = np.ascontiguousarray(keys, dtype=np.int32)
+        return int(f(_p(k), k.size, lo, hi))
+
+    def select(self, keys: np.ndarray, lo: int, hi: int) -> np.ndarray:
+        f = self._get("select").pimdal_ref_select
+        f.restype = _U64
+        f.argtypes = [_P, _U64, C.c_int64, C.c_int64, _P]
+        k = np.ascontiguousarray(keys, dtype=np.int32)
+        out = np.empty(k.size + 1, np.int32)
+        c = int(f(_p(k), k.size, lo, hi, _p(out)))
+        return out[:c]
+
+    def sort_pairs(self, keys, ptr=None, is_signed: bool = False):
+        f = self._get("sort").pimdal_ref_sort_pairs
+        f.restype = None
+        f.argtypes = [_P, _P, _U64, C.c_int, _P, _P]
+        k = _u32(keys)
+        pp = None if ptr is None else _u32(ptr)
+        ok = np.empty(max(k.size, 1), np.uint32)
+        op = np.empty(max(k.size, 1), np.uint32)
+        f(_p(k), _p(pp), k.size, int(is_signed), _p(ok), _p(op))
+        return ok[:k.size], op[:k.size]
+
+    def sort_keys(self, keys):
+        f = self._get("sort").pimdal_ref_sort_keys
+        f.restype = None
+        f.argtypes = [_P, _P, _U64]
+        k = _u32(keys)
+        out = np.empty(max(k.size, 1), np.uint32)
+        f(_p(k), _p(out), k.size)
+        return out[:k.size]
+
+    def hash_join(self, bkey, bpay, pkey, part_n: int = 16384):
+        f = self._get("hash_join").pimdal_ref_hash_join
+        f.restype = _U64
+        f.argtypes = [_P, _P, _U64, _P, _U64, C.c_uint32, _P, _P]
+        bk, bp, pk = map(_u32, (bkey, bpay, pkey))
+        op = np.empty(max(pk.size, 1), np.uint32)
+        orow = np.empty(max(pk.size, 1), np.uint32)
+        c = int(f(_p(bk), _p(bp), bk.size, _p(pk), pk.size, part_n, _p(op), _p(orow)))
+        return op[:c], orow[:c]
+
+    def group_by(self, keys, vals):
+        f = self._get("aggregate").pimdal_ref_group_by
+        f.restype = _U64
+        f.argtypes = [_P, _P, _U64, _P, _P, _P, _P, _P]
+        k = np.ascontiguousarray(keys, dtype=np.int32)
+        v = np.ascontiguousarray(vals, dtype=np.int64)
+        n = k.size
+        outs = [np.empty(max(n, 1), np.int32)] + [np.empty(max(n, 1), np.int64) for _ in range(4)]
+        g = int(f(_p(k), _p(v), n, *map(_p, outs)))
+        return tuple(o[:g] for o in outs)
+
+    def smj(self, inner_keys, outer_keys, buffer_size: int):
+        """Reference sort-merge join on key columns (one thread; the outer
+        size must equal the library's BUFFER_SIZE).  Returns (matched inner
+        keys, sorted outer keys)."""
+        lb = self._get(f"smj_{buffer_size}")
+        lb.pimdal_ref_set_threads.argtypes = [C.c_int]
+        lb.pimdal_ref_set_threads(1)
+        f = lb.pimdal_ref_smj
+        f.restype = None
+        f.argtypes = [_P, _U64, _P, _U64, _P, _P]
+        ik, ok = _u32(inner_keys), _u32(outer_keys)
+        ires = np.zeros(ok.size + 1, np.uint32)
+        ores = np.zeros(ok.size + 1, np.uint32)
+        f(_p(ik), ik.size, _p(ok), ok.size, _p(ires), _p(ores))
+        return ires[:ok.size], ores[:ok.size]

@@ -1,0 +1,100 @@
+"""ctypes binding of the C ABI in include/pimdal_gpu.h.
+
+The shared library is loaded from the package directory only (built in-tree by
+pimdal_b200/build.py).  There is no fallback: if the library is missing every
+operator raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libpimdal_b200.so"
+
+# ---- enums (mirror include/pimdal_gpu.h) ----------------------------------
+PIMDAL_OK = 0
+STATUS_NAMES = {
+    0: "PIMDAL_OK", 1: "PIMDAL_ERR_ARG", 2: "PIMDAL_ERR_OOM", 3: "PIMDAL_ERR_WORKSPACE",
+    4: "PIMDAL_ERR_TABLE_FULL", 5: "PIMDAL_ERR_DEVICE_TIMEOUT", 6: "PIMDAL_ERR_CUDA",
+    7: "PIMDAL_ERR_CAPACITY", 8: "PIMDAL_ERR_BUDGET", 9: "PIMDAL_ERR_NOT_SUPPORTED",
+}
+U32, I32, I64 = 0, 1, 2
+LAYOUT_COLUMNS, LAYOUT_PAIRS = 0, 1
+PRED_LT, PRED_LE, PRED_GT, PRED_GE, PRED_EQ, PRED_NE, PRED_BETWEEN, PRED_RANGE = range(8)
+GEN_UNIFORM, GEN_PERM, GEN_PERM_UNIFORM, GEN_PERM_ZIPF, GEN_PROBE = range(5)
+(KERNEL_SELECT, KERNEL_GEN, KERNEL_SORT_HIST, KERNEL_SORT_PASS, KERNEL_SMJ_MERGE, KERNEL_PARTITION,
+ KERNEL_HJ_BUILD, KERNEL_HJ_PROBE, KERNEL_GROUP, KERNEL_SEGREDUCE, KERNEL_OTHER) = range(11)
+
+
+class PimdalError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        super().__init__(f"{where}: {STATUS_NAMES.get(status, status)}")
+
+
+# ---- structs ----------------------------------------------------------------
+class GenSpec(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32), ("out_dtype", C.c_int32),
+        ("seed", C.c_uint64), ("stream_id", C.c_uint64),
+        ("lo", C.c_int64), ("hi", C.c_int64),
+        ("perm_domain", C.c_uint64),
+        ("cdf", C.c_void_p), ("cdf_n", C.c_uint64),
+        ("match_permille", C.c_uint32), ("pad", C.c_uint32),
+    ]
+
+
+class Pred(C.Structure):
+    _fields_ = [("op", C.c_int32), ("pad", C.c_int32), ("lo", C.c_int64), ("hi", C.c_int64)]
+
+
+class SelArguments(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint64), ("in_", C.c_void_p), ("in_ptr", C.c_void_p),
+        ("ptr_base", C.c_uint64), ("out", C.c_void_p), ("out_ptr", C.c_void_p),
+        ("pred", Pred), ("key_dtype", C.c_int32), ("layout", C.c_int32),
+    ]
+
+
+# Exported symbols and their ctypes signatures.
+_VP, _SZ, _U64, _I = C.c_void_p, C.c_size_t, C.c_uint64, C.c_int
+SIGNATURES = {
+    "pimdal_abi_version": (_I, []),
+    "pimdal_status_string": (C.c_char_p, [_I]),
+    "pimdal_ctx_create": (_I, [C.POINTER(_VP), _I]),
+    "pimdal_ctx_destroy": (_I, [_VP]),
+    "pimdal_ctx_set_workspace": (_I, [_VP, _VP, _SZ]),
+    "pimdal_ctx_sync_status": (_I, [_VP, _VP]),
+    "pimdal_ctx_launch_count": (_U64, [_VP]),
+    "pimdal_ctx_set_profiling": (_I, [_VP, _I]),
+    "pimdal_ctx_kernel_time": (_I, [_VP, _I, C.POINTER(_U64), C.POINTER(C.c_double)]),
+    "pimdal_gen_column": (_I, [_VP, C.POINTER(GenSpec), _VP, _U64, _U64, _VP]),
+    "pimdal_sel_workspace_size": (_I, [C.POINTER(SelArguments), C.POINTER(_SZ)]),
+    "pimdal_sel_kernel": (_I, [_VP, C.POINTER(SelArguments), _VP, _VP]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libpimdal_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m pimdal_b200.build` "
+                "(there is no CPU fallback)")
+        mode = getattr(os, "RTLD_LOCAL", 0)
+        l = C.CDLL(str(LIB_PATH), mode=mode)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(l, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = l
+    return _lib
+
+
+def check(status: int, where: str) -> None:
+    if status != PIMDAL_OK:
+        raise PimdalError(status, where)

@@ -1,0 +1,244 @@
+// Shared internals of the pimdal_b200 CUDA library (sm_100a).
+//
+//  * pimdal_ctx: workspace, device error word, lookback status words.
+//  * Decoupled look-back (single-pass prefix over tiles) with epoch-tagged
+//    64-bit status words and bounded waits that report a timeout instead of
+//    trapping.
+//  * The seeded counter-based generator (host + device), shared bit-for-bit
+//    with the numpy mirror in pimdal_b200/gen.py.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include <vector>
+
+#include "../../include/pimdal_gpu.h"
+
+#define PD_HD __host__ __device__ __forceinline__
+
+// ---------------------------------------------------------------------------
+// Device error word bits (OR-ed by kernels, read by pimdal_ctx_sync_status).
+// ---------------------------------------------------------------------------
+enum : uint32_t {
+  PD_DEVERR_TIMEOUT = 1u,     // a bounded spin gave up
+  PD_DEVERR_TABLE_FULL = 2u,  // hash table had no free slot
+  PD_DEVERR_CAPACITY = 4u,    // output buffer too small for the result
+  PD_DEVERR_ARG = 8u          // a device-side argument check failed
+};
+
+// Lookback status word: [epoch:16][flag:2][value:46].
+enum : uint32_t { PD_FLAG_INVALID = 0, PD_FLAG_AGGREGATE = 1, PD_FLAG_INCLUSIVE = 2 };
+constexpr uint64_t PD_STATUS_VALUE_MASK = (1ull << 46) - 1;
+constexpr uint32_t PD_STATUS_WORDS = 1u << 20;  // max tiles of one lookback launch
+constexpr uint32_t PD_SPIN_LIMIT = 1u << 22;    // bounded wait (~seconds with backoff)
+
+struct pd_prof_rec {
+  int kernel;
+  cudaEvent_t start, stop;
+};
+
+struct pimdal_ctx {
+  int device = 0;
+  int sm_count = 148;
+  // workspace
+  void *ws = nullptr;
+  size_t ws_bytes = 0;
+  bool ws_owned = false;
+  // device words
+  uint32_t *d_error = nullptr;   // error bits
+  uint64_t *d_status = nullptr;  // PD_STATUS_WORDS lookback status words
+  uint32_t epoch = 0;            // 16-bit epoch of the last lookback launch
+  uint64_t launches = 0;         // kernels launched through this context
+  // per-kernel timing (pimdal_ctx_set_profiling)
+  bool profiling = false;
+  std::vector<pd_prof_rec> prof_pending;
+  std::vector<cudaEvent_t> prof_free;
+  uint64_t prof_launches[PIMDAL_KERNEL_COUNT] = {};
+  double prof_ms[PIMDAL_KERNEL_COUNT] = {};
+};
+
+// Brackets one launch with timing events when profiling is on.
+struct pd_launch_scope {
+  pimdal_ctx *ctx;
+  int kernel;
+  cudaStream_t stream;
+  cudaEvent_t start = nullptr;
+  pd_launch_scope(pimdal_ctx *c, int k, cudaStream_t s);
+  ~pd_launch_scope();
+};
+
+// Returns a workspace of at least `bytes` (256-byte aligned) or nullptr with
+// *status set.  Grows an owned workspace; a caller-provided one is never grown.
+void *pd_workspace(pimdal_ctx *ctx, size_t bytes, cudaStream_t stream, int *status);
+
+// Next lookback epoch (1..65535); clears the status words when it wraps.
+uint32_t pd_next_epoch(pimdal_ctx *ctx, cudaStream_t stream, int *status);
+
+// Maps the outcome of a launch to a status code.
+int pd_launch_status(pimdal_ctx *ctx);
+
+static inline size_t pd_align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+static inline uint64_t pd_ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+
+#define PD_CHECK_CUDA(expr)                      \
+  do {                                           \
+    cudaError_t e__ = (expr);                    \
+    if (e__ != cudaSuccess) return PIMDAL_ERR_CUDA; \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void pd_store_release_u64(uint64_t *p, uint64_t v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t pd_load_acquire_u64(const uint64_t *p) {
+  uint64_t v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void pd_store_release_u32(uint32_t *p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t pd_load_acquire_u32(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ uint64_t pd_pack_status(uint32_t epoch, uint32_t flag, uint64_t v) {
+  return ((uint64_t)epoch << 48) | ((uint64_t)flag << 46) | (v & PD_STATUS_VALUE_MASK);
+}
+
+// Warp-cooperative decoupled look-back: returns the exclusive prefix of tile
+// `tile` (sum of the values of tiles < tile).  Must be called by all 32 lanes
+// of one warp.  Gives up after PD_SPIN_LIMIT polls, sets PD_DEVERR_TIMEOUT and
+// returns the partial sum (the result is then invalid but the kernel ends).
+__device__ __forceinline__ uint64_t pd_lookback_warp(const uint64_t *status, int64_t tile,
+                                                     uint32_t epoch, uint32_t *d_error) {
+  const int lane = threadIdx.x & 31;
+  uint64_t exclusive = 0;
+  int64_t base = tile - 1;
+  uint32_t spins = 0;
+  while (true) {
+    int64_t pred = base - lane;
+    uint32_t flag = PD_FLAG_INCLUSIVE;
+    uint64_t val = 0;
+    if (pred >= 0) {
+      uint64_t w = pd_load_acquire_u64(status + pred);
+      flag = ((uint32_t)(w >> 48) == epoch) ? (uint32_t)((w >> 46) & 3u) : PD_FLAG_INVALID;
+      val = w & PD_STATUS_VALUE_MASK;
+    }
+    unsigned incl = __ballot_sync(0xffffffffu, flag == PD_FLAG_INCLUSIVE);
+    unsigned invalid = __ballot_sync(0xffffffffu, flag == PD_FLAG_INVALID);
+    int first = incl ? (__ffs(incl) - 1) : 31;
+    unsigned need = (first >= 31) ? 0xffffffffu : ((2u << first) - 1u);
+    if (invalid & need) {
+      if (++spins > PD_SPIN_LIMIT) {
+        if (lane == 0) atomicOr(d_error, PD_DEVERR_TIMEOUT);
+        return exclusive;
+      }
+      __nanosleep(spins < 64 ? 20 : 200);
+      continue;
+    }
+    uint64_t contrib = (lane <= first) ? val : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) contrib += __shfl_xor_sync(0xffffffffu, contrib, o);
+    exclusive += contrib;
+    if (incl) break;
+    base -= 32;
+  }
+  return exclusive;
+}
+
+// ---------------------------------------------------------------------------
+// Seeded counter-based generator (host + device).
+//
+// The 64-bit finaliser is SplitMix64's output function (Steele, Lea and
+// Flood, "Fast splittable pseudorandom number generators", OOPSLA 2014).
+// ---------------------------------------------------------------------------
+constexpr uint64_t PD_GOLDEN64 = 0x9E3779B97F4A7C15ull;
+
+PD_HD uint64_t pd_mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+// Key of an independent sub-stream.
+PD_HD uint64_t pd_stream_key(uint64_t seed, uint64_t stream) {
+  return pd_mix64((seed * PD_GOLDEN64) ^ pd_mix64(stream + 0x632BE59BD9B4E019ull));
+}
+// i-th 64-bit draw of a sub-stream.
+PD_HD uint64_t pd_rand(uint64_t key, uint64_t i) { return pd_mix64(key + (i + 1) * PD_GOLDEN64); }
+// Second, independent draw for the same row.
+PD_HD uint64_t pd_rand2(uint64_t r) { return pd_mix64(r ^ 0xD1B54A32D192ED03ull); }
+
+// lo + floor(r_hi32 * span / 2^32), span = hi - lo + 1 <= 2^32.
+PD_HD int64_t pd_uniform(uint64_t r, int64_t lo, uint64_t span) {
+  return lo + (int64_t)(((r >> 32) * span) >> 32);
+}
+PD_HD double pd_unit(uint64_t r) { return (double)(r >> 11) * (1.0 / 9007199254740992.0); }
+
+// Bijective permutation of [0, n) (n = 0 means 2^32): four rounds of
+// multiply-by-odd / add / xorshift modulo 2^b, then cycle-walking into [0, n).
+struct pd_perm {
+  uint32_t bits;
+  uint64_t n, mask;
+  uint64_t mul[4], add[4];
+  uint32_t shift;
+};
+PD_HD pd_perm pd_make_perm(uint64_t seed, uint64_t n) {
+  pd_perm p;
+  p.n = n ? n : (1ull << 32);
+  uint32_t b = 0;
+  while ((1ull << b) < p.n) ++b;
+  p.bits = b;
+  p.mask = (b >= 64) ? ~0ull : ((1ull << b) - 1);
+  p.shift = (b + 1) / 2;
+  if (p.shift == 0) p.shift = 1;
+  uint64_t k = pd_stream_key(seed, 0xFFFF0000ull);
+  for (int r = 0; r < 4; ++r) {
+    uint64_t c = pd_rand(k, (uint64_t)r);
+    p.mul[r] = (c | 1ull) & p.mask;
+    p.add[r] = (c >> 32) & p.mask;
+  }
+  return p;
+}
+PD_HD uint64_t pd_perm_pow2(const pd_perm &p, uint64_t x) {
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    x = (x * p.mul[r] + p.add[r]) & p.mask;
+    x ^= x >> p.shift;
+  }
+  return x;
+}
+PD_HD uint64_t pd_perm_apply(const pd_perm &p, uint64_t x) {
+  if (p.bits == 0) return 0;
+  uint64_t y = pd_perm_pow2(p, x);
+  // Cycle-walking needs < 2 steps on average (n > 2^(b-1)); the bound only
+  // guarantees termination and is never reached in practice.
+  for (int walk = 0; y >= p.n && walk < 4096; ++walk) y = pd_perm_pow2(p, y);
+  return y < p.n ? y : y % p.n;
+}
+
+// ---------------------------------------------------------------------------
+// Hash functions.
+// ---------------------------------------------------------------------------
+// hash0 of the reference's partitioning step (pimdal/hash/hash_func.h:5-14):
+// the partition index of part_kernel is an interface-visible value (callers
+// route partition p to consumer p), so it is kept identical.
+PD_HD uint32_t pd_hash0(uint32_t key) {
+  key += 272333u;
+  key += ~(key << 5);
+  key ^= (key >> 18);
+  key += (key << 11);
+  key ^= (key >> 17);
+  return key;
+}
+// Table-slot hash of this library (multiplicative / Fibonacci hashing):
+// the top `bits` bits of key * 2^64/phi.
+PD_HD uint64_t pd_hash_slot(uint32_t key, uint32_t bits) {
+  return bits ? (((uint64_t)key * PD_GOLDEN64) >> (64 - bits)) : 0;
+}

@@ -1,0 +1,136 @@
+"""Python host layer over the C ABI (include/pimdal_gpu.h).
+
+Operator names and argument meaning follow the reference's DPU library
+(pimdal/select/sel.h, pimdal/sort/sort.h, pimdal/join/*.h,
+pimdal/aggregate/aggregate.h).  Columns are torch CUDA tensors resident in
+HBM; torch is used only for device memory and streams.  Every call goes
+through libpimdal_b200.so; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .gen import Spec
+
+_TORCH_DT = {L.U32: torch.int32, L.I32: torch.int32, L.I64: torch.int64}
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _stream(stream) -> int:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return stream.cuda_stream
+
+
+class Context:
+    """A pimdal_ctx_t plus a torch-allocated workspace it grows on demand."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        self.lib = L.lib()
+        h = C.c_void_p()
+        L.check(self.lib.pimdal_ctx_create(C.byref(h), device), "pimdal_ctx_create")
+        self.handle = h
+        self._ws: torch.Tensor | None = None
+
+    def close(self) -> None:
+        if self.handle:
+            torch.cuda.synchronize(self.device)
+            self.lib.pimdal_ctx_destroy(self.handle)
+            self.handle = None
+            self._ws = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reserve(self, nbytes: int) -> None:
+        """Makes sure the caller-owned workspace holds at least nbytes."""
+        if nbytes <= 0:
+            return
+        if self._ws is None or self._ws.numel() < nbytes:
+            size = max(nbytes, 1 << 20)
+            self._ws = torch.empty(size, dtype=torch.uint8, device=f"cuda:{self.device}")
+            L.check(self.lib.pimdal_ctx_set_workspace(self.handle, self._ws.data_ptr(), size),
+                    "pimdal_ctx_set_workspace")
+
+    def sync(self, stream=None) -> None:
+        """Waits for the stream and raises if a kernel reported a device error."""
+        L.check(self.lib.pimdal_ctx_sync_status(self.handle, _stream(stream)),
+                "pimdal_ctx_sync_status")
+
+    def set_profiling(self, enable: bool) -> None:
+        L.check(self.lib.pimdal_ctx_set_profiling(self.handle, int(enable)),
+                "pimdal_ctx_set_profiling")
+
+    def kernel_time(self, kernel_id: int) -> tuple[int, float]:
+        """(launches, summed milliseconds) of one kernel since the last read."""
+        n = C.c_uint64()
+        ms = C.c_double()
+        L.check(self.lib.pimdal_ctx_kernel_time(self.handle, kernel_id, C.byref(n), C.byref(ms)),
+                "pimdal_ctx_kernel_time")
+        return int(n.value), float(ms.value)
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.pimdal_ctx_launch_count(self.handle))
+
+
+# ---------------------------------------------------------------------------
+# Generator
+# ---------------------------------------------------------------------------
+def gen_column(ctx: Context, spec: Spec, n: int, row_offset: int = 0, out=None, stream=None):
+    """Device twin of gen.generate_cpu: returns a CUDA tensor of n values."""
+    dev = f"cuda:{ctx.device}"
+    if out is None:
+        out = torch.empty(n, dtype=_TORCH_DT[spec.out_dtype], device=dev)
+    cdf_t = None
+    if spec.cdf is not None:
+        cdf_t = torch.from_numpy(np.ascontiguousarray(spec.cdf, dtype=np.float64)).to(dev)
+    s = L.GenSpec(kind=spec.kind, out_dtype=spec.out_dtype, seed=spec.seed,
+                  stream_id=spec.stream_id, lo=spec.lo, hi=spec.hi,
+                  perm_domain=spec.perm_domain,
+                  cdf=_ptr(cdf_t), cdf_n=0 if cdf_t is None else cdf_t.numel(),
+                  match_permille=spec.match_permille)
+    L.check(ctx.lib.pimdal_gen_column(ctx.handle, C.byref(s), _ptr(out), n, row_offset,
+                                      _stream(stream)), "pimdal_gen_column")
+    if cdf_t is not None:
+        torch.cuda.current_stream().synchronize() if stream is None else stream.synchronize()
+    return out
+
+
+# ---------------------------------------------------------------------------
+# Selection (sel_kernel, pimdal/select/sel.h:21)
+# ---------------------------------------------------------------------------
+def make_pred(op: int, lo: int = 0, hi: int = 0) -> L.Pred:
+    return L.Pred(op=op, pad=0, lo=lo, hi=hi)
+
+
+def sel_kernel(ctx: Context, keys: torch.Tensor, pred: L.Pred, *, in_ptr=None, ptr_base: int = 0,
+               key_dtype: int = L.I32, out=None, out_ptr=None, want_ptr: bool = True,
+               layout: int = L.LAYOUT_COLUMNS, result=None, stream=None):
+    """Stable selection.  keys: int32 column (or int64 view of key_ptr32 pairs
+    for layout=PAIRS).  Returns (result uint64[1] device tensor, out, out_ptr)."""
+    n = keys.numel()
+    dev = keys.device
+    if out is None:
+        out = torch.empty_like(keys)
+    if layout == L.LAYOUT_COLUMNS and want_ptr and out_ptr is None:
+        out_ptr = torch.empty(n, dtype=torch.int32, device=dev)
+    if result is None:
+        result = torch.empty(1, dtype=torch.int64, device=dev)
+    a = L.SelArguments(size=n, in_=_ptr(keys), in_ptr=_ptr(in_ptr), ptr_base=ptr_base,
+                       out=_ptr(out), out_ptr=_ptr(out_ptr), pred=pred, key_dtype=key_dtype,
+                       layout=layout)
+    L.check(ctx.lib.pimdal_sel_kernel(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
+            "pimdal_sel_kernel")
+    return result, out, out_ptr
