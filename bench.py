@@ -205,8 +205,131 @@ class SelectWorkload(Workload):
         return n * reps, dt, f"reference select() body (select.cpp:77-100) on the full 2^24 column x{reps}"
 
 
-WORKLOADS = {"select": SelectWorkload}
-DEFAULT_WORKLOAD = "select"
+class SortSmjWorkload(Workload):
+    """Stable radix sort of 2^26 (uint32 key, uint32 row id) pairs with uniform
+    32-bit keys and with Zipf(1.0) keys over 2^24 distinct values, then the
+    sort-merge join of R = 2^24 unique int32 keys (a permutation of
+    0..2^24-1) with int32 payloads against S = 2^26 keys drawn uniformly from
+    R's keys with int32 payloads.  One step runs all three."""
+    name = "sort_smj"
+    N = 1 << 26
+    NR = 1 << 24
+    NS = 1 << 26
+
+    def __init__(self):
+        from pimdal_b200 import _lib as L
+        from pimdal_b200 import gen
+        self.L = L
+        s = 0xB200 + 1
+        self.spec_u = gen.Spec(L.GEN_UNIFORM, L.U32, seed=s, lo=0, hi=2**32 - 1)
+        self.spec_z = gen.Spec(L.GEN_PERM_ZIPF, L.U32, seed=s, stream_id=1, perm_domain=0,
+                               cdf=None)
+        self.spec_rk = gen.Spec(L.GEN_PERM, L.I32, seed=s, perm_domain=self.NR)
+        self.spec_rp = gen.Spec(L.GEN_UNIFORM, L.I32, seed=s, stream_id=2, lo=-2**31, hi=2**31 - 1)
+        self.spec_sk = gen.Spec(L.GEN_PERM_UNIFORM, L.I32, seed=s, stream_id=3, lo=0,
+                                hi=self.NR - 1, perm_domain=self.NR)
+        self.spec_sp = gen.Spec(L.GEN_UNIFORM, L.I32, seed=s, stream_id=4, lo=-2**31, hi=2**31 - 1)
+        self.config = {
+            "workload": "radix sort 2^26 (uint32 key, uint32 row id) pairs, uniform keys and "
+                        "Zipf(1.0) over 2^24 keys; sort-merge join R=2^24 unique int32 keys + "
+                        "int32 payload vs S=2^26 keys uniform over R + int32 payload",
+            "sort_rows": self.N, "smj_inner_rows": self.NR, "smj_outer_rows": self.NS,
+            "l2": "inputs larger than L2 (512 MiB per sorted array); L2 also flushed between steps"}
+        self.rows_per_step = 2 * self.N + self.NR + self.NS
+        self.dominant = L.KERNEL_SORT_PASS
+        self.dominant_name = "k_sort_pass (onesweep digit pass)"
+
+    def setup(self, ctx, dev):
+        import torch
+        from pimdal_b200 import gen, ops
+        self.ctx, self.ops = ctx, ops
+        self.spec_z.cdf = gen.zipf_cdf(1 << 24, 1.0)
+        g = lambda spec, n: ops.gen_column(ctx, spec, n)
+        self.ku, self.kz = g(self.spec_u, self.N), g(self.spec_z, self.N)
+        self.rows = torch.arange(self.N, dtype=torch.int32, device=dev)
+        self.rk, self.rp = g(self.spec_rk, self.NR), g(self.spec_rp, self.NR)
+        self.sk, self.sp = g(self.spec_sk, self.NS), g(self.spec_sp, self.NS)
+        e = lambda n: torch.empty(n, dtype=torch.int32, device=dev)
+        self.ou, self.oup, self.oz, self.ozp = e(self.N), e(self.N), e(self.N), e(self.N)
+        self.ji, self.jo = e(self.NS), e(self.NS)
+        self.res = torch.empty(1, dtype=torch.int64, device=dev)
+        self.step()
+        ctx.sync()
+        assert int(self.res.item()) == self.NS
+        # pinned host copies for the end-to-end run
+        pin = lambda t: t.cpu().pin_memory()
+        self.h_in = [pin(t) for t in (self.ku, self.rows, self.kz, self.rk, self.rp, self.sk, self.sp)]
+        self.d_in2 = [torch.empty_like(t) for t in (self.ku, self.rows, self.kz, self.rk, self.rp,
+                                                    self.sk, self.sp)]
+        self.h_out = [torch.empty(t.numel(), dtype=t.dtype).pin_memory()
+                      for t in (self.ou, self.oup, self.oz, self.ozp, self.ji, self.jo)]
+        # algorithmic bytes of the digit passes of one step: 16 B per pair per
+        # active pass (uniform and Zipf keys: 4 passes; R and S keys < 2^24: 3)
+        self.pass_bytes = 16 * (4 * self.N + 4 * self.N + 3 * self.NR + 3 * self.NS)
+        self.active_passes = 4 + 4 + 3 + 3
+
+    def _run(self, ku, rows, kz, rk, rp, sk, sp):
+        ops = self.ops
+        ops.sort_kernel(self.ctx, ku, rows, out=self.ou, out_ptr=self.oup)
+        ops.sort_kernel(self.ctx, kz, rows, out=self.oz, out_ptr=self.ozp)
+        ops.sort_merge_join(self.ctx, rk, rp, sk, sp, out_inner=self.ji, out_outer=self.jo,
+                            result=self.res)
+
+    def step(self):
+        self._run(self.ku, self.rows, self.kz, self.rk, self.rp, self.sk, self.sp)
+
+    def step_e2e(self, stream):
+        for d, h in zip(self.d_in2, self.h_in):
+            d.copy_(h, non_blocking=True)
+        self._run(*self.d_in2)
+        for h, d in zip(self.h_out, (self.ou, self.oup, self.oz, self.ozp, self.ji, self.jo)):
+            h.copy_(d, non_blocking=True)
+        h2d = sum(t.numel() * 4 for t in self.h_in)
+        d2h = sum(t.numel() * 4 for t in self.h_out)
+        return h2d, d2h
+
+    def roofline_bytes(self, launches: int) -> float:
+        """Algorithmic bytes of all digit-pass launches of the timed region."""
+        steps = launches / 16  # 4 + 4 + 4 + 4 pass launches per step
+        return self.pass_bytes * steps
+
+    def algorithmic_bytes_per_launch(self):
+        return self.pass_bytes / self.active_passes
+
+    def cpu_sample(self, ref, threads, budget_s):
+        """1/8 sample: reference sort of 2^23 uniform and 2^23 Zipf pairs and the
+        reference sort-merge join of 2^21 inner / 8,384,000 outer keys."""
+        from pimdal_b200 import gen
+        if not hasattr(self, "_cpu"):
+            n = self.N // 8
+            nr = self.NR // 8
+            no = 8384000
+            self.spec_z.cdf = gen.zipf_cdf(1 << 24, 1.0)
+            ku = gen.generate_cpu(self.spec_u, n)
+            kz = gen.generate_cpu(self.spec_z, n)
+            rk = (gen.generate_cpu(gen.Spec(self.L.GEN_PERM, self.L.U32, seed=7, perm_domain=nr), nr)
+                  + np.uint32(1))
+            sk = (gen.generate_cpu(gen.Spec(self.L.GEN_PERM_UNIFORM, self.L.U32, seed=7, stream_id=1,
+                                            lo=0, hi=nr - 1, perm_domain=nr), no) + np.uint32(1))
+            self._cpu = (ku, kz, rk, sk, 2 * n + nr + no)
+            for lib in ("sort", "smj_8384000"):
+                ref.set_threads(lib, threads)
+        ku, kz, rk, sk, rows = self._cpu
+        reps = 0
+        t0 = time.perf_counter()
+        while reps < 1 or time.perf_counter() - t0 < budget_s:
+            ref.sort_pairs(ku)
+            ref.sort_pairs(kz)
+            ref.smj(rk, sk, 8384000, threads=threads)
+            reps += 1
+        dt = time.perf_counter() - t0
+        return rows * reps, dt, ("reference sort_kernel (sort.cpp:30-40) on 2^23 uniform and 2^23 "
+                                 "Zipf pairs + sort_merge_join_kernel (sort_merge_join.cpp:48-103, "
+                                 f"racy with >1 thread) on 2^21 x 8384000 keys, x{reps}")
+
+
+WORKLOADS = {"select": SelectWorkload, "sort_smj": SortSmjWorkload}
+DEFAULT_WORKLOAD = "sort_smj"
 
 
 # ---------------------------------------------------------------------------
@@ -319,8 +442,11 @@ def run_ours(args) -> None:
     peak, peak_kind = hbm_peak()
     roof = None
     if k_launches:
-        avg_s = k_ms / k_launches / 1e3
-        ach = wl.algorithmic_bytes_per_launch() / avg_s / 1e9
+        if hasattr(wl, "roofline_bytes"):
+            total_b = wl.roofline_bytes(k_launches)
+        else:
+            total_b = wl.algorithmic_bytes_per_launch() * k_launches
+        ach = total_b / (k_ms / 1e3) / 1e9
         roof = {"bound": "hbm", "kernel": wl.dominant_name, "achieved": round(ach, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
                 "peak_source": peak_kind,
@@ -395,7 +521,8 @@ def run_reference(args) -> None:
     value = rows / secs
     print(json.dumps({
         "metric": "rows/s", "value": round(value, 1), "unit": "rows/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(secs / args.steps * 1e3, 3),
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(wl.rows_per_step / value * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32/uint32 keys, int64 sums", "data": "synthetic (seeded counter-based generator)",
         "config": dict(wl.config, parallelism="host CPU"), "impl": "reference",

@@ -196,6 +196,84 @@ int pimdal_sel_workspace_size(const pimdal_sel_arguments_t *args, size_t *bytes)
 int pimdal_sel_kernel(pimdal_ctx_t *ctx, const pimdal_sel_arguments_t *args,
                       pimdal_sel_results_t *d_result, pimdal_stream_t stream);
 
+/* ------------------------------------------------------------------------- */
+/* Sort.  Replaces sort_part_kernel + sort_kernel (pimdal/sort/sort.h:7-25,  */
+/* sort_keyval.c:114-179) and the CPU sort_kernel of                          */
+/* reference/db_operators/sort.cpp:30-40.  Stable ascending sort of          */
+/* (key, row id) pairs by key: equal keys keep their input order, so the     */
+/* result is fully determined.  nr_elements < 2^30.                          */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+  uint64_t nr_elements;   /* sort_arguments_t.nr_elements                      */
+  const void *in;         /* sort_arguments_t.in: key column or pairs          */
+  const uint32_t *in_ptr; /* row ids (COLUMNS); NULL = ptr_base + index         */
+  uint64_t ptr_base;
+  void *out;              /* sort_arguments_t.out: sorted keys or pairs (!= in) */
+  uint32_t *out_ptr;      /* sorted row ids (COLUMNS); NULL = keys only         */
+  int32_t key_dtype;      /* PIMDAL_U32 or PIMDAL_I32 (signed order)            */
+  int32_t layout;         /* pimdal_layout_t                                    */
+  uint32_t begin_bit;     /* sort on key bits [begin_bit, end_bit)              */
+  uint32_t end_bit;       /* 0 = 32                                             */
+} pimdal_sort_arguments_t;
+
+int pimdal_sort_workspace_size(const pimdal_sort_arguments_t *args, size_t *bytes);
+int pimdal_sort_kernel(pimdal_ctx_t *ctx, const pimdal_sort_arguments_t *args,
+                       pimdal_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
+/* Sort-merge join.  pimdal_smj_merge replaces merge_kernel of               */
+/* pimdal/join/sort_merge.h:6-23 (sort_merge.c:86-152): both relations are   */
+/* sorted by key; for every pair of rows with equal keys it emits            */
+/* (outer ptr, inner ptr) (sort_merge.c:76-77).  Every match is emitted,     */
+/* duplicates on both sides included, outer-major then inner order.  With a  */
+/* unique inner key (the reference's inputs) this equals the reference.      */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+  const void *inner;           /* merge_arguments_t.inner: sorted inner keys   */
+  const uint32_t *inner_ptr;   /* inner row ids / payloads                     */
+  uint64_t size_inner;         /* merge_arguments_t.size_inner                 */
+  const void *outer;           /* merge_arguments_t.outer: sorted outer keys   */
+  const uint32_t *outer_ptr;
+  uint64_t size_outer;         /* merge_arguments_t.size_outer                 */
+  uint32_t *out_outer;         /* merge_arguments_t.out, column of outer ptrs  */
+  uint32_t *out_inner;         /* ... and of inner ptrs                        */
+  uint64_t out_capacity;       /* rows available in out_outer / out_inner      */
+  int32_t key_dtype;           /* PIMDAL_I32 or PIMDAL_U32                      */
+  int32_t pad;
+} pimdal_smj_merge_arguments_t;
+
+typedef struct {
+  uint64_t t_count; /* merge_results_t.t_count / .out_n: total matches (even
+                       when larger than out_capacity, which then raises
+                       PIMDAL_ERR_CAPACITY at pimdal_ctx_sync_status) */
+} pimdal_merge_results_t;
+
+int pimdal_smj_merge_workspace_size(const pimdal_smj_merge_arguments_t *args, size_t *bytes);
+int pimdal_smj_merge(pimdal_ctx_t *ctx, const pimdal_smj_merge_arguments_t *args,
+                     pimdal_merge_results_t *d_result, pimdal_stream_t stream);
+
+/* Whole sort-merge join of two unsorted relations (the pipeline of
+ * pimdal/main/join/sort and reference/db_operators/sort_merge_join.cpp:48-156):
+ * stable sort of both sides by key, then the merge.  Output: for every match,
+ * the inner payload and the outer payload (payload NULL = row id). */
+typedef struct {
+  const void *inner_key;
+  const uint32_t *inner_payload;
+  uint64_t size_inner;
+  const void *outer_key;
+  const uint32_t *outer_payload;
+  uint64_t size_outer;
+  uint32_t *out_inner_payload;
+  uint32_t *out_outer_payload;
+  uint64_t out_capacity;
+  int32_t key_dtype;
+  int32_t pad;
+} pimdal_smj_arguments_t;
+
+int pimdal_sort_merge_join_workspace_size(const pimdal_smj_arguments_t *args, size_t *bytes);
+int pimdal_sort_merge_join(pimdal_ctx_t *ctx, const pimdal_smj_arguments_t *args,
+                           pimdal_merge_results_t *d_result, pimdal_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -236,13 +236,15 @@ class Ref:
         g = int(f(_p(k), _p(v), n, *map(_p, outs)))
         return tuple(o[:g] for o in outs)
 
-    def smj(self, inner_keys, outer_keys, buffer_size: int):
-        """Reference sort-merge join on key columns (one thread; the outer
-        size must equal the library's BUFFER_SIZE).  Returns (matched inner
-        keys, sorted outer keys)."""
+    def smj(self, inner_keys, outer_keys, buffer_size: int, threads: int = 1):
+        """Reference sort-merge join on key columns (the outer size must equal
+        the library's BUFFER_SIZE).  With one thread the result is exact:
+        (matched inner keys, sorted outer keys); with more threads the
+        reference's shared merge cursor races (sort_merge_join.cpp:81-101),
+        which is only used for timing."""
         lb = self._get(f"smj_{buffer_size}")
         lb.pimdal_ref_set_threads.argtypes = [C.c_int]
-        lb.pimdal_ref_set_threads(1)
+        lb.pimdal_ref_set_threads(threads)
         f = lb.pimdal_ref_smj
         f.restype = None
         f.argtypes = [_P, _U64, _P, _U64, _P, _P]

@@ -57,6 +57,33 @@ class SelArguments(C.Structure):
     ]
 
 
+class SortArguments(C.Structure):
+    _fields_ = [
+        ("nr_elements", C.c_uint64), ("in_", C.c_void_p), ("in_ptr", C.c_void_p),
+        ("ptr_base", C.c_uint64), ("out", C.c_void_p), ("out_ptr", C.c_void_p),
+        ("key_dtype", C.c_int32), ("layout", C.c_int32),
+        ("begin_bit", C.c_uint32), ("end_bit", C.c_uint32),
+    ]
+
+
+class SmjMergeArguments(C.Structure):
+    _fields_ = [
+        ("inner", C.c_void_p), ("inner_ptr", C.c_void_p), ("size_inner", C.c_uint64),
+        ("outer", C.c_void_p), ("outer_ptr", C.c_void_p), ("size_outer", C.c_uint64),
+        ("out_outer", C.c_void_p), ("out_inner", C.c_void_p), ("out_capacity", C.c_uint64),
+        ("key_dtype", C.c_int32), ("pad", C.c_int32),
+    ]
+
+
+class SmjArguments(C.Structure):
+    _fields_ = [
+        ("inner_key", C.c_void_p), ("inner_payload", C.c_void_p), ("size_inner", C.c_uint64),
+        ("outer_key", C.c_void_p), ("outer_payload", C.c_void_p), ("size_outer", C.c_uint64),
+        ("out_inner_payload", C.c_void_p), ("out_outer_payload", C.c_void_p),
+        ("out_capacity", C.c_uint64), ("key_dtype", C.c_int32), ("pad", C.c_int32),
+    ]
+
+
 # Exported symbols and their ctypes signatures.
 _VP, _SZ, _U64, _I = C.c_void_p, C.c_size_t, C.c_uint64, C.c_int
 SIGNATURES = {
@@ -72,6 +99,12 @@ SIGNATURES = {
     "pimdal_gen_column": (_I, [_VP, C.POINTER(GenSpec), _VP, _U64, _U64, _VP]),
     "pimdal_sel_workspace_size": (_I, [C.POINTER(SelArguments), C.POINTER(_SZ)]),
     "pimdal_sel_kernel": (_I, [_VP, C.POINTER(SelArguments), _VP, _VP]),
+    "pimdal_sort_workspace_size": (_I, [C.POINTER(SortArguments), C.POINTER(_SZ)]),
+    "pimdal_sort_kernel": (_I, [_VP, C.POINTER(SortArguments), _VP]),
+    "pimdal_smj_merge_workspace_size": (_I, [C.POINTER(SmjMergeArguments), C.POINTER(_SZ)]),
+    "pimdal_smj_merge": (_I, [_VP, C.POINTER(SmjMergeArguments), _VP, _VP]),
+    "pimdal_sort_merge_join_workspace_size": (_I, [C.POINTER(SmjArguments), C.POINTER(_SZ)]),
+    "pimdal_sort_merge_join": (_I, [_VP, C.POINTER(SmjArguments), _VP, _VP]),
 }
 
 _lib = None

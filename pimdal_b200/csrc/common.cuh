@@ -28,6 +28,10 @@ enum : uint32_t {
   PD_DEVERR_ARG = 8u          // a device-side argument check failed
 };
 
+// Slots of pimdal_ctx::d_counters (two words each: claim counter, CTAs done).
+enum : uint32_t { PD_COUNTER_SELECT = 0, PD_COUNTER_PARTITION = 2, PD_COUNTER_GROUP = 4,
+                  PD_COUNTER_PROBE = 6, PD_COUNTER_MERGE = 8 };
+
 // Lookback status word: [epoch:16][flag:2][value:46].
 enum : uint32_t { PD_FLAG_INVALID = 0, PD_FLAG_AGGREGATE = 1, PD_FLAG_INCLUSIVE = 2 };
 constexpr uint64_t PD_STATUS_VALUE_MASK = (1ull << 46) - 1;
@@ -47,7 +51,8 @@ struct pimdal_ctx {
   size_t ws_bytes = 0;
   bool ws_owned = false;
   // device words
-  uint32_t *d_error = nullptr;   // error bits
+  uint32_t *d_error = nullptr;   // error bits (word 0 of a zeroed 256-byte block)
+  uint32_t *d_counters = nullptr;  // self-resetting work counters (words 16..63)
   uint64_t *d_status = nullptr;  // PD_STATUS_WORDS lookback status words
   uint32_t epoch = 0;            // 16-bit epoch of the last lookback launch
   uint64_t launches = 0;         // kernels launched through this context
@@ -79,8 +84,8 @@ uint32_t pd_next_epoch(pimdal_ctx *ctx, cudaStream_t stream, int *status);
 // Maps the outcome of a launch to a status code.
 int pd_launch_status(pimdal_ctx *ctx);
 
-static inline size_t pd_align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
-static inline uint64_t pd_ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
+PD_HD uint64_t pd_align_up(uint64_t x, uint64_t a) { return (x + a - 1) / a * a; }
+PD_HD uint64_t pd_ceil_div(uint64_t a, uint64_t b) { return (a + b - 1) / b; }
 
 #define PD_CHECK_CUDA(expr)                      \
   do {                                           \
@@ -108,20 +113,100 @@ __device__ __forceinline__ uint32_t pd_load_acquire_u32(const uint32_t *p) {
   return v;
 }
 
+__device__ __forceinline__ void pd_store_relaxed_u64(uint64_t *p, uint64_t v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t pd_load_relaxed_u64(const uint64_t *p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// ---- TMA bulk copies (non-multicast, this CTA's own shared memory) --------
+__device__ __forceinline__ uint32_t pd_smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void pd_mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(pd_smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void pd_fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void pd_mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(pd_smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool pd_mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(pd_smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Orders this CTA's generic-proxy shared-memory accesses before later
+// async-proxy (bulk copy) writes to the same buffer.
+__device__ __forceinline__ void pd_fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ uint64_t pd_policy_evict_last() {
+  uint64_t pol;
+  asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+  return pol;
+}
+// Global -> shared bulk copy completing on `bar`; src, dst 16-byte aligned,
+// bytes a multiple of 16.  `pol` is an L2 cache policy.
+__device__ __forceinline__ void pd_bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                            uint64_t *bar, uint64_t pol) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+      " [%0], [%1], %2, [%3], %4;" ::"r"(pd_smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(pd_smem_u32(bar)), "l"(pol)
+      : "memory");
+}
+
 __device__ __forceinline__ uint64_t pd_pack_status(uint32_t epoch, uint32_t flag, uint64_t v) {
   return ((uint64_t)epoch << 48) | ((uint64_t)flag << 46) | (v & PD_STATUS_VALUE_MASK);
 }
 
+__device__ __forceinline__ uint64_t pd_globaltimer_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait shared by every spin in the library: returns true when the
+// caller must give up -- either this wait exceeded PD_WAIT_NS (then the
+// timeout bit is set) or another wait in the same launch already gave up
+// (the error word is non-zero), so a broken dependency chain costs one
+// timeout, not one per waiter.
+constexpr uint64_t PD_WAIT_NS = 200ull * 1000 * 1000;
+__device__ __forceinline__ bool pd_wait_expired(uint32_t *d_error, uint64_t t0, uint32_t spins) {
+  if ((spins & 63u) == 0) {
+    if (*(volatile uint32_t *)d_error & PD_DEVERR_TIMEOUT) return true;
+    if (pd_globaltimer_ns() - t0 > PD_WAIT_NS) {
+      atomicOr(d_error, PD_DEVERR_TIMEOUT);
+      return true;
+    }
+  }
+  return spins > PD_SPIN_LIMIT;
+}
+
 // Warp-cooperative decoupled look-back: returns the exclusive prefix of tile
 // `tile` (sum of the values of tiles < tile).  Must be called by all 32 lanes
-// of one warp.  Gives up after PD_SPIN_LIMIT polls, sets PD_DEVERR_TIMEOUT and
-// returns the partial sum (the result is then invalid but the kernel ends).
+// of one warp.  On a bounded-wait expiry it sets PD_DEVERR_TIMEOUT and returns
+// the partial sum (the result is then invalid but the kernel ends).
 __device__ __forceinline__ uint64_t pd_lookback_warp(const uint64_t *status, int64_t tile,
                                                      uint32_t epoch, uint32_t *d_error) {
   const int lane = threadIdx.x & 31;
   uint64_t exclusive = 0;
   int64_t base = tile - 1;
   uint32_t spins = 0;
+  const uint64_t t0 = pd_globaltimer_ns();
   while (true) {
     int64_t pred = base - lane;
     uint32_t flag = PD_FLAG_INCLUSIVE;
@@ -136,7 +221,10 @@ __device__ __forceinline__ uint64_t pd_lookback_warp(const uint64_t *status, int
     int first = incl ? (__ffs(incl) - 1) : 31;
     unsigned need = (first >= 31) ? 0xffffffffu : ((2u << first) - 1u);
     if (invalid & need) {
-      if (++spins > PD_SPIN_LIMIT) {
+      bool give_up = false;
+      ++spins;
+      if (lane == 0) give_up = pd_wait_expired(d_error, t0, spins);
+      if (__shfl_sync(0xffffffffu, give_up, 0)) {
         if (lane == 0) atomicOr(d_error, PD_DEVERR_TIMEOUT);
         return exclusive;
       }
@@ -151,6 +239,73 @@ __device__ __forceinline__ uint64_t pd_lookback_warp(const uint64_t *status, int
     base -= 32;
   }
   return exclusive;
+}
+
+// Block-wide decoupled look-back over epoch-tagged 64-bit status words: thread
+// i inspects predecessor (chunk - 1 - i) in each round, so one round covers
+// THREADS predecessors.  Called by all threads of the block; s_flags holds
+// 2 * THREADS/32 words, s_sum THREADS/32 + 1.
+template <int THREADS>
+__device__ uint64_t pd_block_lookback(const uint64_t *status, int64_t chunk, uint32_t epoch,
+                                   uint32_t *d_error, uint32_t *s_flags, uint64_t *s_sum,
+                                   int *s_state) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint64_t exclusive = 0;
+  int64_t base = chunk - 1;
+  uint32_t spins = 0;
+  const uint64_t t0 = pd_globaltimer_ns();
+  while (true) {
+    int64_t pred = base - tid;
+    uint32_t flag = PD_FLAG_INCLUSIVE;
+    uint64_t val = 0;
+    if (pred >= 0) {
+      uint64_t w = pd_load_relaxed_u64(status + pred);
+      flag = ((uint32_t)(w >> 48) == epoch) ? (uint32_t)((w >> 46) & 3u) : PD_FLAG_INVALID;
+      val = w & PD_STATUS_VALUE_MASK;
+    }
+    unsigned incl = __ballot_sync(0xffffffffu, flag == PD_FLAG_INCLUSIVE);
+    unsigned inval = __ballot_sync(0xffffffffu, flag == PD_FLAG_INVALID);
+    int first = incl ? (__ffs(incl) - 1) : 32;
+    uint64_t c = (lane <= first) ? val : 0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if (lane == 0) {
+      s_flags[2 * warp] = incl;
+      s_flags[2 * warp + 1] = inval;
+      s_sum[warp] = c;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      // 0 = retry, 1 = done, 2 = continue further back
+      int state = 2;
+      uint64_t add = 0;
+      for (int w = 0; w < (THREADS / 32); ++w) {
+        unsigned in = s_flags[2 * w], iv = s_flags[2 * w + 1];
+        int f = in ? (__ffs(in) - 1) : 32;
+        unsigned need = (f >= 31) ? 0xffffffffu : ((2u << f) - 1u);
+        if (iv & need) { state = 0; break; }
+        add += s_sum[w];
+        if (in) { state = 1; break; }
+      }
+      if (state == 0) {
+        if (pd_wait_expired(d_error, t0, ++spins)) state = 3;
+      } else {
+        s_sum[(THREADS / 32)] = add;
+      }
+      *s_state = state;
+    }
+    __syncthreads();
+    int state = *s_state;
+    if (state == 3) return exclusive;
+    if (state == 0) {
+      __nanosleep(100);
+      continue;
+    }
+    exclusive += s_sum[(THREADS / 32)];
+    __syncthreads();
+    if (state == 1) return exclusive;
+    base -= THREADS;
+  }
 }
 
 // ---------------------------------------------------------------------------

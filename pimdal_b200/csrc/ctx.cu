@@ -44,6 +44,7 @@ extern "C" int pimdal_ctx_create(pimdal_ctx_t **out, int device) {
     delete ctx;
     return PIMDAL_ERR_CUDA;
   }
+  ctx->d_counters = ctx->d_error + 16;
   *out = ctx;
   return PIMDAL_OK;
 }
@@ -137,7 +138,7 @@ extern "C" int pimdal_ctx_sync_status(pimdal_ctx_t *ctx, pimdal_stream_t stream)
   PD_CHECK_CUDA(cudaMemcpyAsync(&word, ctx->d_error, sizeof(word), cudaMemcpyDeviceToHost, s));
   PD_CHECK_CUDA(cudaStreamSynchronize(s));
   if (word) {
-    PD_CHECK_CUDA(cudaMemsetAsync(ctx->d_error, 0, sizeof(uint32_t), s));
+    PD_CHECK_CUDA(cudaMemsetAsync(ctx->d_error, 0, 256, s));
     PD_CHECK_CUDA(cudaStreamSynchronize(s));
   }
   if (word & PD_DEVERR_TIMEOUT) return PIMDAL_ERR_DEVICE_TIMEOUT;

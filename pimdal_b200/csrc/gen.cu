@@ -78,9 +78,11 @@ extern "C" int pimdal_gen_column(pimdal_ctx_t *ctx, const pimdal_gen_spec_t *s, 
   p.out_bytes = (s->out_dtype == PIMDAL_I64) ? 8 : 4;
   p.draw_key = pd_stream_key(s->seed, s->stream_id);
   p.lo = s->lo;
-  if (s->hi < s->lo) return PIMDAL_ERR_ARG;
-  p.span = (uint64_t)(s->hi - s->lo) + 1;
-  if (p.span > (1ull << 32) || p.span == 0) p.span = 0;
+  p.span = 0;  // only the uniform kinds use [lo, hi]
+  if (s->hi >= s->lo) {
+    p.span = (uint64_t)(s->hi - s->lo) + 1;
+    if (p.span > (1ull << 32)) p.span = 0;
+  }
   if (s->perm_domain > (1ull << 32)) return PIMDAL_ERR_ARG;
   p.perm = pd_make_perm(s->seed, s->perm_domain);
   p.cdf = s->cdf;

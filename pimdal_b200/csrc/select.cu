@@ -16,6 +16,8 @@
 // elements are compacted in shared memory and written out with coalesced
 // stores.  The create_ptr / out_val glue is fused: row ids are generated
 // (ptr_base + index) unless a row-id column is given.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace {
@@ -35,7 +37,7 @@ struct SelParams {
   void *out;
   uint32_t *out_ptr;
   uint64_t n;
-  int64_t lo, hi;
+  uint32_t lo32, range32;  // selected: (key - lo32) mod 2^32 <= range32, xor invert
   uint32_t invert;
   uint32_t vec_ok;  // input pointers 16-byte aligned
   uint64_t *status;
@@ -44,10 +46,12 @@ struct SelParams {
   uint64_t *d_count;
 };
 
+// One subtract and one unsigned compare: for lo <= hi in the key's own order,
+// lo <= v <= hi  <=>  (v - lo) mod 2^32 <= (hi - lo), for signed and unsigned
+// 32-bit keys alike (the host clamps the interval to the key type's range).
 template <bool SIGNED>
 __device__ __forceinline__ bool sel_pred(uint32_t key, const SelParams &p) {
-  int64_t v = SIGNED ? (int64_t)(int32_t)key : (int64_t)key;
-  return ((v >= p.lo) & (v <= p.hi)) != (p.invert != 0);
+  return ((key - p.lo32) <= p.range32) != (p.invert != 0);
 }
 
 // LAYOUT: PIMDAL_LAYOUT_COLUMNS or PIMDAL_LAYOUT_PAIRS; HAS_PTR: a row-id
@@ -194,7 +198,268 @@ __global__ void __launch_bounds__(SEL_THREADS) k_select(SelParams p) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Large inputs: persistent CTAs, one per SM, each claiming ~450 KB chunks.
+//   A. stream the chunk through a TMA bulk-copy ring (evict_last) and count;
+//   B. publish the chunk count and resolve its output offset with one
+//      block-wide decoupled look-back (1024 predecessors per round);
+//   C. re-read the chunk (L2 hits) tile by tile, rank and write the rows.
+// DRAM sees one read of the input and one write of the output; the look-back
+// happens once per chunk instead of once per 16 KB tile.
+// ---------------------------------------------------------------------------
+constexpr int SL_THREADS = 1024;
+constexpr int SL_WARPS = SL_THREADS / 32;
+constexpr int SL_STAGE_BYTES = 32768;
+constexpr int SL_STAGES = 4;
+constexpr int SL_TILE = SL_THREADS * 8;  // phase-C tile: 8 elements per thread
+constexpr uint64_t SL_CHUNK_MAX = 1u << 17;
+
+struct SlParams {
+  SelParams s;
+  uint64_t chunk_elems, nchunks;
+  uint32_t *claim;  // [0] next chunk, [1] CTAs done claiming (self-resetting)
+};
+
+__device__ __forceinline__ uint32_t block_reduce_sum_1024(uint32_t v, uint32_t *s_red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (lane == 0) s_red[warp] = v;
+  __syncthreads();
+  uint32_t t = s_red[lane];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  __syncthreads();
+  return t;
+}
+
+template <int LAYOUT, bool SIGNED, bool HAS_PTR>
+__global__ void __launch_bounds__(SL_THREADS, 1) k_select_chunked(SlParams q) {
+  extern __shared__ __align__(128) unsigned char s_ring[];
+  __shared__ uint64_t s_bar[SL_STAGES];
+  __shared__ uint32_t s_red[32];
+  __shared__ uint32_t s_flags[2 * SL_WARPS];
+  __shared__ uint64_t s_sum[SL_WARPS + 1];
+  __shared__ uint32_t s_off[2 * SL_WARPS];
+  __shared__ int s_state;
+  __shared__ uint64_t s_chunk, s_prefix;
+
+  const SelParams &p = q.s;
+  constexpr int EB = (LAYOUT == PIMDAL_LAYOUT_PAIRS) ? 8 : 4;  // bytes per element
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    for (int i = 0; i < SL_STAGES; ++i) pd_mbar_init(&s_bar[i], 1);
+    pd_fence_mbar_init();
+  }
+  __syncthreads();
+  const uint64_t pol = pd_policy_evict_last();
+  uint32_t consumed = 0, issued = 0;  // ring stages (thread 0 issues)
+
+  while (true) {
+    if (tid == 0) {
+      uint64_t c = atomicAdd(q.claim, 1u);
+      if (c >= q.nchunks) {
+        // Last claimer of the launch resets the counters for the next launch.
+        if (atomicAdd(q.claim + 1, 1u) == gridDim.x - 1) {
+          q.claim[0] = 0;
+          q.claim[1] = 0;
+        }
+      }
+      s_chunk = c;
+    }
+    __syncthreads();
+    const uint64_t chunk = s_chunk;
+    if (chunk >= q.nchunks) break;
+    const uint64_t c0 = chunk * q.chunk_elems;
+    const uint64_t c1 = min(p.n, c0 + q.chunk_elems);
+    const char *src = reinterpret_cast<const char *>(p.in) + c0 * EB;
+    const uint64_t bytes = (c1 - c0) * EB;
+    const uint64_t bulk_bytes = bytes & ~(uint64_t)15;
+    const uint32_t nst = (uint32_t)pd_ceil_div(bulk_bytes, SL_STAGE_BYTES);
+
+    // ---- A: count through the bulk-copy ring ------------------------------
+    if (tid == 0) {
+      for (uint32_t j = 0; j < nst && j < (uint32_t)SL_STAGES; ++j) {
+        uint32_t slot = issued % SL_STAGES;
+        uint32_t b = (uint32_t)min((uint64_t)SL_STAGE_BYTES, bulk_bytes - (uint64_t)j * SL_STAGE_BYTES);
+        pd_mbar_expect_tx(&s_bar[slot], b);
+        pd_bulk_g2s(s_ring + slot * SL_STAGE_BYTES, src + (uint64_t)j * SL_STAGE_BYTES, b,
+                    &s_bar[slot], pol);
+        ++issued;
+      }
+    }
+    uint32_t cnt = 0;
+    for (uint32_t j = 0; j < nst; ++j) {
+      const uint32_t slot = consumed % SL_STAGES, parity = (consumed / SL_STAGES) & 1u;
+      const uint32_t b = (uint32_t)min((uint64_t)SL_STAGE_BYTES, bulk_bytes - (uint64_t)j * SL_STAGE_BYTES);
+      uint32_t spins = 0;
+      const uint64_t t0 = pd_globaltimer_ns();
+      while (!pd_mbar_try_wait(&s_bar[slot], parity)) {
+        if (pd_wait_expired(p.d_error, t0, ++spins)) break;
+      }
+      const uint4 *v = reinterpret_cast<const uint4 *>(s_ring + slot * SL_STAGE_BYTES);
+      for (uint32_t i = tid; i < b / 16; i += SL_THREADS) {
+        uint4 x = v[i];
+        if (LAYOUT == PIMDAL_LAYOUT_PAIRS) {
+          cnt += sel_pred<SIGNED>(x.x, p) + sel_pred<SIGNED>(x.z, p);
+        } else {
+          cnt += sel_pred<SIGNED>(x.x, p) + sel_pred<SIGNED>(x.y, p) + sel_pred<SIGNED>(x.z, p) +
+                 sel_pred<SIGNED>(x.w, p);
+        }
+      }
+      __syncthreads();
+      if (tid == 0 && j + SL_STAGES < nst) {
+        const uint32_t jn = j + SL_STAGES;
+        const uint32_t bn = (uint32_t)min((uint64_t)SL_STAGE_BYTES, bulk_bytes - (uint64_t)jn * SL_STAGE_BYTES);
+        pd_fence_proxy_async_smem();
+        pd_mbar_expect_tx(&s_bar[slot], bn);
+        pd_bulk_g2s(s_ring + slot * SL_STAGE_BYTES, src + (uint64_t)jn * SL_STAGE_BYTES, bn,
+                    &s_bar[slot], pol);
+        ++issued;
+      }
+      ++consumed;
+    }
+    // tail elements not covered by 16-byte bulk copies
+    for (uint64_t e = c0 + bulk_bytes / EB + tid; e < c1; e += SL_THREADS) {
+      uint32_t k = (LAYOUT == PIMDAL_LAYOUT_PAIRS)
+                       ? reinterpret_cast<const pimdal_key_ptr32_t *>(p.in)[e].key
+                       : reinterpret_cast<const uint32_t *>(p.in)[e];
+      cnt += sel_pred<SIGNED>(k, p);
+    }
+    const uint32_t total = block_reduce_sum_1024(cnt, s_red);
+
+    // ---- B: chunk offset ---------------------------------------------------
+    if (chunk == 0) {
+      if (tid == 0) {
+        pd_store_relaxed_u64(p.status, pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, total));
+        s_prefix = 0;
+      }
+    } else {
+      if (tid == 0)
+        pd_store_relaxed_u64(p.status + chunk, pd_pack_status(p.epoch, PD_FLAG_AGGREGATE, total));
+      uint64_t pre = pd_block_lookback<SL_THREADS>(p.status, (int64_t)chunk, p.epoch, p.d_error, s_flags, s_sum,
+                                    &s_state);
+      if (tid == 0) {
+        pd_store_relaxed_u64(p.status + chunk,
+                             pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, pre + total));
+        s_prefix = pre;
+      }
+    }
+    __syncthreads();
+    uint64_t out_base = s_prefix;
+    if (chunk == q.nchunks - 1 && tid == 0) *p.d_count = out_base + total;
+
+    // ---- C: rank and write, tile by tile (input re-read from L2) -----------
+    for (uint64_t t0e = c0; t0e < c1; t0e += SL_TILE) {
+      uint32_t key[8], ptr[8];
+      uint32_t sel = 0;
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        const uint64_t e0 = t0e + (uint64_t)c * (SL_THREADS * 4) + (uint64_t)tid * 4;
+        if (e0 + 4 <= c1) {
+          if (LAYOUT == PIMDAL_LAYOUT_PAIRS) {
+            const uint4 *s4 = reinterpret_cast<const uint4 *>(
+                reinterpret_cast<const pimdal_key_ptr32_t *>(p.in) + e0);
+            uint4 a = __ldcs(s4), b2 = __ldcs(s4 + 1);
+            key[c * 4 + 0] = a.x; ptr[c * 4 + 0] = a.y; key[c * 4 + 1] = a.z; ptr[c * 4 + 1] = a.w;
+            key[c * 4 + 2] = b2.x; ptr[c * 4 + 2] = b2.y; key[c * 4 + 3] = b2.z; ptr[c * 4 + 3] = b2.w;
+          } else {
+            uint4 a = __ldcs(reinterpret_cast<const uint4 *>(reinterpret_cast<const uint32_t *>(p.in) + e0));
+            key[c * 4 + 0] = a.x; key[c * 4 + 1] = a.y; key[c * 4 + 2] = a.z; key[c * 4 + 3] = a.w;
+            if (HAS_PTR) {
+              uint4 b2 = __ldcs(reinterpret_cast<const uint4 *>(p.in_ptr + e0));
+              ptr[c * 4 + 0] = b2.x; ptr[c * 4 + 1] = b2.y; ptr[c * 4 + 2] = b2.z; ptr[c * 4 + 3] = b2.w;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const bool ok = e0 + j < c1;
+            if (LAYOUT == PIMDAL_LAYOUT_PAIRS) {
+              const pimdal_key_ptr32_t *pp = reinterpret_cast<const pimdal_key_ptr32_t *>(p.in);
+              key[c * 4 + j] = ok ? pp[e0 + j].key : 0u;
+              ptr[c * 4 + j] = ok ? pp[e0 + j].ptr : 0u;
+            } else {
+              key[c * 4 + j] = ok ? reinterpret_cast<const uint32_t *>(p.in)[e0 + j] : 0u;
+              if (HAS_PTR) ptr[c * 4 + j] = ok ? p.in_ptr[e0 + j] : 0u;
+            }
+          }
+        }
+        if (LAYOUT != PIMDAL_LAYOUT_PAIRS && !HAS_PTR) {
+#pragma unroll
+          for (int j = 0; j < 4; ++j) ptr[c * 4 + j] = (uint32_t)(p.ptr_base + e0 + j);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          bool s = (e0 + j < c1) && sel_pred<SIGNED>(key[c * 4 + j], p);
+          sel |= (uint32_t)s << (c * 4 + j);
+        }
+      }
+      // byte-packed counts of the 2 sub-chunks; warp scan; (sub-chunk, warp) scan
+      uint32_t packed = (uint32_t)__popc(sel & 0xFu) | ((uint32_t)__popc((sel >> 4) & 0xFu) << 8);
+      uint32_t inc = packed;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += t;
+      }
+      const uint32_t excl = inc - packed;
+      if (lane == 31) {
+        s_off[warp] = inc & 0xFFu;
+        s_off[SL_WARPS + warp] = (inc >> 8) & 0xFFu;
+      }
+      __syncthreads();
+      if (warp == 0) {
+        // entries in tile order: sub-chunk 0 warps 0..31, then sub-chunk 1
+        uint32_t a = s_off[2 * lane], b2 = s_off[2 * lane + 1];
+        uint32_t x = a + b2, xi = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          uint32_t t = __shfl_up_sync(0xffffffffu, xi, o);
+          if (lane >= o) xi += t;
+        }
+        uint32_t ex = xi - x;
+        s_off[2 * lane] = ex;
+        s_off[2 * lane + 1] = ex + a;
+        if (lane == 31) s_red[0] = xi;
+      }
+      __syncthreads();
+      const uint32_t tile_total = s_red[0];
+#pragma unroll
+      for (int c = 0; c < 2; ++c) {
+        uint64_t r = out_base + s_off[c * SL_WARPS + warp] + ((excl >> (8 * c)) & 0xFFu);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          if ((sel >> (c * 4 + j)) & 1u) {
+            if (LAYOUT == PIMDAL_LAYOUT_PAIRS) {
+              reinterpret_cast<uint2 *>(p.out)[r] = make_uint2(key[c * 4 + j], ptr[c * 4 + j]);
+            } else {
+              reinterpret_cast<uint32_t *>(p.out)[r] = key[c * 4 + j];
+              if (p.out_ptr) p.out_ptr[r] = ptr[c * 4 + j];
+            }
+            ++r;
+          }
+        }
+      }
+      out_base += tile_total;
+      __syncthreads();
+    }
+  }
+}
+
 using SelKernel = void (*)(SelParams);
+using SlKernel = void (*)(SlParams);
+
+SlKernel pick_chunked(int layout, bool is_signed, bool has_ptr) {
+  if (layout == PIMDAL_LAYOUT_PAIRS)
+    return is_signed ? k_select_chunked<PIMDAL_LAYOUT_PAIRS, true, true>
+                     : k_select_chunked<PIMDAL_LAYOUT_PAIRS, false, true>;
+  if (is_signed)
+    return has_ptr ? k_select_chunked<PIMDAL_LAYOUT_COLUMNS, true, true>
+                   : k_select_chunked<PIMDAL_LAYOUT_COLUMNS, true, false>;
+  return has_ptr ? k_select_chunked<PIMDAL_LAYOUT_COLUMNS, false, true>
+                 : k_select_chunked<PIMDAL_LAYOUT_COLUMNS, false, false>;
+}
 
 SelKernel pick_kernel(int layout, bool is_signed, bool has_ptr) {
   if (layout == PIMDAL_LAYOUT_PAIRS)
@@ -248,7 +513,23 @@ extern "C" int pimdal_sel_kernel(pimdal_ctx_t *ctx, const pimdal_sel_arguments_t
   if (a->layout == PIMDAL_LAYOUT_PAIRS && (((uintptr_t)a->in | (uintptr_t)a->out) & 7u))
     return PIMDAL_ERR_ARG;
   SelParams p{};
-  if (!pd_pred_interval(a->pred, &p.lo, &p.hi, &p.invert)) return PIMDAL_ERR_ARG;
+  int64_t lo, hi;
+  if (!pd_pred_interval(a->pred, &lo, &hi, &p.invert)) return PIMDAL_ERR_ARG;
+  {
+    // clamp to the key type's range; an empty interval selects nothing
+    const int64_t tmin = a->key_dtype == PIMDAL_I32 ? INT32_MIN : 0;
+    const int64_t tmax = a->key_dtype == PIMDAL_I32 ? INT32_MAX : (int64_t)UINT32_MAX;
+    lo = std::max(lo, tmin);
+    hi = std::min(hi, tmax);
+    if (lo > hi) {  // empty: "all in range, inverted" (or all, when inverted)
+      p.lo32 = 0;
+      p.range32 = 0xFFFFFFFFu;
+      p.invert ^= 1u;
+    } else {
+      p.lo32 = (uint32_t)lo;
+      p.range32 = (uint32_t)(hi - lo);
+    }
+  }
   cudaStream_t s = (cudaStream_t)stream;
   cudaSetDevice(ctx->device);
   if (a->size == 0) {
@@ -270,8 +551,22 @@ extern "C" int pimdal_sel_kernel(pimdal_ctx_t *ctx, const pimdal_sel_arguments_t
   p.status = ctx->d_status;
   p.d_error = ctx->d_error;
   p.d_count = &d_result->t_count;
-  SelKernel k = pick_kernel(a->layout, a->key_dtype == PIMDAL_I32, p.in_ptr != nullptr);
-  {
+  const bool is_signed = a->key_dtype == PIMDAL_I32;
+  if (p.vec_ok && a->size >= (1u << 20)) {
+    SlParams q{};
+    q.s = p;
+    const uint64_t per_sm = pd_ceil_div(a->size, (uint64_t)ctx->sm_count);
+    q.chunk_elems = std::min<uint64_t>(SL_CHUNK_MAX, pd_align_up(per_sm, SL_TILE));
+    q.nchunks = pd_ceil_div(a->size, q.chunk_elems);
+    q.claim = ctx->d_counters + PD_COUNTER_SELECT;
+    const unsigned grid = (unsigned)std::min<uint64_t>(q.nchunks, (uint64_t)ctx->sm_count);
+    SlKernel k = pick_chunked(a->layout, is_signed, p.in_ptr != nullptr);
+    const int smem = SL_STAGES * SL_STAGE_BYTES;
+    PD_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    pd_launch_scope scope(ctx, PIMDAL_KERNEL_SELECT, s);
+    k<<<grid, SL_THREADS, smem, s>>>(q);
+  } else {
+    SelKernel k = pick_kernel(a->layout, is_signed, p.in_ptr != nullptr);
     pd_launch_scope scope(ctx, PIMDAL_KERNEL_SELECT, s);
     k<<<(unsigned)tiles, SEL_THREADS, 0, s>>>(p);
   }

@@ -1,0 +1,331 @@
+// K-SMJ: merge-path sort-merge join (pimdal_smj_merge, pimdal_sort_merge_join).
+//
+// Reference behaviour: merge_kernel (pimdal/join/sort_merge.h:6-23,
+// sort_merge.c:54-152) walks a sorted outer relation against a sorted inner
+// relation and emits (outer ptr, inner ptr) for equal keys (sort_merge.c:76-77);
+// the CPU operator reference/db_operators/sort_merge_join.cpp:48-103 sorts
+// both relations and merges them.  This operator emits every matching pair
+// (duplicates on both sides included), outer-major and, within one outer
+// row, in inner order -- with stably sorted inputs the output order is fully
+// determined.
+//
+// B200 design:
+//  1. k_smj_bounds: one thread per 2048-row outer tile finds the inner range
+//     the tile can match: [lower_bound(first key), upper_bound(last key)).
+//  2. k_smj_merge: a CTA takes the next outer tile, stages the tile's inner
+//     range in shared memory (when it fits; otherwise it searches HBM), finds
+//     each outer row's match range by binary search, scans the match counts,
+//     resolves the tile's output offset with a block-wide decoupled
+//     look-back, and writes the pairs.
+// The full join (pimdal_sort_merge_join) sorts both sides with K-SORT first.
+#include <algorithm>
+
+#include "common.cuh"
+
+int pd_sort_with_workspace(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, void *ws,
+                           cudaStream_t s);
+
+namespace {
+
+constexpr int MJ_THREADS = 256;
+constexpr int MJ_WARPS = MJ_THREADS / 32;
+constexpr int MJ_ITEMS = 8;
+constexpr int MJ_TILE = MJ_THREADS * MJ_ITEMS;  // 2048 outer rows per tile
+constexpr int MJ_INNER_CAP = 4096;               // inner rows staged in shared memory
+
+struct MergeParams {
+  const uint32_t *ikey, *iptr;  // sorted inner (keys, payload / row id)
+  const uint32_t *okey, *optr;  // sorted outer
+  uint64_t ni, no;
+  uint32_t *out_outer, *out_inner;
+  uint64_t cap;
+  uint32_t flip;
+  uint64_t tiles;
+  uint64_t *bounds;  // [2 * tiles]: inner range per tile
+  uint64_t *status;
+  uint32_t epoch;
+  uint32_t *claim;   // tile counter (zeroed by the host before the launch)
+  uint32_t *d_error;
+  uint64_t *d_count;
+};
+
+__device__ __forceinline__ uint32_t ord(uint32_t k, uint32_t flip) { return k ^ flip; }
+
+// First index in [lo, hi) whose key is >= v (upper = false) or > v (upper = true).
+__device__ __forceinline__ uint64_t gsearch(const uint32_t *key, uint64_t lo, uint64_t hi, uint32_t v,
+                                            uint32_t flip, bool upper) {
+  while (lo < hi) {
+    uint64_t mid = (lo + hi) >> 1;
+    uint32_t k = ord(key[mid], flip);
+    bool go_right = upper ? (k <= v) : (k < v);
+    if (go_right) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) k_smj_bounds(MergeParams p) {
+  uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= p.tiles) return;
+  uint64_t o0 = t * MJ_TILE, o1 = min(p.no, o0 + MJ_TILE);
+  uint32_t kf = ord(p.okey[o0], p.flip), kl = ord(p.okey[o1 - 1], p.flip);
+  p.bounds[2 * t] = gsearch(p.ikey, 0, p.ni, kf, p.flip, false);
+  p.bounds[2 * t + 1] = gsearch(p.ikey, 0, p.ni, kl, p.flip, true);
+}
+
+__global__ void __launch_bounds__(MJ_THREADS) k_smj_merge(MergeParams p) {
+  __shared__ uint32_t s_ik[MJ_INNER_CAP];
+  __shared__ uint32_t s_ip[MJ_INNER_CAP];
+  __shared__ uint32_t s_warp[MJ_WARPS];
+  __shared__ uint32_t s_flags[2 * MJ_WARPS];
+  __shared__ uint64_t s_sum[MJ_WARPS + 1];
+  __shared__ int s_state;
+  __shared__ uint32_t s_tile;
+  __shared__ uint64_t s_prefix;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(p.claim, 1u);
+  __syncthreads();
+  const uint64_t tile = s_tile;
+  const uint64_t o0 = tile * MJ_TILE, o1 = min(p.no, o0 + MJ_TILE);
+  const uint64_t a0 = p.bounds[2 * tile], a1 = p.bounds[2 * tile + 1];
+  const uint64_t range = a1 > a0 ? a1 - a0 : 0;
+  const bool staged = range <= MJ_INNER_CAP;
+  if (staged) {
+    for (uint64_t i = tid; i < range; i += MJ_THREADS) {
+      s_ik[i] = ord(p.ikey[a0 + i], p.flip);
+      s_ip[i] = p.iptr[a0 + i];
+    }
+  }
+  // Blocked arrangement: thread t owns outer rows o0 + 8t .. o0 + 8t + 7.
+  uint32_t lb[MJ_ITEMS], cnt[MJ_ITEMS];
+  uint32_t okey[MJ_ITEMS];
+  const uint64_t r0 = o0 + (uint64_t)tid * MJ_ITEMS;
+#pragma unroll
+  for (int j = 0; j < MJ_ITEMS; ++j) okey[j] = (r0 + j < o1) ? ord(p.okey[r0 + j], p.flip) : 0u;
+  __syncthreads();
+  uint32_t mine = 0;
+#pragma unroll
+  for (int j = 0; j < MJ_ITEMS; ++j) {
+    lb[j] = 0;
+    cnt[j] = 0;
+    if (r0 + j >= o1 || range == 0) continue;
+    uint64_t l, u;
+    if (staged) {
+      uint32_t lo = 0, hi = (uint32_t)range;
+      while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (s_ik[m] < okey[j]) lo = m + 1; else hi = m; }
+      l = lo;
+      hi = (uint32_t)range;
+      while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (s_ik[m] <= okey[j]) lo = m + 1; else hi = m; }
+      u = lo;
+    } else {
+      l = gsearch(p.ikey, a0, a1, okey[j], p.flip, false) - a0;
+      u = gsearch(p.ikey, a0 + l, a1, okey[j], p.flip, true) - a0;
+    }
+    lb[j] = (uint32_t)l;
+    cnt[j] = (uint32_t)(u - l);
+    mine += cnt[j];
+  }
+  // Block exclusive scan of the per-thread match counts.
+  uint32_t inc = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  uint32_t wpre = 0, total = 0;
+#pragma unroll
+  for (int w = 0; w < MJ_WARPS; ++w) {
+    uint32_t x = s_warp[w];
+    if (w < warp) wpre += x;
+    total += x;
+  }
+  const uint32_t excl = wpre + inc - mine;
+
+  if (tile == 0) {
+    if (tid == 0) {
+      pd_store_relaxed_u64(p.status, pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, total));
+      s_prefix = 0;
+    }
+  } else {
+    if (tid == 0)
+      pd_store_relaxed_u64(p.status + tile, pd_pack_status(p.epoch, PD_FLAG_AGGREGATE, total));
+    uint64_t pre = pd_block_lookback<MJ_THREADS>(p.status, (int64_t)tile, p.epoch, p.d_error,
+                                                 s_flags, s_sum, &s_state);
+    if (tid == 0) {
+      pd_store_relaxed_u64(p.status + tile, pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, pre + total));
+      s_prefix = pre;
+    }
+  }
+  __syncthreads();
+  const uint64_t base = s_prefix;
+  if (tile == p.tiles - 1 && tid == 0) *p.d_count = base + total;
+
+  // Emit (outer payload, inner payload) pairs.
+  uint64_t w = base + excl;
+  bool overflow = false;
+#pragma unroll
+  for (int j = 0; j < MJ_ITEMS; ++j) {
+    if (!cnt[j]) continue;
+    const uint32_t op = p.optr[r0 + j];
+    for (uint32_t m = 0; m < cnt[j]; ++m, ++w) {
+      if (w >= p.cap) { overflow = true; continue; }
+      const uint32_t ip = staged ? s_ip[lb[j] + m] : p.iptr[a0 + lb[j] + m];
+      p.out_outer[w] = op;
+      p.out_inner[w] = ip;
+    }
+  }
+  if (overflow) atomicOr(p.d_error, PD_DEVERR_CAPACITY);
+}
+
+int launch_merge(pimdal_ctx *ctx, MergeParams &p, cudaStream_t s) {
+  p.tiles = pd_ceil_div(p.no, MJ_TILE);
+  if (p.tiles > PD_STATUS_WORDS) return PIMDAL_ERR_ARG;
+  int st;
+  p.epoch = pd_next_epoch(ctx, s, &st);
+  if (st) return st;
+  p.status = ctx->d_status;
+  p.d_error = ctx->d_error;
+  PD_CHECK_CUDA(cudaMemsetAsync(p.claim, 0, sizeof(uint32_t), s));
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_smj_bounds<<<(unsigned)pd_ceil_div(p.tiles, 256), 256, 0, s>>>(p);
+  }
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_SMJ_MERGE, s);
+    k_smj_merge<<<(unsigned)p.tiles, MJ_THREADS, 0, s>>>(p);
+  }
+  return pd_launch_status(ctx);
+}
+
+size_t merge_ws_bytes(uint64_t no) {
+  return 256 + pd_align_up(sizeof(uint64_t) * 2 * pd_ceil_div(no ? no : 1, MJ_TILE), 256);
+}
+
+}  // namespace
+
+extern "C" int pimdal_smj_merge_workspace_size(const pimdal_smj_merge_arguments_t *a, size_t *bytes) {
+  if (!a || !bytes) return PIMDAL_ERR_ARG;
+  *bytes = merge_ws_bytes(a->size_outer);
+  return PIMDAL_OK;
+}
+
+extern "C" int pimdal_smj_merge(pimdal_ctx_t *ctx, const pimdal_smj_merge_arguments_t *a,
+                                pimdal_merge_results_t *d_result, pimdal_stream_t stream) {
+  if (!ctx || !a || !d_result) return PIMDAL_ERR_ARG;
+  if (a->key_dtype != PIMDAL_I32 && a->key_dtype != PIMDAL_U32) return PIMDAL_ERR_ARG;
+  if ((a->size_inner && (!a->inner || !a->inner_ptr)) || (a->size_outer && (!a->outer || !a->outer_ptr)))
+    return PIMDAL_ERR_ARG;
+  if (a->out_capacity && (!a->out_outer || !a->out_inner)) return PIMDAL_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaSetDevice(ctx->device);
+  if (a->size_inner == 0 || a->size_outer == 0) {
+    PD_CHECK_CUDA(cudaMemsetAsync(d_result, 0, sizeof(uint64_t), s));
+    return PIMDAL_OK;
+  }
+  int st;
+  char *ws = (char *)pd_workspace(ctx, merge_ws_bytes(a->size_outer), s, &st);
+  if (!ws) return st;
+  MergeParams p{};
+  p.ikey = (const uint32_t *)a->inner;
+  p.iptr = a->inner_ptr;
+  p.okey = (const uint32_t *)a->outer;
+  p.optr = a->outer_ptr;
+  p.ni = a->size_inner;
+  p.no = a->size_outer;
+  p.out_outer = a->out_outer;
+  p.out_inner = a->out_inner;
+  p.cap = a->out_capacity;
+  p.flip = a->key_dtype == PIMDAL_I32 ? 0x80000000u : 0u;
+  p.claim = (uint32_t *)ws;
+  p.bounds = (uint64_t *)(ws + 256);
+  p.d_count = &d_result->t_count;
+  return launch_merge(ctx, p, s);
+}
+
+// ---------------------------------------------------------------------------
+// Full sort-merge join: stable sort of both relations, then the merge.
+// Workspace: sorted inner (keys, payloads), sorted outer, one sort workspace
+// (reused by both sorts), merge workspace.
+// ---------------------------------------------------------------------------
+namespace {
+struct SmjLayout {
+  size_t ik, ip, ok, op, sort_ws, merge_ws, total;
+};
+bool smj_layout(const pimdal_smj_arguments_t *a, SmjLayout *l) {
+  pimdal_sort_arguments_t si{}, so{};
+  si.nr_elements = a->size_inner;
+  so.nr_elements = a->size_outer;
+  size_t wi = 0, wo = 0;
+  if (pimdal_sort_workspace_size(&si, &wi) || pimdal_sort_workspace_size(&so, &wo)) return false;
+  size_t o = 0;
+  l->ik = o; o += pd_align_up(4 * a->size_inner, 256);
+  l->ip = o; o += pd_align_up(4 * a->size_inner, 256);
+  l->ok = o; o += pd_align_up(4 * a->size_outer, 256);
+  l->op = o; o += pd_align_up(4 * a->size_outer, 256);
+  l->merge_ws = o; o += merge_ws_bytes(a->size_outer);
+  l->sort_ws = o; o += std::max(wi, wo);
+  l->total = o;
+  return true;
+}
+}  // namespace
+
+extern "C" int pimdal_sort_merge_join_workspace_size(const pimdal_smj_arguments_t *a, size_t *bytes) {
+  if (!a || !bytes) return PIMDAL_ERR_ARG;
+  SmjLayout l;
+  if (!smj_layout(a, &l)) return PIMDAL_ERR_ARG;
+  *bytes = l.total;
+  return PIMDAL_OK;
+}
+
+extern "C" int pimdal_sort_merge_join(pimdal_ctx_t *ctx, const pimdal_smj_arguments_t *a,
+                                      pimdal_merge_results_t *d_result, pimdal_stream_t stream) {
+  if (!ctx || !a || !d_result) return PIMDAL_ERR_ARG;
+  if (a->key_dtype != PIMDAL_I32 && a->key_dtype != PIMDAL_U32) return PIMDAL_ERR_ARG;
+  if ((a->size_inner && !a->inner_key) || (a->size_outer && !a->outer_key)) return PIMDAL_ERR_ARG;
+  if (a->out_capacity && (!a->out_inner_payload || !a->out_outer_payload)) return PIMDAL_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaSetDevice(ctx->device);
+  if (a->size_inner == 0 || a->size_outer == 0) {
+    PD_CHECK_CUDA(cudaMemsetAsync(d_result, 0, sizeof(uint64_t), s));
+    return PIMDAL_OK;
+  }
+  SmjLayout l;
+  if (!smj_layout(a, &l)) return PIMDAL_ERR_ARG;
+  int st;
+  char *ws = (char *)pd_workspace(ctx, l.total, s, &st);
+  if (!ws) return st;
+  pimdal_sort_arguments_t sa{};
+  sa.key_dtype = a->key_dtype;
+  sa.layout = PIMDAL_LAYOUT_COLUMNS;
+  // inner
+  sa.nr_elements = a->size_inner;
+  sa.in = a->inner_key;
+  sa.in_ptr = a->inner_payload;
+  sa.out = ws + l.ik;
+  sa.out_ptr = (uint32_t *)(ws + l.ip);
+  if ((st = pd_sort_with_workspace(ctx, &sa, ws + l.sort_ws, s))) return st;
+  // outer
+  sa.nr_elements = a->size_outer;
+  sa.in = a->outer_key;
+  sa.in_ptr = a->outer_payload;
+  sa.out = ws + l.ok;
+  sa.out_ptr = (uint32_t *)(ws + l.op);
+  if ((st = pd_sort_with_workspace(ctx, &sa, ws + l.sort_ws, s))) return st;
+  MergeParams p{};
+  p.ikey = (const uint32_t *)(ws + l.ik);
+  p.iptr = (const uint32_t *)(ws + l.ip);
+  p.okey = (const uint32_t *)(ws + l.ok);
+  p.optr = (const uint32_t *)(ws + l.op);
+  p.ni = a->size_inner;
+  p.no = a->size_outer;
+  p.out_outer = a->out_outer_payload;
+  p.out_inner = a->out_inner_payload;
+  p.cap = a->out_capacity;
+  p.flip = a->key_dtype == PIMDAL_I32 ? 0x80000000u : 0u;
+  p.claim = (uint32_t *)(ws + l.merge_ws);
+  p.bounds = (uint64_t *)(ws + l.merge_ws + 256);
+  p.d_count = &d_result->t_count;
+  return launch_merge(ctx, p, s);
+}

@@ -1,0 +1,451 @@
+// K-SORT: stable onesweep LSD radix sort of (uint32/int32 key, uint32 row id)
+// (pimdal_sort_kernel).
+//
+// Reference behaviour: sort_kernel / sort_part_kernel (pimdal/sort/sort.h:7-25,
+// sort_keyval.c:37-179) range-partition key_ptr pairs and quicksort each
+// bucket (not stable); the CPU operator reference/db_operators/sort.cpp:30-40
+// sorts one key column ascending.  This operator returns the stable
+// ascending order of (key, row id) pairs, row ids fused in from the index
+// when no row-id column is given (the create_ptr glue of
+// pimdal/main/sort/dpu/kernel_sort.c).
+//
+// B200 design (HBM-bound, no tensor cores):
+//  1. k_sort_hist: one read of the keys builds the 256-bin histograms of all
+//     digit positions (warp-private shared-memory counters).
+//  2. k_sort_plan (one CTA): exclusive scans of the histograms; a pass whose
+//     digit is the same for every key (count == n) is skipped; buffers are
+//     routed so the last active pass writes the caller's output.  Computed on
+//     the device, so the whole sort is stream-ordered and capturable.
+//  3. k_sort_pass, once per digit: a CTA takes the next 4096-key tile (atomic
+//     tile counter, so tiles are processed in input order), ranks keys per
+//     warp with match.any, publishes per-digit tile counts and resolves their
+//     global offsets with a per-digit decoupled look-back, stages the tile in
+//     shared memory in digit order and writes each digit run contiguously.
+#include "common.cuh"
+
+namespace {
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_WARPS = RS_THREADS / 32;
+constexpr int RS_ITEMS = 16;
+constexpr int RS_WARP_TILE = 32 * RS_ITEMS;        // 512
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;     // 4096
+constexpr int RS_RADIX_BITS = 8;
+constexpr int RS_RADIX = 1 << RS_RADIX_BITS;       // 256 (== RS_THREADS)
+constexpr int RS_MAX_PASSES = 4;
+constexpr uint32_t RS_FLAG_AGG = 1u << 30, RS_FLAG_INC = 2u << 30, RS_COUNT_MASK = (1u << 30) - 1;
+static_assert(RS_RADIX == RS_THREADS, "one thread per digit");
+
+enum : uint32_t { BUF_IN = 0, BUF_OUT = 1, BUF_ALT = 2 };
+
+struct SortPlan {
+  uint32_t active[RS_MAX_PASSES];
+  uint32_t src[RS_MAX_PASSES];
+  uint32_t dst[RS_MAX_PASSES];
+  uint32_t first[RS_MAX_PASSES];  // first active pass (reads the input row ids)
+  uint32_t n_active;
+};
+
+struct SortParams {
+  const void *in;
+  const uint32_t *in_ptr;  // NULL: row id = ptr_base + index
+  uint64_t ptr_base;
+  void *out;
+  uint32_t *out_ptr;
+  uint32_t *alt_key, *alt_ptr;
+  uint64_t n;
+  uint32_t flip;        // 0x80000000 for signed keys
+  uint32_t begin_bit, end_bit, npasses;
+  int pairs;            // in/out are key_ptr32 arrays
+  int has_vals;
+  uint32_t *hist;       // [RS_MAX_PASSES][RS_RADIX]
+  uint32_t *offsets;    // [RS_MAX_PASSES][RS_RADIX]
+  SortPlan *plan;
+  uint32_t *status;     // [RS_MAX_PASSES][tiles][RS_RADIX]
+  uint32_t *counters;   // [RS_MAX_PASSES]
+  uint64_t tiles;
+  uint32_t *d_error;
+};
+
+__device__ __forceinline__ uint32_t digit_of(uint32_t k, const SortParams &p, uint32_t pass) {
+  uint32_t shift = p.begin_bit + pass * RS_RADIX_BITS;
+  uint32_t bits = min((uint32_t)RS_RADIX_BITS, p.end_bit - shift);
+  return ((k ^ p.flip) >> shift) & ((1u << bits) - 1u);
+}
+
+__device__ __forceinline__ uint32_t load_key_in(const SortParams &p, uint64_t i) {
+  return p.pairs ? reinterpret_cast<const uint2 *>(p.in)[i].x
+                 : reinterpret_cast<const uint32_t *>(p.in)[i];
+}
+
+// ---------------------------------------------------------------- histogram
+__global__ void __launch_bounds__(RS_THREADS) k_sort_hist(SortParams p) {
+  __shared__ uint32_t sh[RS_WARPS][RS_MAX_PASSES][RS_RADIX];
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int i = tid; i < RS_WARPS * RS_MAX_PASSES * RS_RADIX; i += RS_THREADS)
+    (&sh[0][0][0])[i] = 0;
+  __syncthreads();
+  const uint64_t stride = (uint64_t)gridDim.x * RS_THREADS;
+  const bool vec = !p.pairs && ((uintptr_t)p.in & 15u) == 0;
+  if (vec) {
+    const uint4 *in4 = reinterpret_cast<const uint4 *>(p.in);
+    const uint64_t n4 = p.n / 4;
+    for (uint64_t i = (uint64_t)blockIdx.x * RS_THREADS + tid; i < n4; i += stride) {
+      uint4 v = __ldcs(in4 + i);
+      uint32_t k[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+        for (uint32_t q = 0; q < p.npasses; ++q) atomicAdd(&sh[warp][q][digit_of(k[j], p, q)], 1u);
+    }
+    for (uint64_t i = n4 * 4 + (uint64_t)blockIdx.x * RS_THREADS + tid; i < p.n; i += stride) {
+      uint32_t k = load_key_in(p, i);
+      for (uint32_t q = 0; q < p.npasses; ++q) atomicAdd(&sh[warp][q][digit_of(k, p, q)], 1u);
+    }
+  } else {
+    for (uint64_t i = (uint64_t)blockIdx.x * RS_THREADS + tid; i < p.n; i += stride) {
+      uint32_t k = load_key_in(p, i);
+      for (uint32_t q = 0; q < p.npasses; ++q) atomicAdd(&sh[warp][q][digit_of(k, p, q)], 1u);
+    }
+  }
+  __syncthreads();
+  for (uint32_t q = 0; q < p.npasses; ++q) {
+    uint32_t s = 0;
+#pragma unroll
+    for (int w = 0; w < RS_WARPS; ++w) s += sh[w][q][tid];
+    if (s) atomicAdd(&p.hist[q * RS_RADIX + tid], s);
+  }
+}
+
+// Block-wide exclusive scan of one value per thread (RS_THREADS threads).
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t *s_warp,
+                                                         uint32_t *total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  if (lane == 31) s_warp[warp] = inc;
+  __syncthreads();
+  uint32_t wpre = 0, tot = 0;
+#pragma unroll
+  for (int w = 0; w < RS_WARPS; ++w) {
+    uint32_t x = s_warp[w];
+    if (w < warp) wpre += x;
+    tot += x;
+  }
+  __syncthreads();
+  if (total) *total = tot;
+  return wpre + inc - v;
+}
+
+// -------------------------------------------------------------------- plan
+__global__ void __launch_bounds__(RS_THREADS) k_sort_plan(SortParams p) {
+  __shared__ uint32_t s_warp[RS_WARPS];
+  __shared__ uint32_t s_trivial[RS_MAX_PASSES];
+  const int d = threadIdx.x;
+  if (d < RS_MAX_PASSES) s_trivial[d] = 0;
+  __syncthreads();
+  for (uint32_t q = 0; q < p.npasses; ++q) {
+    uint32_t c = p.hist[q * RS_RADIX + d];
+    if ((uint64_t)c == p.n) s_trivial[q] = 1;
+    p.offsets[q * RS_RADIX + d] = block_exclusive_scan(c, s_warp, nullptr);
+  }
+  __syncthreads();
+  if (d == 0) {
+    SortPlan pl{};
+    uint32_t m = 0;
+    for (uint32_t q = 0; q < p.npasses; ++q) {
+      pl.active[q] = !s_trivial[q];
+      m += pl.active[q];
+    }
+    pl.n_active = m;
+    uint32_t j = 0, prev = BUF_IN;
+    for (uint32_t q = 0; q < p.npasses; ++q) {
+      if (!pl.active[q]) continue;
+      ++j;
+      pl.src[q] = prev;
+      pl.dst[q] = ((m - j) % 2 == 0) ? BUF_OUT : BUF_ALT;
+      pl.first[q] = (j == 1);
+      prev = pl.dst[q];
+    }
+    *p.plan = pl;
+  }
+}
+
+// No active pass (all keys share every digit, or n small): copy in -> out.
+__global__ void __launch_bounds__(RS_THREADS) k_sort_copy(SortParams p) {
+  if (p.plan->n_active != 0) return;
+  const uint64_t stride = (uint64_t)gridDim.x * RS_THREADS;
+  for (uint64_t i = (uint64_t)blockIdx.x * RS_THREADS + threadIdx.x; i < p.n; i += stride) {
+    uint32_t k, v;
+    if (p.pairs) {
+      uint2 e = reinterpret_cast<const uint2 *>(p.in)[i];
+      k = e.x;
+      v = e.y;
+    } else {
+      k = reinterpret_cast<const uint32_t *>(p.in)[i];
+      v = p.in_ptr ? p.in_ptr[i] : (uint32_t)(p.ptr_base + i);
+    }
+    if (p.pairs) reinterpret_cast<uint2 *>(p.out)[i] = make_uint2(k, v);
+    else {
+      reinterpret_cast<uint32_t *>(p.out)[i] = k;
+      if (p.has_vals) p.out_ptr[i] = v;
+    }
+  }
+}
+
+// ------------------------------------------------------------ onesweep pass
+template <bool HAS_VALS>
+__global__ void __launch_bounds__(RS_THREADS, 3) k_sort_pass(SortParams p, uint32_t pass) {
+  __shared__ uint32_t s_keys[RS_TILE];
+  __shared__ uint32_t s_vals[HAS_VALS ? RS_TILE : 1];
+  __shared__ uint32_t s_whist[RS_WARPS][RS_RADIX];
+  __shared__ uint32_t s_dstart[RS_RADIX];
+  __shared__ long long s_gdelta[RS_RADIX];
+  __shared__ uint32_t s_warp[RS_WARPS];
+  __shared__ uint32_t s_tile;
+
+  const SortPlan *plan = p.plan;
+  if (!plan->active[pass]) return;
+  const uint32_t src = plan->src[pass], dst = plan->dst[pass];
+  const bool first = plan->first[pass] != 0;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_tile = atomicAdd(&p.counters[pass], 1u);
+#pragma unroll
+  for (int w = 0; w < RS_WARPS; ++w) s_whist[w][tid] = 0;
+  __syncthreads();
+  const uint64_t tile = s_tile;
+  const uint64_t base = tile * (uint64_t)RS_TILE;
+  const uint64_t wbase = base + (uint64_t)warp * RS_WARP_TILE;
+
+  // Source / destination views.  ALT is always structure-of-arrays.
+  const bool src_pairs = (src != BUF_ALT) && p.pairs;
+  const bool dst_pairs = (dst != BUF_ALT) && p.pairs;
+  const void *skey = src == BUF_IN ? p.in : (src == BUF_OUT ? p.out : (const void *)p.alt_key);
+  const uint32_t *sval = src == BUF_IN ? p.in_ptr : (src == BUF_OUT ? p.out_ptr : p.alt_ptr);
+  void *dkey = dst == BUF_OUT ? p.out : (void *)p.alt_key;
+  uint32_t *dval = dst == BUF_OUT ? p.out_ptr : p.alt_ptr;
+
+  // Load keys and values up front (all loads in flight together):
+  // warp-striped, item k of lane l is element wbase + 32k + l.
+  uint32_t key[RS_ITEMS];
+  uint32_t val[HAS_VALS ? RS_ITEMS : 1];
+  const bool gen_vals = first && src == BUF_IN && sval == nullptr && !src_pairs;
+#pragma unroll
+  for (int k = 0; k < RS_ITEMS; ++k) {
+    uint64_t i = wbase + (uint64_t)k * 32 + lane;
+    key[k] = 0;
+    if (HAS_VALS) val[k] = 0;
+    if (i < p.n) {
+      if (src_pairs) {
+        uint2 e = __ldcs(reinterpret_cast<const uint2 *>(skey) + i);
+        key[k] = e.x;
+        if (HAS_VALS) val[k] = e.y;
+      } else {
+        key[k] = __ldcs(reinterpret_cast<const uint32_t *>(skey) + i);
+        if (HAS_VALS) val[k] = gen_vals ? (uint32_t)(p.ptr_base + i) : __ldcs(sval + i);
+      }
+    }
+  }
+
+  // Warp-level stable ranking.
+  uint32_t rank[RS_ITEMS];
+  const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int k = 0; k < RS_ITEMS; ++k) {
+    uint64_t i = wbase + (uint64_t)k * 32 + lane;
+    const bool valid = i < p.n;
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+    rank[k] = 0;
+    if (valid) {
+      uint32_t d = digit_of(key[k], p, pass);
+      unsigned peers = __match_any_sync(vmask, d);
+      int leader = __ffs(peers) - 1;
+      uint32_t old = 0;
+      if (lane == leader) {
+        old = s_whist[warp][d];
+        s_whist[warp][d] = old + __popc(peers);
+      }
+      old = __shfl_sync(vmask, old, leader);
+      rank[k] = old + __popc(peers & lt);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // Per digit (thread tid = digit): warp offsets, tile count, publish, look-back.
+  const int d = tid;
+  uint32_t run = 0;
+#pragma unroll
+  for (int w = 0; w < RS_WARPS; ++w) {
+    uint32_t t = s_whist[w][d];
+    s_whist[w][d] = run;
+    run += t;
+  }
+  const uint32_t count = run;
+  uint32_t *st = p.status + ((uint64_t)pass * p.tiles) * RS_RADIX + d;
+  if (tile == 0) pd_store_release_u32(st, RS_FLAG_INC | count);
+  else pd_store_release_u32(st + tile * RS_RADIX, RS_FLAG_AGG | count);
+  const uint32_t dstart = block_exclusive_scan(count, s_warp, nullptr);
+  s_dstart[d] = dstart;
+
+  uint64_t excl = 0;
+  if (tile > 0) {
+    int64_t t = (int64_t)tile - 1;
+    uint32_t spins = 0;
+    const uint64_t t0 = pd_globaltimer_ns();
+    while (t >= 0) {
+      uint32_t w = pd_load_acquire_u32(st + (uint64_t)t * RS_RADIX);
+      uint32_t flag = w & ~RS_COUNT_MASK;
+      if (flag == 0) {
+        if (pd_wait_expired(p.d_error, t0, ++spins)) break;
+        __nanosleep(32);
+        continue;
+      }
+      excl += w & RS_COUNT_MASK;
+      if (flag == RS_FLAG_INC) break;
+      --t;
+    }
+    pd_store_release_u32(st + tile * RS_RADIX, RS_FLAG_INC | (uint32_t)((excl + count) & RS_COUNT_MASK));
+  }
+  s_gdelta[d] = (long long)(p.offsets[pass * RS_RADIX + d] + excl) - (long long)dstart;
+  __syncthreads();
+
+  // Stage the tile in digit order.
+#pragma unroll
+  for (int k = 0; k < RS_ITEMS; ++k) {
+    uint64_t i = wbase + (uint64_t)k * 32 + lane;
+    if (i < p.n) {
+      uint32_t dg = digit_of(key[k], p, pass);
+      uint32_t pos = s_dstart[dg] + s_whist[warp][dg] + rank[k];
+      s_keys[pos] = key[k];
+      if (HAS_VALS) s_vals[pos] = val[k];
+    }
+  }
+  __syncthreads();
+
+  // Write each digit run contiguously.
+  const uint32_t tile_n = (uint32_t)min((uint64_t)RS_TILE, p.n - base);
+  for (uint32_t i = tid; i < tile_n; i += RS_THREADS) {
+    uint32_t k = s_keys[i];
+    uint64_t g = (uint64_t)(s_gdelta[digit_of(k, p, pass)] + (long long)i);
+    if (dst_pairs) {
+      reinterpret_cast<uint2 *>(dkey)[g] = make_uint2(k, HAS_VALS ? s_vals[i] : 0u);
+    } else {
+      reinterpret_cast<uint32_t *>(dkey)[g] = k;
+      if (HAS_VALS) dval[g] = s_vals[i];
+    }
+  }
+}
+
+struct SortLayout {
+  size_t off_counters, off_hist, off_offsets, off_plan, off_status, off_alt_key, off_alt_ptr,
+      total, memset_bytes;
+  uint64_t tiles;
+  uint32_t npasses;
+};
+
+bool sort_layout(const pimdal_sort_arguments_t *a, SortLayout *l) {
+  uint32_t b = a->begin_bit, e = a->end_bit ? a->end_bit : 32;
+  if (b >= e || e > 32) return false;
+  l->npasses = (e - b + RS_RADIX_BITS - 1) / RS_RADIX_BITS;
+  l->tiles = pd_ceil_div(a->nr_elements ? a->nr_elements : 1, RS_TILE);
+  size_t o = 0;
+  l->off_counters = o; o += 256;
+  l->off_hist = o; o += sizeof(uint32_t) * RS_MAX_PASSES * RS_RADIX;
+  l->off_status = o; o += pd_align_up(sizeof(uint32_t) * RS_MAX_PASSES * l->tiles * RS_RADIX, 256);
+  l->memset_bytes = o;
+  l->off_offsets = o; o += sizeof(uint32_t) * RS_MAX_PASSES * RS_RADIX;
+  l->off_plan = o; o += 256;
+  l->off_alt_key = o; o += pd_align_up(sizeof(uint32_t) * a->nr_elements, 256);
+  l->off_alt_ptr = o; o += pd_align_up(sizeof(uint32_t) * a->nr_elements, 256);
+  l->total = o;
+  return true;
+}
+
+}  // namespace
+
+extern "C" int pimdal_sort_workspace_size(const pimdal_sort_arguments_t *a, size_t *bytes) {
+  if (!a || !bytes) return PIMDAL_ERR_ARG;
+  SortLayout l;
+  if (!sort_layout(a, &l)) return PIMDAL_ERR_ARG;
+  *bytes = l.total;
+  return PIMDAL_OK;
+}
+
+// Stream-ordered sort with a given workspace (used by the operators that
+// sort internally, e.g. the sort-merge join and the sort group-by).
+int pd_sort_with_workspace(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, void *ws,
+                           cudaStream_t s) {
+  SortLayout l;
+  if (!sort_layout(a, &l)) return PIMDAL_ERR_ARG;
+  if (a->nr_elements > RS_COUNT_MASK) return PIMDAL_ERR_ARG;  // < 2^30 elements
+  char *w = (char *)ws;
+  SortParams p{};
+  p.in = a->in;
+  p.in_ptr = a->layout == PIMDAL_LAYOUT_COLUMNS ? a->in_ptr : nullptr;
+  p.ptr_base = a->ptr_base;
+  p.out = a->out;
+  p.out_ptr = a->layout == PIMDAL_LAYOUT_COLUMNS ? a->out_ptr : nullptr;
+  p.pairs = a->layout == PIMDAL_LAYOUT_PAIRS;
+  p.has_vals = p.pairs || p.out_ptr != nullptr;
+  p.alt_key = (uint32_t *)(w + l.off_alt_key);
+  p.alt_ptr = (uint32_t *)(w + l.off_alt_ptr);
+  p.n = a->nr_elements;
+  p.flip = a->key_dtype == PIMDAL_I32 ? 0x80000000u : 0u;
+  p.begin_bit = a->begin_bit;
+  p.end_bit = a->end_bit ? a->end_bit : 32;
+  p.npasses = l.npasses;
+  p.hist = (uint32_t *)(w + l.off_hist);
+  p.offsets = (uint32_t *)(w + l.off_offsets);
+  p.plan = (SortPlan *)(w + l.off_plan);
+  p.status = (uint32_t *)(w + l.off_status);
+  p.counters = (uint32_t *)(w + l.off_counters);
+  p.tiles = l.tiles;
+  p.d_error = ctx->d_error;
+
+  PD_CHECK_CUDA(cudaMemsetAsync(w, 0, l.memset_bytes, s));
+  const unsigned hist_blocks =
+      (unsigned)std::min<uint64_t>(pd_ceil_div(p.n, (uint64_t)RS_THREADS * 16), (uint64_t)ctx->sm_count * 4);
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_SORT_HIST, s);
+    k_sort_hist<<<hist_blocks ? hist_blocks : 1, RS_THREADS, 0, s>>>(p);
+  }
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_sort_plan<<<1, RS_THREADS, 0, s>>>(p);
+  }
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    unsigned cb = (unsigned)std::min<uint64_t>(pd_ceil_div(p.n, RS_THREADS), (uint64_t)ctx->sm_count * 8);
+    k_sort_copy<<<cb ? cb : 1, RS_THREADS, 0, s>>>(p);
+  }
+  for (uint32_t q = 0; q < l.npasses; ++q) {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_SORT_PASS, s);
+    if (p.has_vals) k_sort_pass<true><<<(unsigned)l.tiles, RS_THREADS, 0, s>>>(p, q);
+    else k_sort_pass<false><<<(unsigned)l.tiles, RS_THREADS, 0, s>>>(p, q);
+  }
+  return pd_launch_status(ctx);
+}
+
+extern "C" int pimdal_sort_kernel(pimdal_ctx_t *ctx, const pimdal_sort_arguments_t *a,
+                                  pimdal_stream_t stream) {
+  if (!ctx || !a) return PIMDAL_ERR_ARG;
+  if (a->layout != PIMDAL_LAYOUT_COLUMNS && a->layout != PIMDAL_LAYOUT_PAIRS) return PIMDAL_ERR_ARG;
+  if (a->key_dtype != PIMDAL_I32 && a->key_dtype != PIMDAL_U32) return PIMDAL_ERR_ARG;
+  if (a->nr_elements == 0) return PIMDAL_OK;
+  if (!a->in || !a->out || a->in == a->out) return PIMDAL_ERR_ARG;
+  if (a->layout == PIMDAL_LAYOUT_COLUMNS && a->out_ptr && a->in_ptr == a->out_ptr)
+    return PIMDAL_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaSetDevice(ctx->device);
+  size_t need;
+  int st = pimdal_sort_workspace_size(a, &need);
+  if (st) return st;
+  void *ws = pd_workspace(ctx, need, s, &st);
+  if (!ws) return st;
+  return pd_sort_with_workspace(ctx, a, ws, s);
+}

@@ -134,3 +134,83 @@ def sel_kernel(ctx: Context, keys: torch.Tensor, pred: L.Pred, *, in_ptr=None, p
     L.check(ctx.lib.pimdal_sel_kernel(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
             "pimdal_sel_kernel")
     return result, out, out_ptr
+
+
+# ---------------------------------------------------------------------------
+# Sort (sort_kernel, pimdal/sort/sort.h:25)
+# ---------------------------------------------------------------------------
+def _workspace(ctx: Context, fn, args) -> None:
+    sz = C.c_size_t()
+    L.check(fn(C.byref(args), C.byref(sz)), fn.__name__)
+    ctx.reserve(sz.value)
+
+
+def sort_kernel(ctx: Context, keys: torch.Tensor, ptr: torch.Tensor | None = None, *,
+                ptr_base: int = 0, key_dtype: int = L.U32, layout: int = L.LAYOUT_COLUMNS,
+                out=None, out_ptr=None, want_ptr: bool = True, begin_bit: int = 0,
+                end_bit: int = 32, stream=None):
+    """Stable ascending sort of (key, row id).  keys: int32 tensor (or int64
+    view of key_ptr32 pairs with layout=PAIRS).  Returns (out, out_ptr)."""
+    n = keys.numel()
+    if out is None:
+        out = torch.empty_like(keys)
+    if layout == L.LAYOUT_COLUMNS and want_ptr and out_ptr is None:
+        out_ptr = torch.empty(n, dtype=torch.int32, device=keys.device)
+    a = L.SortArguments(nr_elements=n, in_=_ptr(keys), in_ptr=_ptr(ptr), ptr_base=ptr_base,
+                        out=_ptr(out), out_ptr=_ptr(out_ptr), key_dtype=key_dtype, layout=layout,
+                        begin_bit=begin_bit, end_bit=end_bit)
+    _workspace(ctx, ctx.lib.pimdal_sort_workspace_size, a)
+    L.check(ctx.lib.pimdal_sort_kernel(ctx.handle, C.byref(a), _stream(stream)),
+            "pimdal_sort_kernel")
+    return out, out_ptr
+
+
+# ---------------------------------------------------------------------------
+# Sort-merge join (merge_kernel, pimdal/join/sort_merge.h:23)
+# ---------------------------------------------------------------------------
+def smj_merge(ctx: Context, inner, inner_ptr, outer, outer_ptr, *, key_dtype: int = L.I32,
+              capacity: int | None = None, out_outer=None, out_inner=None, result=None,
+              stream=None):
+    """Merge of key-sorted relations.  Returns (result, out_outer, out_inner)."""
+    dev = outer.device
+    if capacity is None:
+        capacity = max(outer.numel(), 1)
+    if out_outer is None:
+        out_outer = torch.empty(capacity, dtype=torch.int32, device=dev)
+    if out_inner is None:
+        out_inner = torch.empty(capacity, dtype=torch.int32, device=dev)
+    if result is None:
+        result = torch.empty(1, dtype=torch.int64, device=dev)
+    a = L.SmjMergeArguments(inner=_ptr(inner), inner_ptr=_ptr(inner_ptr), size_inner=inner.numel(),
+                            outer=_ptr(outer), outer_ptr=_ptr(outer_ptr), size_outer=outer.numel(),
+                            out_outer=_ptr(out_outer), out_inner=_ptr(out_inner),
+                            out_capacity=capacity, key_dtype=key_dtype)
+    _workspace(ctx, ctx.lib.pimdal_smj_merge_workspace_size, a)
+    L.check(ctx.lib.pimdal_smj_merge(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
+            "pimdal_smj_merge")
+    return result, out_outer, out_inner
+
+
+def sort_merge_join(ctx: Context, inner_key, inner_payload, outer_key, outer_payload, *,
+                    key_dtype: int = L.I32, capacity: int | None = None, out_inner=None,
+                    out_outer=None, result=None, stream=None):
+    """Sorts both relations and merges them.  Returns (result, inner payloads,
+    outer payloads) of the matches, outer-major."""
+    dev = outer_key.device
+    if capacity is None:
+        capacity = max(outer_key.numel(), 1)
+    if out_inner is None:
+        out_inner = torch.empty(capacity, dtype=torch.int32, device=dev)
+    if out_outer is None:
+        out_outer = torch.empty(capacity, dtype=torch.int32, device=dev)
+    if result is None:
+        result = torch.empty(1, dtype=torch.int64, device=dev)
+    a = L.SmjArguments(inner_key=_ptr(inner_key), inner_payload=_ptr(inner_payload),
+                       size_inner=inner_key.numel(), outer_key=_ptr(outer_key),
+                       outer_payload=_ptr(outer_payload), size_outer=outer_key.numel(),
+                       out_inner_payload=_ptr(out_inner), out_outer_payload=_ptr(out_outer),
+                       out_capacity=capacity, key_dtype=key_dtype)
+    _workspace(ctx, ctx.lib.pimdal_sort_merge_join_workspace_size, a)
+    L.check(ctx.lib.pimdal_sort_merge_join(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
+            "pimdal_sort_merge_join")
+    return result, out_inner, out_outer
