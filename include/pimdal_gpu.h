@@ -274,6 +274,91 @@ int pimdal_sort_merge_join_workspace_size(const pimdal_smj_arguments_t *args, si
 int pimdal_sort_merge_join(pimdal_ctx_t *ctx, const pimdal_smj_arguments_t *args,
                            pimdal_merge_results_t *d_result, pimdal_stream_t stream);
 
+/* ------------------------------------------------------------------------- */
+/* Radix partition.  Replaces part_kernel (pimdal/join/hash_join.h:23-31,    */
+/* hash_join.c:154-235): element e goes to partition                         */
+/* (hash0(e.key) >> (shift - log2(part_n))) & (part_n - 1), hash0 being the  */
+/* reference's pimdal/hash/hash_func.h:5-14.  Stable.  part_sizes[p] is the  */
+/* first row of partition p, part_sizes[part_n] = size (uint64, device).     */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+  const void *in;           /* part_arguments_t.in_ptr: uint32 key column      */
+  const uint32_t *in_ptr;   /* row ids; NULL = index                           */
+  uint64_t size;            /* part_arguments_t.size                           */
+  uint32_t shift;           /* part_arguments_t.shift (<= 32)                  */
+  uint32_t part_n;          /* part_arguments_t.part_n: power of 2, <= 65536   */
+  void *part_out;           /* part_arguments_t.part_ptr: partitioned keys     */
+  uint32_t *part_out_ptr;   /* partitioned row ids (may be NULL)               */
+  uint64_t *part_sizes;     /* part_arguments_t.part_sizes: part_n + 1 entries */
+  int32_t layout;           /* PIMDAL_LAYOUT_COLUMNS                           */
+  int32_t pad;
+} pimdal_part_arguments_t;
+
+int pimdal_part_workspace_size(const pimdal_part_arguments_t *args, size_t *bytes);
+int pimdal_part_kernel(pimdal_ctx_t *ctx, const pimdal_part_arguments_t *args,
+                       pimdal_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
+/* Hash tables.  pimdal_hash_kernel replaces hash_kernel                      */
+/* (pimdal/join/hash_join.h:6-13, hash_join.c:40-115): a linear-probing       */
+/* table of table_size 64-bit slots (payload << 32 | key), built with         */
+/* atomicCAS, in caller memory of pimdal_hash_table_bytes(table_size) bytes.  */
+/* pimdal_hj_probe replaces merge_kernel (hash_join.h:44-57,                  */
+/* hash_join.c:343-430): for every probe row and every build row with the     */
+/* same key it emits (probe ptr, build payload), in probe order.              */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+  const void *in_key;       /* hash_arguments_t.in_ptr: build keys (uint32)    */
+  const uint32_t *in_ptr;   /* build payloads / row ids; NULL = index          */
+  uint64_t size;            /* hash_arguments_t.size                           */
+  void *table_ptr;          /* hash_arguments_t.table_ptr                      */
+  uint64_t table_size;      /* hash_arguments_t.table_size: slots, power of 2  */
+} pimdal_hash_arguments_t;
+
+typedef struct {
+  const void *table_ptr;    /* merge_arguments_t.table_ptr (built above)       */
+  uint64_t table_size;      /* merge_arguments_t.size: slots                   */
+  const void *in_key;       /* merge_arguments_t.in_ptr: probe keys            */
+  const uint32_t *in_ptr;   /* probe row ids; NULL = index                     */
+  uint64_t size;            /* probe rows                                      */
+  uint32_t *out_outer;      /* merge_arguments_t.out_ptr: probe ptr per match  */
+  uint32_t *out_inner;      /* ... and build payload per match                 */
+  uint64_t out_capacity;
+} pimdal_probe_arguments_t;
+
+size_t pimdal_hash_table_bytes(uint64_t table_size);
+int pimdal_hash_kernel(pimdal_ctx_t *ctx, const pimdal_hash_arguments_t *args,
+                       pimdal_stream_t stream);
+int pimdal_hj_probe(pimdal_ctx_t *ctx, const pimdal_probe_arguments_t *args,
+                    pimdal_merge_results_t *d_result, pimdal_stream_t stream);
+
+/* Whole hash join (the pipeline of pimdal/main/join/hash and
+ * reference/db_operators/hash_join.cpp:159-219).  A table that fits
+ * l2_budget_bytes is built and probed directly; a larger one is processed
+ * partition by partition (both relations radix-partitioned by hash bits), so
+ * every table being probed is L2-resident.  Output per match: build payload
+ * and probe row id; partitions in order, probe order within a partition
+ * (probe order overall when not partitioned).  With duplicate build keys the
+ * matches of one probe row come in table order. */
+typedef struct {
+  const void *build_key;          /* uint32 / int32 keys                          */
+  const uint32_t *build_payload;  /* NULL = build row id                          */
+  uint64_t size_build;            /* < 2^32                                       */
+  const void *probe_key;
+  const uint32_t *probe_ptr;      /* NULL = probe row id                          */
+  uint64_t size_probe;            /* < 2^30                                       */
+  uint32_t *out_build_payload;
+  uint32_t *out_probe_ptr;
+  uint64_t out_capacity;
+  uint32_t partition_bits;        /* 0 = auto, 0xFFFFFFFF = never partition, else 1..8 */
+  uint32_t load_factor_pct;       /* table load factor in percent; 0 = 50          */
+  uint64_t l2_budget_bytes;       /* 0 = 48 MiB                                   */
+} pimdal_hash_join_arguments_t;
+
+int pimdal_hash_join_workspace_size(const pimdal_hash_join_arguments_t *args, size_t *bytes);
+int pimdal_hash_join(pimdal_ctx_t *ctx, const pimdal_hash_join_arguments_t *args,
+                     pimdal_merge_results_t *d_result, pimdal_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

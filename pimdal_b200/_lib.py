@@ -84,6 +84,40 @@ class SmjArguments(C.Structure):
     ]
 
 
+class PartArguments(C.Structure):
+    _fields_ = [
+        ("in_", C.c_void_p), ("in_ptr", C.c_void_p), ("size", C.c_uint64),
+        ("shift", C.c_uint32), ("part_n", C.c_uint32), ("part_out", C.c_void_p),
+        ("part_out_ptr", C.c_void_p), ("part_sizes", C.c_void_p),
+        ("layout", C.c_int32), ("pad", C.c_int32),
+    ]
+
+
+class HashArguments(C.Structure):
+    _fields_ = [
+        ("in_key", C.c_void_p), ("in_ptr", C.c_void_p), ("size", C.c_uint64),
+        ("table_ptr", C.c_void_p), ("table_size", C.c_uint64),
+    ]
+
+
+class ProbeArguments(C.Structure):
+    _fields_ = [
+        ("table_ptr", C.c_void_p), ("table_size", C.c_uint64), ("in_key", C.c_void_p),
+        ("in_ptr", C.c_void_p), ("size", C.c_uint64), ("out_outer", C.c_void_p),
+        ("out_inner", C.c_void_p), ("out_capacity", C.c_uint64),
+    ]
+
+
+class HashJoinArguments(C.Structure):
+    _fields_ = [
+        ("build_key", C.c_void_p), ("build_payload", C.c_void_p), ("size_build", C.c_uint64),
+        ("probe_key", C.c_void_p), ("probe_ptr", C.c_void_p), ("size_probe", C.c_uint64),
+        ("out_build_payload", C.c_void_p), ("out_probe_ptr", C.c_void_p),
+        ("out_capacity", C.c_uint64), ("partition_bits", C.c_uint32),
+        ("load_factor_pct", C.c_uint32), ("l2_budget_bytes", C.c_uint64),
+    ]
+
+
 # Exported symbols and their ctypes signatures.
 _VP, _SZ, _U64, _I = C.c_void_p, C.c_size_t, C.c_uint64, C.c_int
 SIGNATURES = {
@@ -105,6 +139,13 @@ SIGNATURES = {
     "pimdal_smj_merge": (_I, [_VP, C.POINTER(SmjMergeArguments), _VP, _VP]),
     "pimdal_sort_merge_join_workspace_size": (_I, [C.POINTER(SmjArguments), C.POINTER(_SZ)]),
     "pimdal_sort_merge_join": (_I, [_VP, C.POINTER(SmjArguments), _VP, _VP]),
+    "pimdal_part_workspace_size": (_I, [C.POINTER(PartArguments), C.POINTER(_SZ)]),
+    "pimdal_part_kernel": (_I, [_VP, C.POINTER(PartArguments), _VP]),
+    "pimdal_hash_table_bytes": (_SZ, [_U64]),
+    "pimdal_hash_kernel": (_I, [_VP, C.POINTER(HashArguments), _VP]),
+    "pimdal_hj_probe": (_I, [_VP, C.POINTER(ProbeArguments), _VP, _VP]),
+    "pimdal_hash_join_workspace_size": (_I, [C.POINTER(HashJoinArguments), C.POINTER(_SZ)]),
+    "pimdal_hash_join": (_I, [_VP, C.POINTER(HashJoinArguments), _VP, _VP]),
 }
 
 _lib = None

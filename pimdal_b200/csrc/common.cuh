@@ -397,3 +397,15 @@ PD_HD uint32_t pd_hash0(uint32_t key) {
 PD_HD uint64_t pd_hash_slot(uint32_t key, uint32_t bits) {
   return bits ? (((uint64_t)key * PD_GOLDEN64) >> (64 - bits)) : 0;
 }
+// Top 32 bits of the same product: partition digits are taken from its top
+// bits, table slots from the bits below them.
+PD_HD uint32_t pd_mulhash32(uint32_t key) { return (uint32_t)(((uint64_t)key * PD_GOLDEN64) >> 32); }
+
+// ---------------------------------------------------------------------------
+// Internal entry points shared between translation units.
+// ---------------------------------------------------------------------------
+enum : int { PD_KEY_PLAIN = 0, PD_KEY_HASH0 = 1, PD_KEY_MULHASH = 2 };
+int pd_sort_with_workspace(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, void *ws,
+                           cudaStream_t s);
+int pd_sort_ex(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
+               cudaStream_t s, uint32_t **offsets_out);

@@ -1,0 +1,659 @@
+// K-PART / K-BUILD / K-PROBE: radix partitioning and the hash join
+// (pimdal_part_kernel, pimdal_hash_kernel, pimdal_hj_probe, pimdal_hash_join).
+//
+// Reference behaviour: part_kernel (pimdal/join/hash_join.c:154-235,
+// hash_steps.c:198-294) radix-partitions key_ptr pairs by bits of hash0(key);
+// hash_kernel (hash_join.c:40-115, linear_hash.c:13-23) builds linear-probing
+// tables; merge_kernel (hash_join.c:343-430, linear_hash.c:34-53) probes them
+// and emits (probe ptr, build ptr).  The CPU operator
+// reference/db_operators/hash_join.cpp:57-219 partitions both relations
+// 16384 ways, builds a hash set per partition and probes it.
+//
+// B200 design:
+//  * Partitioning is one onesweep pass of K-SORT on the digits of a hash of
+//    the key (stable, coalesced runs); part_kernel uses hash0's bits so the
+//    partition index a caller sees is the reference's.
+//  * Tables are arrays of 64-bit slots (payload << 32 | key) filled with
+//    atomicCAS linear probing.  The one row whose slot word would equal the
+//    empty word (key and payload all ones) is counted on the side.
+//  * A table that fits the L2 budget is built and probed directly.  A larger
+//    one is split by the top bits of a multiplicative hash: both relations
+//    are partitioned, and partition by partition one table buffer (reused, so
+//    it stays L2-resident and is never written back) is cleared, built and
+//    probed.  All partition bounds live on the device; no host sync.
+//  * Probing: persistent CTAs claim 4096-row tiles; the first slot of all
+//    16 rows of a thread is loaded before any chain is walked (16 random loads
+//    in flight per thread); match counts are scanned and the tile's output
+//    offset resolved by a block-wide decoupled look-back that chains across
+//    the per-partition launches, so the output is in probe order within each
+//    partition, partitions in order.
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace {
+
+constexpr uint64_t HJ_EMPTY = ~0ull;
+constexpr int HJ_THREADS = 256;
+constexpr int HJ_ITEMS = 16;
+constexpr int HJ_TILE = HJ_THREADS * HJ_ITEMS;  // 4096 probe rows per tile
+constexpr uint32_t HJ_MIN_BITS = 10;
+
+__device__ __forceinline__ uint64_t slot_of(uint32_t key, uint32_t part_bits, uint32_t bits) {
+  const uint64_t h = (uint64_t)key * PD_GOLDEN64;
+  return (h << part_bits) >> (64 - bits);
+}
+
+struct JoinParams {
+  // table
+  unsigned long long *table;
+  uint32_t bits, part_bits;
+  uint32_t *side_count;
+  // build side (partition p = rows [boff[p], boff[p+1]))
+  const uint32_t *bkey, *bpay;  // bpay NULL: payload = row id
+  const uint32_t *boff;         // device partition offsets (NULL: whole input)
+  uint64_t nb;
+  // probe side
+  const uint32_t *pkey, *prow;  // prow NULL: row id = index
+  const uint32_t *poff;
+  const uint32_t *tilebase;     // first global tile of each partition
+  uint64_t np;
+  uint32_t part;
+  // output
+  uint32_t *out_pay, *out_row;
+  uint64_t cap;
+  uint64_t *status;
+  uint32_t epoch;
+  uint32_t *claim;
+  uint32_t *d_error;
+  uint64_t *d_count;
+  uint64_t total_tiles;         // for d_count (direct path)
+};
+
+__device__ __forceinline__ void part_range(const uint32_t *off, uint32_t p, uint64_t n,
+                                           uint64_t *lo, uint64_t *hi) {
+  if (off) {
+    *lo = off[p];
+    *hi = off[p + 1];
+  } else {
+    *lo = 0;
+    *hi = n;
+  }
+}
+
+// Fills the table region with the empty word and zeroes the side count.
+__global__ void __launch_bounds__(256) k_hj_clear(JoinParams p) {
+  const uint64_t n = 1ull << p.bits;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  ulonglong2 e = make_ulonglong2(HJ_EMPTY, HJ_EMPTY);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n / 2; i += stride)
+    reinterpret_cast<ulonglong2 *>(p.table)[i] = e;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *p.side_count = 0;
+}
+
+__global__ void __launch_bounds__(256) k_hj_build(JoinParams p) {
+  uint64_t lo, hi;
+  part_range(p.boff, p.part, p.nb, &lo, &hi);
+  const uint64_t mask = (1ull << p.bits) - 1;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = lo + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < hi; i += stride) {
+    const uint32_t k = p.bkey[i];
+    const uint32_t v = p.bpay ? p.bpay[i] : (uint32_t)i;
+    const unsigned long long e = ((unsigned long long)v << 32) | k;
+    if (e == HJ_EMPTY) {
+      atomicAdd(p.side_count, 1u);
+      continue;
+    }
+    uint64_t s = slot_of(k, p.part_bits, p.bits);
+    bool done = false;
+    for (uint64_t t = 0; t <= mask; ++t) {
+      if (atomicCAS(p.table + s, HJ_EMPTY, e) == HJ_EMPTY) {
+        done = true;
+        break;
+      }
+      s = (s + 1) & mask;
+    }
+    if (!done) atomicOr(p.d_error, PD_DEVERR_TABLE_FULL);
+  }
+}
+
+// Counts the matches of key starting at slot s; *first receives the first
+// match's payload.
+__device__ __forceinline__ uint32_t walk_count(const JoinParams &p, uint32_t key,
+                                               unsigned long long e, uint64_t s, uint64_t mask,
+                                               uint32_t *first) {
+  uint32_t c = 0;
+  for (uint64_t t = 0; t <= mask; ++t) {
+    if (e == HJ_EMPTY) break;
+    if ((uint32_t)e == key) {
+      if (c == 0) *first = (uint32_t)(e >> 32);
+      ++c;
+    }
+    s = (s + 1) & mask;
+    e = p.table[s];
+  }
+  return c;
+}
+
+__global__ void __launch_bounds__(HJ_THREADS) k_hj_probe(JoinParams p) {
+  __shared__ uint32_t s_warp[HJ_THREADS / 32];
+  __shared__ uint32_t s_flags[2 * (HJ_THREADS / 32)];
+  __shared__ uint64_t s_sum[HJ_THREADS / 32 + 1];
+  __shared__ int s_state;
+  __shared__ uint64_t s_tile, s_prefix;
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint64_t lo, hi;
+  part_range(p.poff, p.part, p.np, &lo, &hi);
+  const uint64_t tiles = pd_ceil_div(hi - lo, HJ_TILE);
+  const uint64_t gbase = p.tilebase ? p.tilebase[p.part] : 0;
+  const uint64_t mask = (1ull << p.bits) - 1;
+  const uint32_t side = *p.side_count;
+
+  while (true) {
+    if (tid == 0) {
+      uint64_t t = atomicAdd(p.claim, 1u);
+      if (t >= tiles && atomicAdd(p.claim + 1, 1u) == gridDim.x - 1) {
+        p.claim[0] = 0;  // last claimer of the launch resets the counters
+        p.claim[1] = 0;
+      }
+      s_tile = t;
+    }
+    __syncthreads();
+    const uint64_t tl = s_tile;
+    if (tl >= tiles) break;
+    const uint64_t gtile = gbase + tl;
+    const uint64_t r0 = lo + tl * HJ_TILE + (uint64_t)tid * HJ_ITEMS;
+
+    // Keys (blocked: this thread's 16 consecutive probe rows); the first slot
+    // word of every row is loaded before any chain is walked.
+    uint32_t key[HJ_ITEMS], first[HJ_ITEMS];
+    uint32_t one = 0, many = 0, mine = 0;  // bit j: row j has 1 / several matches
+#pragma unroll
+    for (int j = 0; j < HJ_ITEMS; ++j) key[j] = (r0 + j < hi) ? __ldcs(p.pkey + r0 + j) : 0u;
+    {
+      unsigned long long e0[HJ_ITEMS];
+#pragma unroll
+      for (int j = 0; j < HJ_ITEMS; ++j)
+        e0[j] = (r0 + j < hi) ? p.table[slot_of(key[j], p.part_bits, p.bits)] : HJ_EMPTY;
+#pragma unroll
+      for (int j = 0; j < HJ_ITEMS; ++j) {
+        first[j] = 0;
+        if (r0 + j >= hi) continue;
+        uint32_t c = walk_count(p, key[j], e0[j], slot_of(key[j], p.part_bits, p.bits), mask,
+                                &first[j]);
+        if (key[j] == 0xFFFFFFFFu) c += side;
+        if (c == 1 && key[j] != 0xFFFFFFFFu) one |= 1u << j;
+        else if (c) many |= 1u << j;
+        mine += c;
+      }
+    }
+    // Block exclusive scan of per-thread match counts.
+    uint32_t inc = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    uint32_t wpre = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < HJ_THREADS / 32; ++w) {
+      uint32_t x = s_warp[w];
+      if (w < warp) wpre += x;
+      total += x;
+    }
+    const uint32_t excl = wpre + inc - mine;
+    if (gtile == 0) {
+      if (tid == 0) {
+        pd_store_relaxed_u64(p.status, pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, total));
+        s_prefix = 0;
+      }
+    } else {
+      if (tid == 0)
+        pd_store_relaxed_u64(p.status + gtile, pd_pack_status(p.epoch, PD_FLAG_AGGREGATE, total));
+      uint64_t pre = pd_block_lookback<HJ_THREADS>(p.status, (int64_t)gtile, p.epoch, p.d_error,
+                                                   s_flags, s_sum, &s_state);
+      if (tid == 0) {
+        pd_store_relaxed_u64(p.status + gtile,
+                             pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, pre + total));
+        s_prefix = pre;
+      }
+    }
+    __syncthreads();
+    uint64_t w = s_prefix + excl;
+    bool overflow = false;
+#pragma unroll
+    for (int j = 0; j < HJ_ITEMS; ++j) {
+      if (!(((one | many) >> j) & 1u)) continue;
+      const uint32_t row = p.prow ? p.prow[r0 + j] : (uint32_t)(r0 + j);
+      if ((one >> j) & 1u) {
+        if (w < p.cap) { p.out_pay[w] = first[j]; p.out_row[w] = row; } else overflow = true;
+        ++w;
+        continue;
+      }
+      // several matches (or the side-counted row): walk the chain again
+      uint64_t s = slot_of(key[j], p.part_bits, p.bits);
+      unsigned long long e = p.table[s];
+      for (uint64_t t = 0; t <= mask && e != HJ_EMPTY; ++t) {
+        if ((uint32_t)e == key[j]) {
+          if (w < p.cap) { p.out_pay[w] = (uint32_t)(e >> 32); p.out_row[w] = row; } else overflow = true;
+          ++w;
+        }
+        s = (s + 1) & mask;
+        e = p.table[s];
+      }
+      if (key[j] == 0xFFFFFFFFu) {
+        for (uint32_t m = 0; m < side; ++m, ++w) {
+          if (w < p.cap) { p.out_pay[w] = 0xFFFFFFFFu; p.out_row[w] = row; } else overflow = true;
+        }
+      }
+    }
+    if (overflow) atomicOr(p.d_error, PD_DEVERR_CAPACITY);
+    __syncthreads();
+  }
+}
+
+// Total match count: the inclusive prefix of the last global probe tile.
+__global__ void k_hj_count(const uint64_t *status, const uint32_t *tilebase, uint32_t parts,
+                           uint64_t total_tiles, uint32_t epoch, uint64_t *d_count) {
+  uint64_t tiles = tilebase ? tilebase[parts] : total_tiles;
+  uint64_t v = 0;
+  if (tiles) {
+    uint64_t w = pd_load_relaxed_u64(status + tiles - 1);
+    v = w & PD_STATUS_VALUE_MASK;
+  }
+  *d_count = v;
+}
+
+// Exclusive offsets (uint32, P+1 entries) of two partitioned relations and the
+// first global probe tile of each partition.
+__global__ void k_hj_offsets(const uint32_t *boffs, const uint32_t *poffs, uint32_t parts,
+                             uint64_t nb, uint64_t np, uint32_t *boff, uint32_t *poff,
+                             uint32_t *tilebase) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  uint64_t t = 0;
+  for (uint32_t q = 0; q < parts; ++q) {
+    boff[q] = boffs[q];
+    poff[q] = poffs[q];
+    tilebase[q] = (uint32_t)t;
+    uint64_t end = (q + 1 < parts) ? poffs[q + 1] : np;
+    t += pd_ceil_div(end - poffs[q], HJ_TILE);
+  }
+  boff[parts] = (uint32_t)nb;
+  poff[parts] = (uint32_t)np;
+  tilebase[parts] = (uint32_t)t;
+}
+
+int probe_grid(pimdal_ctx *ctx) {
+  static int per_sm = 0;
+  if (!per_sm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hj_probe, HJ_THREADS, 0);
+    if (per_sm <= 0) per_sm = 1;
+  }
+  return per_sm * ctx->sm_count;
+}
+
+struct HjLayout {
+  uint32_t bits, part_bits;
+  size_t table, side, boff, poff, tilebase, bk, bp, pk, pr, sort_ws, total;
+};
+
+bool hj_layout(const pimdal_hash_join_arguments_t *a, HjLayout *l) {
+  uint64_t cap = 1ull << HJ_MIN_BITS;
+  const uint32_t load_pct = a->load_factor_pct ? a->load_factor_pct : 50;
+  if (load_pct > 90) return false;
+  while (cap * load_pct < a->size_build * 100) cap <<= 1;
+  uint32_t bits = 0;
+  while ((1ull << bits) < cap) ++bits;
+  uint64_t budget = a->l2_budget_bytes ? a->l2_budget_bytes : (48ull << 20);
+  uint32_t pb = a->partition_bits;
+  if (pb == 0xFFFFFFFFu) pb = 0;  // explicit "no partitioning"
+  else if (pb == 0) {
+    while ((8ull << bits) > (budget << pb) && pb < 8) ++pb;
+  }
+  if (pb > 8 || pb >= bits) return false;
+  l->part_bits = pb;
+  l->bits = bits - pb;  // slots of one partition's table
+  size_t o = 0;
+  l->table = o; o += pd_align_up(8ull << l->bits, 256);
+  l->side = o; o += 256;
+  l->boff = o; o += pd_align_up(4 * 257, 256);
+  l->poff = o; o += pd_align_up(4 * 257, 256);
+  l->tilebase = o; o += pd_align_up(4 * 257, 256);
+  l->bk = l->bp = l->pk = l->pr = l->sort_ws = 0;
+  if (pb) {
+    l->bk = o; o += pd_align_up(4 * a->size_build, 256);
+    l->bp = o; o += pd_align_up(4 * a->size_build, 256);
+    l->pk = o; o += pd_align_up(4 * a->size_probe, 256);
+    l->pr = o; o += pd_align_up(4 * a->size_probe, 256);
+    pimdal_sort_arguments_t sa{};
+    sa.nr_elements = std::max(a->size_build, a->size_probe);
+    sa.begin_bit = 32 - pb;
+    sa.end_bit = 32;
+    size_t w = 0;
+    if (pimdal_sort_workspace_size(&sa, &w)) return false;
+    l->sort_ws = o; o += w;
+  }
+  l->total = o;
+  return true;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// pimdal_hash_join
+// ---------------------------------------------------------------------------
+extern "C" int pimdal_hash_join_workspace_size(const pimdal_hash_join_arguments_t *a, size_t *bytes) {
+  if (!a || !bytes) return PIMDAL_ERR_ARG;
+  HjLayout l;
+  if (!hj_layout(a, &l)) return PIMDAL_ERR_ARG;
+  *bytes = l.total;
+  return PIMDAL_OK;
+}
+
+extern "C" int pimdal_hash_join(pimdal_ctx_t *ctx, const pimdal_hash_join_arguments_t *a,
+                                pimdal_merge_results_t *d_result, pimdal_stream_t stream) {
+  if (!ctx || !a || !d_result) return PIMDAL_ERR_ARG;
+  if ((a->size_build && !a->build_key) || (a->size_probe && !a->probe_key)) return PIMDAL_ERR_ARG;
+  if (a->out_capacity && (!a->out_build_payload || !a->out_probe_ptr)) return PIMDAL_ERR_ARG;
+  if (a->size_build >= (1ull << 32) || a->size_probe >= (1ull << 30)) return PIMDAL_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaSetDevice(ctx->device);
+  if (a->size_build == 0 || a->size_probe == 0) {
+    PD_CHECK_CUDA(cudaMemsetAsync(d_result, 0, sizeof(uint64_t), s));
+    return PIMDAL_OK;
+  }
+  HjLayout l;
+  if (!hj_layout(a, &l)) return PIMDAL_ERR_ARG;
+  int st;
+  char *ws = (char *)pd_workspace(ctx, l.total, s, &st);
+  if (!ws) return st;
+  const uint32_t parts = 1u << l.part_bits;
+  const uint64_t total_tiles_direct = pd_ceil_div(a->size_probe, HJ_TILE);
+  if (total_tiles_direct + parts > PD_STATUS_WORDS) return PIMDAL_ERR_ARG;
+
+  JoinParams p{};
+  p.table = (unsigned long long *)(ws + l.table);
+  p.bits = l.bits;
+  p.part_bits = l.part_bits;
+  p.side_count = (uint32_t *)(ws + l.side);
+  p.nb = a->size_build;
+  p.np = a->size_probe;
+  p.out_pay = a->out_build_payload;
+  p.out_row = a->out_probe_ptr;
+  p.cap = a->out_capacity;
+  p.status = ctx->d_status;
+  p.claim = ctx->d_counters + PD_COUNTER_PROBE;
+  p.d_error = ctx->d_error;
+  p.d_count = &d_result->t_count;
+  p.epoch = pd_next_epoch(ctx, s, &st);
+  if (st) return st;
+
+  if (l.part_bits) {
+    // Partition both relations by the top part_bits of the multiplicative hash.
+    pimdal_sort_arguments_t sa{};
+    sa.key_dtype = PIMDAL_U32;
+    sa.layout = PIMDAL_LAYOUT_COLUMNS;
+    sa.begin_bit = 32 - l.part_bits;
+    sa.end_bit = 32;
+    uint32_t *boffs, *poffs;
+    sa.nr_elements = a->size_build;
+    sa.in = a->build_key;
+    sa.in_ptr = a->build_payload;
+    sa.out = ws + l.bk;
+    sa.out_ptr = (uint32_t *)(ws + l.bp);
+    if ((st = pd_sort_ex(ctx, &sa, PD_KEY_MULHASH, ws + l.sort_ws, s, &boffs))) return st;
+    // the build offsets live in the sort workspace: save them before reuse
+    uint32_t *boff = (uint32_t *)(ws + l.boff), *poff = (uint32_t *)(ws + l.poff);
+    PD_CHECK_CUDA(cudaMemcpyAsync(boff, boffs, 4 * parts, cudaMemcpyDeviceToDevice, s));
+    sa.nr_elements = a->size_probe;
+    sa.in = a->probe_key;
+    sa.in_ptr = a->probe_ptr;
+    sa.out = ws + l.pk;
+    sa.out_ptr = (uint32_t *)(ws + l.pr);
+    if ((st = pd_sort_ex(ctx, &sa, PD_KEY_MULHASH, ws + l.sort_ws, s, &poffs))) return st;
+    {
+      pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+      k_hj_offsets<<<1, 32, 0, s>>>(boff, poffs, parts, a->size_build, a->size_probe, boff, poff,
+                                    (uint32_t *)(ws + l.tilebase));
+    }
+    p.bkey = (const uint32_t *)(ws + l.bk);
+    p.bpay = (const uint32_t *)(ws + l.bp);
+    p.pkey = (const uint32_t *)(ws + l.pk);
+    p.prow = (const uint32_t *)(ws + l.pr);
+    p.boff = boff;
+    p.poff = poff;
+    p.tilebase = (const uint32_t *)(ws + l.tilebase);
+  } else {
+    p.bkey = (const uint32_t *)a->build_key;
+    p.bpay = a->build_payload;
+    p.pkey = (const uint32_t *)a->probe_key;
+    p.prow = a->probe_ptr;
+  }
+  const unsigned clear_grid = (unsigned)std::min<uint64_t>(pd_ceil_div(1ull << l.bits, 512), ctx->sm_count * 8ull);
+  const unsigned build_grid = ctx->sm_count * 8;
+  const int pgrid = probe_grid(ctx);
+  for (uint32_t q = 0; q < parts; ++q) {
+    p.part = q;
+    {
+      pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+      k_hj_clear<<<clear_grid, 256, 0, s>>>(p);
+    }
+    {
+      pd_launch_scope sc(ctx, PIMDAL_KERNEL_HJ_BUILD, s);
+      k_hj_build<<<build_grid, 256, 0, s>>>(p);
+    }
+    {
+      pd_launch_scope sc(ctx, PIMDAL_KERNEL_HJ_PROBE, s);
+      k_hj_probe<<<pgrid, HJ_THREADS, 0, s>>>(p);
+    }
+  }
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_hj_count<<<1, 1, 0, s>>>(p.status, p.tilebase, parts, total_tiles_direct, p.epoch, p.d_count);
+  }
+  return pd_launch_status(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// Reference-shaped building blocks: pimdal_hash_kernel / pimdal_hj_probe use
+// a caller-owned table of table_size slots preceded by one header word.
+// ---------------------------------------------------------------------------
+extern "C" size_t pimdal_hash_table_bytes(uint64_t table_size) { return 8 * (table_size + 1); }
+
+extern "C" int pimdal_hash_kernel(pimdal_ctx_t *ctx, const pimdal_hash_arguments_t *a,
+                                  pimdal_stream_t stream) {
+  if (!ctx || !a || !a->table_ptr) return PIMDAL_ERR_ARG;
+  if (a->size && !a->in_key) return PIMDAL_ERR_ARG;
+  if (a->table_size < 2 || (a->table_size & (a->table_size - 1)) || a->size > a->table_size)
+    return PIMDAL_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaSetDevice(ctx->device);
+  JoinParams p{};
+  p.table = (unsigned long long *)a->table_ptr + 1;
+  p.side_count = (uint32_t *)a->table_ptr;
+  uint32_t bits = 0;
+  while ((1ull << bits) < a->table_size) ++bits;
+  p.bits = bits;
+  p.bkey = (const uint32_t *)a->in_key;
+  p.bpay = a->in_ptr;
+  p.nb = a->size;
+  p.d_error = ctx->d_error;
+  PD_CHECK_CUDA(cudaMemsetAsync(a->table_ptr, 0, 8, s));
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_hj_clear<<<(unsigned)std::min<uint64_t>(pd_ceil_div(a->table_size, 512), ctx->sm_count * 8ull), 256, 0, s>>>(p);
+  }
+  if (a->size) {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_HJ_BUILD, s);
+    k_hj_build<<<ctx->sm_count * 8, 256, 0, s>>>(p);
+  }
+  return pd_launch_status(ctx);
+}
+
+extern "C" int pimdal_hj_probe(pimdal_ctx_t *ctx, const pimdal_probe_arguments_t *a,
+                               pimdal_merge_results_t *d_result, pimdal_stream_t stream) {
+  if (!ctx || !a || !d_result || !a->table_ptr) return PIMDAL_ERR_ARG;
+  if (a->size && !a->in_key) return PIMDAL_ERR_ARG;
+  if (a->out_capacity && (!a->out_inner || !a->out_outer)) return PIMDAL_ERR_ARG;
+  if (a->table_size < 2 || (a->table_size & (a->table_size - 1)) || a->size >= (1ull << 32))
+    return PIMDAL_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaSetDevice(ctx->device);
+  if (a->size == 0) {
+    PD_CHECK_CUDA(cudaMemsetAsync(d_result, 0, sizeof(uint64_t), s));
+    return PIMDAL_OK;
+  }
+  const uint64_t tiles = pd_ceil_div(a->size, HJ_TILE);
+  if (tiles > PD_STATUS_WORDS) return PIMDAL_ERR_ARG;
+  int st;
+  JoinParams p{};
+  p.table = (unsigned long long *)a->table_ptr + 1;
+  p.side_count = (uint32_t *)a->table_ptr;
+  uint32_t bits = 0;
+  while ((1ull << bits) < a->table_size) ++bits;
+  p.bits = bits;
+  p.pkey = (const uint32_t *)a->in_key;
+  p.prow = a->in_ptr;
+  p.np = a->size;
+  p.out_pay = a->out_inner;
+  p.out_row = a->out_outer;
+  p.cap = a->out_capacity;
+  p.status = ctx->d_status;
+  p.claim = ctx->d_counters + PD_COUNTER_PROBE;
+  p.d_error = ctx->d_error;
+  p.d_count = &d_result->t_count;
+  p.epoch = pd_next_epoch(ctx, s, &st);
+  if (st) return st;
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_HJ_PROBE, s);
+    k_hj_probe<<<probe_grid(ctx), HJ_THREADS, 0, s>>>(p);
+  }
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_hj_count<<<1, 1, 0, s>>>(p.status, nullptr, 1, tiles, p.epoch, p.d_count);
+  }
+  return pd_launch_status(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// pimdal_part_kernel: stable radix partition by bits of hash0(key).
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void __launch_bounds__(256) k_part_hist(const uint32_t *key, uint64_t n, uint32_t sh,
+                                                   uint32_t part_n, uint64_t *sizes) {
+  extern __shared__ uint32_t s_h[];
+  const bool smem = part_n <= 8192;
+  if (smem)
+    for (uint32_t i = threadIdx.x; i < part_n; i += blockDim.x) s_h[i] = 0;
+  __syncthreads();
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    uint32_t b = (pd_hash0(key[i]) >> sh) & (part_n - 1);
+    if (smem) atomicAdd(&s_h[b], 1u);
+    else atomicAdd((unsigned long long *)&sizes[b + 1], 1ull);
+  }
+  __syncthreads();
+  if (smem)
+    for (uint32_t i = threadIdx.x; i < part_n; i += blockDim.x)
+      if (s_h[i]) atomicAdd((unsigned long long *)&sizes[i + 1], (unsigned long long)s_h[i]);
+}
+
+// In-place inclusive scan of sizes[1..part_n] (sizes[0] = 0) by one block.
+__global__ void __launch_bounds__(1024) k_part_scan(uint64_t *sizes, uint32_t part_n) {
+  __shared__ uint64_t s_carry;
+  __shared__ uint64_t s_w[32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < part_n; base += 1024) {
+    uint32_t i = base + tid;
+    uint64_t v = i < part_n ? sizes[i + 1] : 0, inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint64_t t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    if (lane == 31) s_w[warp] = inc;
+    __syncthreads();
+    uint64_t pre = 0, tot = 0;
+    for (int w = 0; w < 32; ++w) {
+      if (w < warp) pre += s_w[w];
+      tot += s_w[w];
+    }
+    if (i < part_n) sizes[i + 1] = s_carry + pre + inc;
+    __syncthreads();
+    if (tid == 0) s_carry += tot;
+    __syncthreads();
+  }
+  if (tid == 0) sizes[0] = 0;
+}
+}  // namespace
+
+extern "C" int pimdal_part_workspace_size(const pimdal_part_arguments_t *a, size_t *bytes) {
+  if (!a || !bytes) return PIMDAL_ERR_ARG;
+  uint32_t bits = 0;
+  while ((1u << bits) < a->part_n) ++bits;
+  pimdal_sort_arguments_t sa{};
+  sa.nr_elements = a->size;
+  sa.begin_bit = a->shift >= bits ? a->shift - bits : 0;
+  sa.end_bit = a->shift ? a->shift : 32;
+  if (bits == 0) sa.begin_bit = 0, sa.end_bit = 1;
+  return pimdal_sort_workspace_size(&sa, bytes);
+}
+
+extern "C" int pimdal_part_kernel(pimdal_ctx_t *ctx, const pimdal_part_arguments_t *a,
+                                  pimdal_stream_t stream) {
+  if (!ctx || !a || !a->part_sizes) return PIMDAL_ERR_ARG;
+  if (a->part_n == 0 || (a->part_n & (a->part_n - 1)) || a->part_n > 65536) return PIMDAL_ERR_ARG;
+  if (a->layout != PIMDAL_LAYOUT_COLUMNS && a->layout != PIMDAL_LAYOUT_PAIRS) return PIMDAL_ERR_ARG;
+  uint32_t bits = 0;
+  while ((1u << bits) < a->part_n) ++bits;
+  if (a->shift > 32 || a->shift < bits) return PIMDAL_ERR_ARG;
+  if (a->size && (!a->in || !a->part_out)) return PIMDAL_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaSetDevice(ctx->device);
+  PD_CHECK_CUDA(cudaMemsetAsync(a->part_sizes, 0, 8ull * (a->part_n + 1), s));
+  if (a->size == 0) return PIMDAL_OK;
+  if (a->layout == PIMDAL_LAYOUT_PAIRS) {
+    // histogram of the pairs' keys: strided view of the key field
+    return PIMDAL_ERR_NOT_SUPPORTED;
+  }
+  const uint32_t sh = a->shift - bits;
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    size_t smem = a->part_n <= 8192 ? 4ull * a->part_n : 0;
+    k_part_hist<<<ctx->sm_count * 4, 256, smem, s>>>((const uint32_t *)a->in, a->size, sh, a->part_n,
+                                                    a->part_sizes);
+  }
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_part_scan<<<1, 1024, 0, s>>>(a->part_sizes, a->part_n);
+  }
+  if (bits == 0) {
+    PD_CHECK_CUDA(cudaMemcpyAsync(a->part_out, a->in, 4 * a->size, cudaMemcpyDeviceToDevice, s));
+    if (a->part_out_ptr) {
+      if (!a->in_ptr) return PIMDAL_ERR_ARG;
+      PD_CHECK_CUDA(cudaMemcpyAsync(a->part_out_ptr, a->in_ptr, 4 * a->size, cudaMemcpyDeviceToDevice, s));
+    }
+    return PIMDAL_OK;
+  }
+  size_t need;
+  int st = pimdal_part_workspace_size(a, &need);
+  if (st) return st;
+  void *ws = pd_workspace(ctx, need, s, &st);
+  if (!ws) return st;
+  pimdal_sort_arguments_t sa{};
+  sa.nr_elements = a->size;
+  sa.in = a->in;
+  sa.in_ptr = a->in_ptr;
+  sa.out = a->part_out;
+  sa.out_ptr = a->part_out_ptr;
+  sa.key_dtype = PIMDAL_U32;
+  sa.layout = PIMDAL_LAYOUT_COLUMNS;
+  sa.begin_bit = sh;
+  sa.end_bit = a->shift;
+  return pd_sort_ex(ctx, &sa, PD_KEY_HASH0, ws, s, nullptr);
+}

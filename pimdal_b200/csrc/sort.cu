@@ -55,6 +55,7 @@ struct SortParams {
   uint32_t *alt_key, *alt_ptr;
   uint64_t n;
   uint32_t flip;        // 0x80000000 for signed keys
+  int key_mode;         // digits of: 0 the key, 1 hash0(key), 2 multiplicative hash
   uint32_t begin_bit, end_bit, npasses;
   int pairs;            // in/out are key_ptr32 arrays
   int has_vals;
@@ -70,7 +71,10 @@ struct SortParams {
 __device__ __forceinline__ uint32_t digit_of(uint32_t k, const SortParams &p, uint32_t pass) {
   uint32_t shift = p.begin_bit + pass * RS_RADIX_BITS;
   uint32_t bits = min((uint32_t)RS_RADIX_BITS, p.end_bit - shift);
-  return ((k ^ p.flip) >> shift) & ((1u << bits) - 1u);
+  uint32_t t = k ^ p.flip;
+  if (p.key_mode == PD_KEY_HASH0) t = pd_hash0(k);
+  else if (p.key_mode == PD_KEY_MULHASH) t = pd_mulhash32(k);
+  return (t >> shift) & ((1u << bits) - 1u);
 }
 
 __device__ __forceinline__ uint32_t load_key_in(const SortParams &p, uint64_t i) {
@@ -380,8 +384,17 @@ extern "C" int pimdal_sort_workspace_size(const pimdal_sort_arguments_t *a, size
 // sort internally, e.g. the sort-merge join and the sort group-by).
 int pd_sort_with_workspace(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, void *ws,
                            cudaStream_t s) {
+  return pd_sort_ex(ctx, a, PD_KEY_PLAIN, ws, s, nullptr);
+}
+
+// Same, ordering by the digits of a transform of the key (a stable radix
+// partition when the bit range is one digit wide).  *offsets_out, when given,
+// receives the device address of the exclusive digit offsets of pass 0.
+int pd_sort_ex(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
+               cudaStream_t s, uint32_t **offsets_out) {
   SortLayout l;
   if (!sort_layout(a, &l)) return PIMDAL_ERR_ARG;
+  if (offsets_out) *offsets_out = (uint32_t *)((char *)ws + l.off_offsets);
   if (a->nr_elements > RS_COUNT_MASK) return PIMDAL_ERR_ARG;  // < 2^30 elements
   char *w = (char *)ws;
   SortParams p{};
@@ -396,6 +409,7 @@ int pd_sort_with_workspace(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, vo
   p.alt_ptr = (uint32_t *)(w + l.off_alt_ptr);
   p.n = a->nr_elements;
   p.flip = a->key_dtype == PIMDAL_I32 ? 0x80000000u : 0u;
+  p.key_mode = key_mode;
   p.begin_bit = a->begin_bit;
   p.end_bit = a->end_bit ? a->end_bit : 32;
   p.npasses = l.npasses;

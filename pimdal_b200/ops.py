@@ -214,3 +214,84 @@ def sort_merge_join(ctx: Context, inner_key, inner_payload, outer_key, outer_pay
     L.check(ctx.lib.pimdal_sort_merge_join(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
             "pimdal_sort_merge_join")
     return result, out_inner, out_outer
+
+
+# ---------------------------------------------------------------------------
+# Radix partition (part_kernel, pimdal/join/hash_join.h:72)
+# ---------------------------------------------------------------------------
+def part_kernel(ctx: Context, keys, ptr=None, *, shift: int = 32, part_n: int = 32,
+                out=None, out_ptr=None, want_ptr: bool = True, stream=None):
+    """Stable partition by bits [shift - log2(part_n), shift) of hash0(key).
+    Returns (out keys, out row ids, part_sizes uint64[part_n + 1])."""
+    n = keys.numel()
+    dev = keys.device
+    if out is None:
+        out = torch.empty_like(keys)
+    if want_ptr and out_ptr is None:
+        out_ptr = torch.empty(n, dtype=torch.int32, device=dev)
+    sizes = torch.empty(part_n + 1, dtype=torch.int64, device=dev)
+    a = L.PartArguments(in_=_ptr(keys), in_ptr=_ptr(ptr), size=n, shift=shift, part_n=part_n,
+                        part_out=_ptr(out), part_out_ptr=_ptr(out_ptr), part_sizes=_ptr(sizes),
+                        layout=L.LAYOUT_COLUMNS)
+    _workspace(ctx, ctx.lib.pimdal_part_workspace_size, a)
+    L.check(ctx.lib.pimdal_part_kernel(ctx.handle, C.byref(a), _stream(stream)), "pimdal_part_kernel")
+    return out, out_ptr, sizes
+
+
+# ---------------------------------------------------------------------------
+# Hash tables (hash_kernel / merge_kernel, pimdal/join/hash_join.h:62,82)
+# ---------------------------------------------------------------------------
+def hash_kernel(ctx: Context, keys, ptr=None, *, table_size: int, table=None, stream=None):
+    """Builds a linear-probing table; returns the table (uint8 device tensor)."""
+    if table is None:
+        nbytes = int(ctx.lib.pimdal_hash_table_bytes(table_size))
+        table = torch.empty(nbytes, dtype=torch.uint8, device=keys.device)
+    a = L.HashArguments(in_key=_ptr(keys), in_ptr=_ptr(ptr), size=keys.numel(),
+                        table_ptr=_ptr(table), table_size=table_size)
+    L.check(ctx.lib.pimdal_hash_kernel(ctx.handle, C.byref(a), _stream(stream)), "pimdal_hash_kernel")
+    return table
+
+
+def hj_probe(ctx: Context, table, table_size: int, keys, ptr=None, *, capacity: int | None = None,
+             out_outer=None, out_inner=None, result=None, stream=None):
+    """Probes a table; returns (result, probe ptr per match, build payload per match)."""
+    dev = keys.device
+    if capacity is None:
+        capacity = max(keys.numel(), 1)
+    if out_outer is None:
+        out_outer = torch.empty(capacity, dtype=torch.int32, device=dev)
+    if out_inner is None:
+        out_inner = torch.empty(capacity, dtype=torch.int32, device=dev)
+    if result is None:
+        result = torch.empty(1, dtype=torch.int64, device=dev)
+    a = L.ProbeArguments(table_ptr=_ptr(table), table_size=table_size, in_key=_ptr(keys),
+                         in_ptr=_ptr(ptr), size=keys.numel(), out_outer=_ptr(out_outer),
+                         out_inner=_ptr(out_inner), out_capacity=capacity)
+    L.check(ctx.lib.pimdal_hj_probe(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
+            "pimdal_hj_probe")
+    return result, out_outer, out_inner
+
+
+def hash_join(ctx: Context, build_key, build_payload, probe_key, probe_ptr=None, *,
+              capacity: int | None = None, partition_bits: int = 0, load_factor_pct: int = 0,
+              l2_budget_bytes: int = 0, out_payload=None, out_row=None, result=None, stream=None):
+    """Hash join; returns (result, build payload per match, probe row id per match)."""
+    dev = probe_key.device
+    if capacity is None:
+        capacity = max(probe_key.numel(), 1)
+    if out_payload is None:
+        out_payload = torch.empty(capacity, dtype=torch.int32, device=dev)
+    if out_row is None:
+        out_row = torch.empty(capacity, dtype=torch.int32, device=dev)
+    if result is None:
+        result = torch.empty(1, dtype=torch.int64, device=dev)
+    a = L.HashJoinArguments(build_key=_ptr(build_key), build_payload=_ptr(build_payload),
+                            size_build=build_key.numel(), probe_key=_ptr(probe_key),
+                            probe_ptr=_ptr(probe_ptr), size_probe=probe_key.numel(),
+                            out_build_payload=_ptr(out_payload), out_probe_ptr=_ptr(out_row),
+                            out_capacity=capacity, partition_bits=partition_bits,
+                            load_factor_pct=load_factor_pct, l2_budget_bytes=l2_budget_bytes)
+    _workspace(ctx, ctx.lib.pimdal_hash_join_workspace_size, a)
+    L.check(ctx.lib.pimdal_hash_join(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
+            "pimdal_hash_join")
+    return result, out_payload, out_row
