@@ -359,6 +359,46 @@ int pimdal_hash_join_workspace_size(const pimdal_hash_join_arguments_t *args, si
 int pimdal_hash_join(pimdal_ctx_t *ctx, const pimdal_hash_join_arguments_t *args,
                      pimdal_merge_results_t *d_result, pimdal_stream_t stream);
 
+/* ------------------------------------------------------------------------- */
+/* Group-by.  Replaces group_kernel (pimdal/aggregate/aggregate.h:7-25):      */
+/* the hash variant of aggregate_hash.c:123-194 and the sort variant of       */
+/* aggregate.c:82-158, plus the host merge and order_by of                    */
+/* pimdal/main/aggregate/hash/host/host_aggregate_sync.cpp:71-95, and the CPU */
+/* hash_table_aggregate of reference/db_operators/aggregate.cpp:40-83.  The   */
+/* combiner function pointer (aggregate.h:11; UNIQUE / COUNT / SUM of         */
+/* groupby.h:17-21) becomes a fixed set of exact int64 aggregates -- any of   */
+/* SUM (wrapping mod 2^64), COUNT, MIN, MAX -- each requested by passing its  */
+/* output column.  Groups come out ascending by key (signed for I32).         */
+/* ------------------------------------------------------------------------- */
+typedef enum {
+  PIMDAL_GROUP_AUTO = 0, /* hash */
+  PIMDAL_GROUP_HASH = 1, /* shared-memory tables + global table, then key order */
+  PIMDAL_GROUP_SORT = 2  /* stable radix sort, then reduce-by-key              */
+} pimdal_group_method_t;
+
+typedef struct {
+  uint64_t size;           /* aggr_arguments_t.size: rows (< 2^30)              */
+  const void *in;          /* aggr_arguments_t.in: group keys (int32 / uint32)  */
+  const int64_t *in_val;   /* values; NULL = 1 for every row                    */
+  void *out;               /* aggr_arguments_t.out: group keys, ascending       */
+  int64_t *out_sum;        /* per group; any of these may be NULL               */
+  int64_t *out_count;
+  int64_t *out_min;
+  int64_t *out_max;
+  uint64_t out_capacity;   /* groups room in the outputs                        */
+  uint64_t expected_groups;/* hash method: table sizing hint (0 = min(size, 2^22)) */
+  int32_t key_dtype;       /* PIMDAL_I32 or PIMDAL_U32                           */
+  int32_t method;          /* pimdal_group_method_t                             */
+} pimdal_aggr_arguments_t;
+
+typedef struct {
+  uint64_t t_count; /* aggr_results_t.t_count: number of groups */
+} pimdal_aggr_results_t;
+
+int pimdal_group_workspace_size(const pimdal_aggr_arguments_t *args, size_t *bytes);
+int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_arguments_t *args,
+                        pimdal_aggr_results_t *d_result, pimdal_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -118,6 +118,18 @@ class HashJoinArguments(C.Structure):
     ]
 
 
+GROUP_AUTO, GROUP_HASH, GROUP_SORT = 0, 1, 2
+
+
+class AggrArguments(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint64), ("in_", C.c_void_p), ("in_val", C.c_void_p), ("out", C.c_void_p),
+        ("out_sum", C.c_void_p), ("out_count", C.c_void_p), ("out_min", C.c_void_p),
+        ("out_max", C.c_void_p), ("out_capacity", C.c_uint64), ("expected_groups", C.c_uint64),
+        ("key_dtype", C.c_int32), ("method", C.c_int32),
+    ]
+
+
 # Exported symbols and their ctypes signatures.
 _VP, _SZ, _U64, _I = C.c_void_p, C.c_size_t, C.c_uint64, C.c_int
 SIGNATURES = {
@@ -146,6 +158,8 @@ SIGNATURES = {
     "pimdal_hj_probe": (_I, [_VP, C.POINTER(ProbeArguments), _VP, _VP]),
     "pimdal_hash_join_workspace_size": (_I, [C.POINTER(HashJoinArguments), C.POINTER(_SZ)]),
     "pimdal_hash_join": (_I, [_VP, C.POINTER(HashJoinArguments), _VP, _VP]),
+    "pimdal_group_workspace_size": (_I, [C.POINTER(AggrArguments), C.POINTER(_SZ)]),
+    "pimdal_group_kernel": (_I, [_VP, C.POINTER(AggrArguments), _VP, _VP]),
 }
 
 _lib = None

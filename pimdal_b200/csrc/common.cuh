@@ -409,3 +409,5 @@ int pd_sort_with_workspace(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, vo
                            cudaStream_t s);
 int pd_sort_ex(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
                cudaStream_t s, uint32_t **offsets_out);
+int pd_sort_ex2(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
+                cudaStream_t s, uint32_t **offsets_out, const uint64_t *n_dev);

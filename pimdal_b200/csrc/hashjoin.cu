@@ -21,9 +21,10 @@
 //    are partitioned, and partition by partition one table buffer (reused, so
 //    it stays L2-resident and is never written back) is cleared, built and
 //    probed.  All partition bounds live on the device; no host sync.
-//  * Probing: persistent CTAs claim 4096-row tiles; the first slot of all
-//    16 rows of a thread is loaded before any chain is walked (16 random loads
-//    in flight per thread); match counts are scanned and the tile's output
+//  * Probing: persistent CTAs claim 2048-row tiles; a thread walks its 8 rows
+//    4 at a time in lockstep, reading the table in 32-byte groups of 4 slots
+//    (one sector per step, 4 sector loads in flight per thread; with no
+//    duplicate build key a walk stops at its first match); match counts are scanned and the tile's output
 //    offset resolved by a block-wide decoupled look-back that chains across
 //    the per-partition launches, so the output is in probe order within each
 //    partition, partitions in order.
@@ -35,8 +36,8 @@ namespace {
 
 constexpr uint64_t HJ_EMPTY = ~0ull;
 constexpr int HJ_THREADS = 256;
-constexpr int HJ_ITEMS = 16;
-constexpr int HJ_TILE = HJ_THREADS * HJ_ITEMS;  // 4096 probe rows per tile
+constexpr int HJ_ITEMS = 8;
+constexpr int HJ_TILE = HJ_THREADS * HJ_ITEMS;  // 2048 probe rows per tile
 constexpr uint32_t HJ_MIN_BITS = 10;
 
 __device__ __forceinline__ uint64_t slot_of(uint32_t key, uint32_t part_bits, uint32_t bits) {
@@ -49,6 +50,7 @@ struct JoinParams {
   unsigned long long *table;
   uint32_t bits, part_bits;
   uint32_t *side_count;
+  uint32_t *dup_flag;           // set by the build when a key occurs twice
   // build side (partition p = rows [boff[p], boff[p+1]))
   const uint32_t *bkey, *bpay;  // bpay NULL: payload = row id
   const uint32_t *boff;         // device partition offsets (NULL: whole input)
@@ -88,7 +90,10 @@ __global__ void __launch_bounds__(256) k_hj_clear(JoinParams p) {
   ulonglong2 e = make_ulonglong2(HJ_EMPTY, HJ_EMPTY);
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n / 2; i += stride)
     reinterpret_cast<ulonglong2 *>(p.table)[i] = e;
-  if (blockIdx.x == 0 && threadIdx.x == 0) *p.side_count = 0;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    *p.side_count = 0;
+    *p.dup_flag = 0;
+  }
 }
 
 __global__ void __launch_bounds__(256) k_hj_build(JoinParams p) {
@@ -106,33 +111,76 @@ __global__ void __launch_bounds__(256) k_hj_build(JoinParams p) {
     }
     uint64_t s = slot_of(k, p.part_bits, p.bits);
     bool done = false;
+    bool dup = false;
     for (uint64_t t = 0; t <= mask; ++t) {
-      if (atomicCAS(p.table + s, HJ_EMPTY, e) == HJ_EMPTY) {
+      const unsigned long long old = atomicCAS(p.table + s, HJ_EMPTY, e);
+      if (old == HJ_EMPTY) {
         done = true;
         break;
       }
+      dup |= (uint32_t)old == k;  // an equal key always lies on this key's probe path
       s = (s + 1) & mask;
     }
+    if (dup) *p.dup_flag = 1;
     if (!done) atomicOr(p.d_error, PD_DEVERR_TABLE_FULL);
   }
 }
 
-// Counts the matches of key starting at slot s; *first receives the first
-// match's payload.
-__device__ __forceinline__ uint32_t walk_count(const JoinParams &p, uint32_t key,
-                                               unsigned long long e, uint64_t s, uint64_t mask,
-                                               uint32_t *first) {
-  uint32_t c = 0;
-  for (uint64_t t = 0; t <= mask; ++t) {
-    if (e == HJ_EMPTY) break;
-    if ((uint32_t)e == key) {
-      if (c == 0) *first = (uint32_t)(e >> 32);
-      ++c;
-    }
-    s = (s + 1) & mask;
-    e = p.table[s];
+// Match walk of HJ_BATCH probe rows in lockstep.  The table is read in
+// aligned groups of 4 slots (one 32-byte sector): the walk of a row starts at
+// its slot inside the first group and ends at the first empty slot (or, when
+// the build saw no duplicate key, at the first match).  The loads of all
+// rows of the batch are issued before any is inspected.
+constexpr int HJ_BATCH = 4;
+
+__device__ __forceinline__ void walk_batch(const JoinParams &p, const uint32_t *key,
+                                           const bool *valid, bool stop_first, uint64_t mask,
+                                           uint32_t *cnt, uint32_t *first) {
+  uint64_t g[HJ_BATCH];
+  uint32_t off[HJ_BATCH];
+  bool active[HJ_BATCH];
+#pragma unroll
+  for (int i = 0; i < HJ_BATCH; ++i) {
+    const uint64_t s = slot_of(key[i], p.part_bits, p.bits);
+    g[i] = s & ~3ull;
+    off[i] = (uint32_t)(s & 3);
+    active[i] = valid[i];
+    cnt[i] = 0;
+    first[i] = 0;
   }
-  return c;
+  const bool early = stop_first;
+  for (uint64_t round = 0; round <= (mask >> 2); ++round) {
+    ulonglong2 lo[HJ_BATCH], hi[HJ_BATCH];
+    bool any = false;
+#pragma unroll
+    for (int i = 0; i < HJ_BATCH; ++i) {
+      if (active[i]) {
+        const ulonglong2 *q = reinterpret_cast<const ulonglong2 *>(p.table + g[i]);
+        lo[i] = q[0];
+        hi[i] = q[1];
+        any = true;
+      }
+    }
+    if (!any) break;
+#pragma unroll
+    for (int i = 0; i < HJ_BATCH; ++i) {
+      if (!active[i]) continue;
+      const unsigned long long e[4] = {lo[i].x, lo[i].y, hi[i].x, hi[i].y};
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (!active[i] || (uint32_t)j < off[i]) continue;
+        if (e[j] == HJ_EMPTY) {
+          active[i] = false;
+        } else if ((uint32_t)e[j] == key[i]) {
+          if (cnt[i] == 0) first[i] = (uint32_t)(e[j] >> 32);
+          ++cnt[i];
+          if (early && key[i] != 0xFFFFFFFFu) active[i] = false;
+        }
+      }
+      off[i] = 0;
+      g[i] = (g[i] + 4) & mask;
+    }
+  }
 }
 
 __global__ void __launch_bounds__(HJ_THREADS) k_hj_probe(JoinParams p) {
@@ -149,6 +197,7 @@ __global__ void __launch_bounds__(HJ_THREADS) k_hj_probe(JoinParams p) {
   const uint64_t gbase = p.tilebase ? p.tilebase[p.part] : 0;
   const uint64_t mask = (1ull << p.bits) - 1;
   const uint32_t side = *p.side_count;
+  const bool stop_first = *p.dup_flag == 0;
 
   while (true) {
     if (tid == 0) {
@@ -165,24 +214,23 @@ __global__ void __launch_bounds__(HJ_THREADS) k_hj_probe(JoinParams p) {
     const uint64_t gtile = gbase + tl;
     const uint64_t r0 = lo + tl * HJ_TILE + (uint64_t)tid * HJ_ITEMS;
 
-    // Keys (blocked: this thread's 16 consecutive probe rows); the first slot
-    // word of every row is loaded before any chain is walked.
+    // This thread's 8 consecutive probe rows, walked 4 at a time.
     uint32_t key[HJ_ITEMS], first[HJ_ITEMS];
     uint32_t one = 0, many = 0, mine = 0;  // bit j: row j has 1 / several matches
 #pragma unroll
     for (int j = 0; j < HJ_ITEMS; ++j) key[j] = (r0 + j < hi) ? __ldcs(p.pkey + r0 + j) : 0u;
-    {
-      unsigned long long e0[HJ_ITEMS];
 #pragma unroll
-      for (int j = 0; j < HJ_ITEMS; ++j)
-        e0[j] = (r0 + j < hi) ? p.table[slot_of(key[j], p.part_bits, p.bits)] : HJ_EMPTY;
+    for (int b = 0; b < HJ_ITEMS; b += HJ_BATCH) {
+      bool valid[HJ_BATCH];
+      uint32_t cnt[HJ_BATCH];
 #pragma unroll
-      for (int j = 0; j < HJ_ITEMS; ++j) {
-        first[j] = 0;
-        if (r0 + j >= hi) continue;
-        uint32_t c = walk_count(p, key[j], e0[j], slot_of(key[j], p.part_bits, p.bits), mask,
-                                &first[j]);
-        if (key[j] == 0xFFFFFFFFu) c += side;
+      for (int i = 0; i < HJ_BATCH; ++i) valid[i] = r0 + b + i < hi;
+      walk_batch(p, key + b, valid, stop_first, mask, cnt, first + b);
+#pragma unroll
+      for (int i = 0; i < HJ_BATCH; ++i) {
+        const int j = b + i;
+        uint32_t c = cnt[i];
+        if (valid[i] && key[j] == 0xFFFFFFFFu) c += side;
         if (c == 1 && key[j] != 0xFFFFFFFFu) one |= 1u << j;
         else if (c) many |= 1u << j;
         mine += c;
@@ -379,6 +427,7 @@ extern "C" int pimdal_hash_join(pimdal_ctx_t *ctx, const pimdal_hash_join_argume
   p.bits = l.bits;
   p.part_bits = l.part_bits;
   p.side_count = (uint32_t *)(ws + l.side);
+  p.dup_flag = (uint32_t *)(ws + l.side) + 2;
   p.nb = a->size_build;
   p.np = a->size_probe;
   p.out_pay = a->out_build_payload;
@@ -461,19 +510,20 @@ extern "C" int pimdal_hash_join(pimdal_ctx_t *ctx, const pimdal_hash_join_argume
 // Reference-shaped building blocks: pimdal_hash_kernel / pimdal_hj_probe use
 // a caller-owned table of table_size slots preceded by one header word.
 // ---------------------------------------------------------------------------
-extern "C" size_t pimdal_hash_table_bytes(uint64_t table_size) { return 8 * (table_size + 1); }
+extern "C" size_t pimdal_hash_table_bytes(uint64_t table_size) { return 8 * (table_size + 4); }
 
 extern "C" int pimdal_hash_kernel(pimdal_ctx_t *ctx, const pimdal_hash_arguments_t *a,
                                   pimdal_stream_t stream) {
-  if (!ctx || !a || !a->table_ptr) return PIMDAL_ERR_ARG;
+  if (!ctx || !a || !a->table_ptr || ((uintptr_t)a->table_ptr & 31u)) return PIMDAL_ERR_ARG;
   if (a->size && !a->in_key) return PIMDAL_ERR_ARG;
   if (a->table_size < 2 || (a->table_size & (a->table_size - 1)) || a->size > a->table_size)
     return PIMDAL_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   cudaSetDevice(ctx->device);
   JoinParams p{};
-  p.table = (unsigned long long *)a->table_ptr + 1;
+  p.table = (unsigned long long *)a->table_ptr + 4;
   p.side_count = (uint32_t *)a->table_ptr;
+  p.dup_flag = (uint32_t *)a->table_ptr + 2;
   uint32_t bits = 0;
   while ((1ull << bits) < a->table_size) ++bits;
   p.bits = bits;
@@ -481,7 +531,7 @@ extern "C" int pimdal_hash_kernel(pimdal_ctx_t *ctx, const pimdal_hash_arguments
   p.bpay = a->in_ptr;
   p.nb = a->size;
   p.d_error = ctx->d_error;
-  PD_CHECK_CUDA(cudaMemsetAsync(a->table_ptr, 0, 8, s));
+  PD_CHECK_CUDA(cudaMemsetAsync(a->table_ptr, 0, 32, s));
   {
     pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
     k_hj_clear<<<(unsigned)std::min<uint64_t>(pd_ceil_div(a->table_size, 512), ctx->sm_count * 8ull), 256, 0, s>>>(p);
@@ -495,7 +545,7 @@ extern "C" int pimdal_hash_kernel(pimdal_ctx_t *ctx, const pimdal_hash_arguments
 
 extern "C" int pimdal_hj_probe(pimdal_ctx_t *ctx, const pimdal_probe_arguments_t *a,
                                pimdal_merge_results_t *d_result, pimdal_stream_t stream) {
-  if (!ctx || !a || !d_result || !a->table_ptr) return PIMDAL_ERR_ARG;
+  if (!ctx || !a || !d_result || !a->table_ptr || ((uintptr_t)a->table_ptr & 31u)) return PIMDAL_ERR_ARG;
   if (a->size && !a->in_key) return PIMDAL_ERR_ARG;
   if (a->out_capacity && (!a->out_inner || !a->out_outer)) return PIMDAL_ERR_ARG;
   if (a->table_size < 2 || (a->table_size & (a->table_size - 1)) || a->size >= (1ull << 32))
@@ -510,8 +560,9 @@ extern "C" int pimdal_hj_probe(pimdal_ctx_t *ctx, const pimdal_probe_arguments_t
   if (tiles > PD_STATUS_WORDS) return PIMDAL_ERR_ARG;
   int st;
   JoinParams p{};
-  p.table = (unsigned long long *)a->table_ptr + 1;
+  p.table = (unsigned long long *)a->table_ptr + 4;
   p.side_count = (uint32_t *)a->table_ptr;
+  p.dup_flag = (uint32_t *)a->table_ptr + 2;
   uint32_t bits = 0;
   while ((1ull << bits) < a->table_size) ++bits;
   p.bits = bits;
@@ -559,6 +610,13 @@ __global__ void __launch_bounds__(256) k_part_hist(const uint32_t *key, uint64_t
   if (smem)
     for (uint32_t i = threadIdx.x; i < part_n; i += blockDim.x)
       if (s_h[i]) atomicAdd((unsigned long long *)&sizes[i + 1], (unsigned long long)s_h[i]);
+}
+
+// out[i] = i (row ids of a one-partition "partition").
+__global__ void __launch_bounds__(256) k_iota(uint32_t *out, uint64_t n) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    out[i] = (uint32_t)i;
 }
 
 // In-place inclusive scan of sizes[1..part_n] (sizes[0] = 0) by one block.
@@ -635,10 +693,15 @@ extern "C" int pimdal_part_kernel(pimdal_ctx_t *ctx, const pimdal_part_arguments
   if (bits == 0) {
     PD_CHECK_CUDA(cudaMemcpyAsync(a->part_out, a->in, 4 * a->size, cudaMemcpyDeviceToDevice, s));
     if (a->part_out_ptr) {
-      if (!a->in_ptr) return PIMDAL_ERR_ARG;
-      PD_CHECK_CUDA(cudaMemcpyAsync(a->part_out_ptr, a->in_ptr, 4 * a->size, cudaMemcpyDeviceToDevice, s));
+      if (a->in_ptr) {
+        PD_CHECK_CUDA(cudaMemcpyAsync(a->part_out_ptr, a->in_ptr, 4 * a->size,
+                                      cudaMemcpyDeviceToDevice, s));
+      } else {
+        pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+        k_iota<<<ctx->sm_count * 4, 256, 0, s>>>(a->part_out_ptr, a->size);
+      }
     }
-    return PIMDAL_OK;
+    return pd_launch_status(ctx);
   }
   size_t need;
   int st = pimdal_part_workspace_size(a, &need);

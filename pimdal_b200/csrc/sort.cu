@@ -21,6 +21,8 @@
 //     warp with match.any, publishes per-digit tile counts and resolves their
 //     global offsets with a per-digit decoupled look-back, stages the tile in
 //     shared memory in digit order and writes each digit run contiguously.
+#include <algorithm>
+
 #include "common.cuh"
 
 namespace {
@@ -53,7 +55,8 @@ struct SortParams {
   void *out;
   uint32_t *out_ptr;
   uint32_t *alt_key, *alt_ptr;
-  uint64_t n;
+  uint64_t n;           // element count (upper bound when n_dev is set)
+  const uint64_t *n_dev;  // device-resident element count, or NULL
   uint32_t flip;        // 0x80000000 for signed keys
   int key_mode;         // digits of: 0 the key, 1 hash0(key), 2 multiplicative hash
   uint32_t begin_bit, end_bit, npasses;
@@ -68,14 +71,7 @@ struct SortParams {
   uint32_t *d_error;
 };
 
-__device__ __forceinline__ uint32_t digit_of(uint32_t k, const SortParams &p, uint32_t pass) {
-  uint32_t shift = p.begin_bit + pass * RS_RADIX_BITS;
-  uint32_t bits = min((uint32_t)RS_RADIX_BITS, p.end_bit - shift);
-  uint32_t t = k ^ p.flip;
-  if (p.key_mode == PD_KEY_HASH0) t = pd_hash0(k);
-  else if (p.key_mode == PD_KEY_MULHASH) t = pd_mulhash32(k);
-  return (t >> shift) & ((1u << bits) - 1u);
-}
+__device__ __forceinline__ uint64_t sort_n(const SortParams &p) { return p.n_dev ? *p.n_dev : p.n; }
 
 __device__ __forceinline__ uint32_t load_key_in(const SortParams &p, uint64_t i) {
   return p.pairs ? reinterpret_cast<const uint2 *>(p.in)[i].x
@@ -83,34 +79,53 @@ __device__ __forceinline__ uint32_t load_key_in(const SortParams &p, uint64_t i)
 }
 
 // ---------------------------------------------------------------- histogram
+template <int KEY_MODE>
+__device__ __forceinline__ uint32_t hist_xform(uint32_t k, uint32_t flip) {
+  if (KEY_MODE == PD_KEY_HASH0) return pd_hash0(k);
+  if (KEY_MODE == PD_KEY_MULHASH) return pd_mulhash32(k);
+  return k ^ flip;
+}
+
+template <int KEY_MODE>
 __global__ void __launch_bounds__(RS_THREADS) k_sort_hist(SortParams p) {
   __shared__ uint32_t sh[RS_WARPS][RS_MAX_PASSES][RS_RADIX];
   const int tid = threadIdx.x, warp = tid >> 5;
   for (int i = tid; i < RS_WARPS * RS_MAX_PASSES * RS_RADIX; i += RS_THREADS)
     (&sh[0][0][0])[i] = 0;
+  uint32_t shift[RS_MAX_PASSES], mask[RS_MAX_PASSES];
+#pragma unroll
+  for (int q = 0; q < RS_MAX_PASSES; ++q) {
+    shift[q] = min(31u, p.begin_bit + q * RS_RADIX_BITS);
+    uint32_t bits = q < (int)p.npasses ? min((uint32_t)RS_RADIX_BITS, p.end_bit - shift[q]) : 0u;
+    mask[q] = (1u << bits) - 1u;
+  }
   __syncthreads();
+  uint32_t (*h)[RS_RADIX] = sh[warp];
+  const uint32_t np = p.npasses, flip = p.flip;
+  auto add = [&](uint32_t k) {
+    const uint32_t t = hist_xform<KEY_MODE>(k, flip);
+#pragma unroll
+    for (int q = 0; q < RS_MAX_PASSES; ++q)
+      if (q < (int)np) atomicAdd(&h[q][(t >> shift[q]) & mask[q]], 1u);
+  };
   const uint64_t stride = (uint64_t)gridDim.x * RS_THREADS;
   const bool vec = !p.pairs && ((uintptr_t)p.in & 15u) == 0;
+  const uint64_t n = sort_n(p);
+  uint64_t done = 0;
   if (vec) {
     const uint4 *in4 = reinterpret_cast<const uint4 *>(p.in);
-    const uint64_t n4 = p.n / 4;
+    const uint64_t n4 = n / 4;
     for (uint64_t i = (uint64_t)blockIdx.x * RS_THREADS + tid; i < n4; i += stride) {
       uint4 v = __ldcs(in4 + i);
-      uint32_t k[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-      for (int j = 0; j < 4; ++j)
-        for (uint32_t q = 0; q < p.npasses; ++q) atomicAdd(&sh[warp][q][digit_of(k[j], p, q)], 1u);
+      add(v.x);
+      add(v.y);
+      add(v.z);
+      add(v.w);
     }
-    for (uint64_t i = n4 * 4 + (uint64_t)blockIdx.x * RS_THREADS + tid; i < p.n; i += stride) {
-      uint32_t k = load_key_in(p, i);
-      for (uint32_t q = 0; q < p.npasses; ++q) atomicAdd(&sh[warp][q][digit_of(k, p, q)], 1u);
-    }
-  } else {
-    for (uint64_t i = (uint64_t)blockIdx.x * RS_THREADS + tid; i < p.n; i += stride) {
-      uint32_t k = load_key_in(p, i);
-      for (uint32_t q = 0; q < p.npasses; ++q) atomicAdd(&sh[warp][q][digit_of(k, p, q)], 1u);
-    }
+    done = n4 * 4;
   }
+  for (uint64_t i = done + (uint64_t)blockIdx.x * RS_THREADS + tid; i < n; i += stride)
+    add(load_key_in(p, i));
   __syncthreads();
   for (uint32_t q = 0; q < p.npasses; ++q) {
     uint32_t s = 0;
@@ -149,11 +164,12 @@ __global__ void __launch_bounds__(RS_THREADS) k_sort_plan(SortParams p) {
   __shared__ uint32_t s_warp[RS_WARPS];
   __shared__ uint32_t s_trivial[RS_MAX_PASSES];
   const int d = threadIdx.x;
+  const uint64_t n = sort_n(p);
   if (d < RS_MAX_PASSES) s_trivial[d] = 0;
   __syncthreads();
   for (uint32_t q = 0; q < p.npasses; ++q) {
     uint32_t c = p.hist[q * RS_RADIX + d];
-    if ((uint64_t)c == p.n) s_trivial[q] = 1;
+    if ((uint64_t)c == n) s_trivial[q] = 1;
     p.offsets[q * RS_RADIX + d] = block_exclusive_scan(c, s_warp, nullptr);
   }
   __syncthreads();
@@ -182,7 +198,8 @@ __global__ void __launch_bounds__(RS_THREADS) k_sort_plan(SortParams p) {
 __global__ void __launch_bounds__(RS_THREADS) k_sort_copy(SortParams p) {
   if (p.plan->n_active != 0) return;
   const uint64_t stride = (uint64_t)gridDim.x * RS_THREADS;
-  for (uint64_t i = (uint64_t)blockIdx.x * RS_THREADS + threadIdx.x; i < p.n; i += stride) {
+  const uint64_t n = sort_n(p);
+  for (uint64_t i = (uint64_t)blockIdx.x * RS_THREADS + threadIdx.x; i < n; i += stride) {
     uint32_t k, v;
     if (p.pairs) {
       uint2 e = reinterpret_cast<const uint2 *>(p.in)[i];
@@ -201,13 +218,23 @@ __global__ void __launch_bounds__(RS_THREADS) k_sort_copy(SortParams p) {
 }
 
 // ------------------------------------------------------------ onesweep pass
-template <bool HAS_VALS>
-__global__ void __launch_bounds__(RS_THREADS, 3) k_sort_pass(SortParams p, uint32_t pass) {
+template <int KEY_MODE>
+__device__ __forceinline__ uint32_t sort_xform(uint32_t k, uint32_t flip) {
+  if (KEY_MODE == PD_KEY_HASH0) return pd_hash0(k);
+  if (KEY_MODE == PD_KEY_MULHASH) return pd_mulhash32(k);
+  return k ^ flip;
+}
+
+// One digit pass.  FULL tiles take a path without bounds checks; indices
+// inside a tile are 32-bit; the digit is (xform(key) >> shift) & mask.
+template <bool HAS_VALS, int KEY_MODE>
+__global__ void __launch_bounds__(RS_THREADS, 3)
+k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   __shared__ uint32_t s_keys[RS_TILE];
   __shared__ uint32_t s_vals[HAS_VALS ? RS_TILE : 1];
   __shared__ uint32_t s_whist[RS_WARPS][RS_RADIX];
   __shared__ uint32_t s_dstart[RS_RADIX];
-  __shared__ long long s_gdelta[RS_RADIX];
+  __shared__ int32_t s_gdelta[RS_RADIX];
   __shared__ uint32_t s_warp[RS_WARPS];
   __shared__ uint32_t s_tile;
 
@@ -215,6 +242,8 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_sort_pass(SortParams p, uint3
   if (!plan->active[pass]) return;
   const uint32_t src = plan->src[pass], dst = plan->dst[pass];
   const bool first = plan->first[pass] != 0;
+  const uint32_t flip = p.flip;
+  auto dig = [&](uint32_t k) { return (sort_xform<KEY_MODE>(k, flip) >> shift) & mask; };
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_tile = atomicAdd(&p.counters[pass], 1u);
@@ -223,7 +252,11 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_sort_pass(SortParams p, uint3
   __syncthreads();
   const uint64_t tile = s_tile;
   const uint64_t base = tile * (uint64_t)RS_TILE;
-  const uint64_t wbase = base + (uint64_t)warp * RS_WARP_TILE;
+  const uint64_t n = sort_n(p);
+  if (base >= n) return;  // tile past a device-resident count: nothing to do
+  const uint32_t tile_n = (uint32_t)min((uint64_t)RS_TILE, n - base);
+  const bool full = tile_n == RS_TILE;
+  const uint32_t wl = (uint32_t)warp * RS_WARP_TILE + lane;  // tile-local index of item 0
 
   // Source / destination views.  ALT is always structure-of-arrays.
   const bool src_pairs = (src != BUF_ALT) && p.pairs;
@@ -232,51 +265,72 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_sort_pass(SortParams p, uint3
   const uint32_t *sval = src == BUF_IN ? p.in_ptr : (src == BUF_OUT ? p.out_ptr : p.alt_ptr);
   void *dkey = dst == BUF_OUT ? p.out : (void *)p.alt_key;
   uint32_t *dval = dst == BUF_OUT ? p.out_ptr : p.alt_ptr;
+  const uint32_t *skey32 = reinterpret_cast<const uint32_t *>(skey) + base;
+  const uint2 *skey64 = reinterpret_cast<const uint2 *>(skey) + base;
+  const uint32_t *sval32 = sval ? sval + base : nullptr;
+  const bool gen_vals = first && src == BUF_IN && sval == nullptr && !src_pairs;
+  const uint32_t vbase = (uint32_t)(p.ptr_base + base);
 
   // Load keys and values up front (all loads in flight together):
-  // warp-striped, item k of lane l is element wbase + 32k + l.
+  // warp-striped, item k of lane l is tile element wl + 32k.
   uint32_t key[RS_ITEMS];
   uint32_t val[HAS_VALS ? RS_ITEMS : 1];
-  const bool gen_vals = first && src == BUF_IN && sval == nullptr && !src_pairs;
 #pragma unroll
   for (int k = 0; k < RS_ITEMS; ++k) {
-    uint64_t i = wbase + (uint64_t)k * 32 + lane;
+    const uint32_t li = wl + 32u * k;
     key[k] = 0;
     if (HAS_VALS) val[k] = 0;
-    if (i < p.n) {
+    if (full || li < tile_n) {
       if (src_pairs) {
-        uint2 e = __ldcs(reinterpret_cast<const uint2 *>(skey) + i);
+        uint2 e = __ldcs(skey64 + li);
         key[k] = e.x;
         if (HAS_VALS) val[k] = e.y;
       } else {
-        key[k] = __ldcs(reinterpret_cast<const uint32_t *>(skey) + i);
-        if (HAS_VALS) val[k] = gen_vals ? (uint32_t)(p.ptr_base + i) : __ldcs(sval + i);
+        key[k] = __ldcs(skey32 + li);
+        if (HAS_VALS) val[k] = gen_vals ? vbase + li : __ldcs(sval32 + li);
       }
     }
   }
 
-  // Warp-level stable ranking.
+  // Warp-level stable ranking (match.any groups the lanes of one digit).
   uint32_t rank[RS_ITEMS];
   const uint32_t lt = (1u << lane) - 1u;
+  uint32_t *whist = s_whist[warp];
+  if (full) {
 #pragma unroll
-  for (int k = 0; k < RS_ITEMS; ++k) {
-    uint64_t i = wbase + (uint64_t)k * 32 + lane;
-    const bool valid = i < p.n;
-    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-    rank[k] = 0;
-    if (valid) {
-      uint32_t d = digit_of(key[k], p, pass);
-      unsigned peers = __match_any_sync(vmask, d);
-      int leader = __ffs(peers) - 1;
+    for (int k = 0; k < RS_ITEMS; ++k) {
+      const uint32_t d = dig(key[k]);
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const int leader = __ffs(peers) - 1;
       uint32_t old = 0;
       if (lane == leader) {
-        old = s_whist[warp][d];
-        s_whist[warp][d] = old + __popc(peers);
+        old = whist[d];
+        whist[d] = old + __popc(peers);
       }
-      old = __shfl_sync(vmask, old, leader);
+      old = __shfl_sync(0xffffffffu, old, leader);
       rank[k] = old + __popc(peers & lt);
+      __syncwarp();
     }
-    __syncwarp();
+  } else {
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+      const bool valid = wl + 32u * k < tile_n;
+      const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+      rank[k] = 0;
+      if (valid) {
+        const uint32_t d = dig(key[k]);
+        const unsigned peers = __match_any_sync(vmask, d);
+        const int leader = __ffs(peers) - 1;
+        uint32_t old = 0;
+        if (lane == leader) {
+          old = whist[d];
+          whist[d] = old + __popc(peers);
+        }
+        old = __shfl_sync(vmask, old, leader);
+        rank[k] = old + __popc(peers & lt);
+      }
+      __syncwarp();
+    }
   }
   __syncthreads();
 
@@ -296,7 +350,7 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_sort_pass(SortParams p, uint3
   const uint32_t dstart = block_exclusive_scan(count, s_warp, nullptr);
   s_dstart[d] = dstart;
 
-  uint64_t excl = 0;
+  uint32_t excl = 0;
   if (tile > 0) {
     int64_t t = (int64_t)tile - 1;
     uint32_t spins = 0;
@@ -313,36 +367,45 @@ __global__ void __launch_bounds__(RS_THREADS, 3) k_sort_pass(SortParams p, uint3
       if (flag == RS_FLAG_INC) break;
       --t;
     }
-    pd_store_release_u32(st + tile * RS_RADIX, RS_FLAG_INC | (uint32_t)((excl + count) & RS_COUNT_MASK));
+    pd_store_release_u32(st + tile * RS_RADIX, RS_FLAG_INC | ((excl + count) & RS_COUNT_MASK));
   }
-  s_gdelta[d] = (long long)(p.offsets[pass * RS_RADIX + d] + excl) - (long long)dstart;
+  s_gdelta[d] = (int32_t)(p.offsets[pass * RS_RADIX + d] + excl) - (int32_t)dstart;
   __syncthreads();
 
   // Stage the tile in digit order.
 #pragma unroll
   for (int k = 0; k < RS_ITEMS; ++k) {
-    uint64_t i = wbase + (uint64_t)k * 32 + lane;
-    if (i < p.n) {
-      uint32_t dg = digit_of(key[k], p, pass);
-      uint32_t pos = s_dstart[dg] + s_whist[warp][dg] + rank[k];
+    if (full || wl + 32u * k < tile_n) {
+      const uint32_t dg = dig(key[k]);
+      const uint32_t pos = s_dstart[dg] + whist[dg] + rank[k];
       s_keys[pos] = key[k];
       if (HAS_VALS) s_vals[pos] = val[k];
     }
   }
   __syncthreads();
 
-  // Write each digit run contiguously.
-  const uint32_t tile_n = (uint32_t)min((uint64_t)RS_TILE, p.n - base);
+  // Write each digit run contiguously (global index < 2^30).
+  uint32_t *dkey32 = reinterpret_cast<uint32_t *>(dkey);
+  uint2 *dkey64 = reinterpret_cast<uint2 *>(dkey);
+#pragma unroll 4
   for (uint32_t i = tid; i < tile_n; i += RS_THREADS) {
-    uint32_t k = s_keys[i];
-    uint64_t g = (uint64_t)(s_gdelta[digit_of(k, p, pass)] + (long long)i);
+    const uint32_t k = s_keys[i];
+    const uint32_t g = (uint32_t)(s_gdelta[dig(k)] + (int32_t)i);
     if (dst_pairs) {
-      reinterpret_cast<uint2 *>(dkey)[g] = make_uint2(k, HAS_VALS ? s_vals[i] : 0u);
+      dkey64[g] = make_uint2(k, HAS_VALS ? s_vals[i] : 0u);
     } else {
-      reinterpret_cast<uint32_t *>(dkey)[g] = k;
+      dkey32[g] = k;
       if (HAS_VALS) dval[g] = s_vals[i];
     }
   }
+}
+
+using PassKernel = void (*)(SortParams, uint32_t, uint32_t, uint32_t);
+PassKernel pick_pass(bool vals, int key_mode) {
+  if (key_mode == PD_KEY_HASH0) return vals ? k_sort_pass<true, PD_KEY_HASH0> : k_sort_pass<false, PD_KEY_HASH0>;
+  if (key_mode == PD_KEY_MULHASH)
+    return vals ? k_sort_pass<true, PD_KEY_MULHASH> : k_sort_pass<false, PD_KEY_MULHASH>;
+  return vals ? k_sort_pass<true, PD_KEY_PLAIN> : k_sort_pass<false, PD_KEY_PLAIN>;
 }
 
 struct SortLayout {
@@ -392,6 +455,13 @@ int pd_sort_with_workspace(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, vo
 // receives the device address of the exclusive digit offsets of pass 0.
 int pd_sort_ex(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
                cudaStream_t s, uint32_t **offsets_out) {
+  return pd_sort_ex2(ctx, a, key_mode, ws, s, offsets_out, nullptr);
+}
+
+// Same, with the element count read on the device from *n_dev (a->nr_elements
+// is then an upper bound that sizes the workspace and the grids).
+int pd_sort_ex2(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
+                cudaStream_t s, uint32_t **offsets_out, const uint64_t *n_dev) {
   SortLayout l;
   if (!sort_layout(a, &l)) return PIMDAL_ERR_ARG;
   if (offsets_out) *offsets_out = (uint32_t *)((char *)ws + l.off_offsets);
@@ -408,6 +478,7 @@ int pd_sort_ex(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, 
   p.alt_key = (uint32_t *)(w + l.off_alt_key);
   p.alt_ptr = (uint32_t *)(w + l.off_alt_ptr);
   p.n = a->nr_elements;
+  p.n_dev = n_dev;
   p.flip = a->key_dtype == PIMDAL_I32 ? 0x80000000u : 0u;
   p.key_mode = key_mode;
   p.begin_bit = a->begin_bit;
@@ -426,7 +497,9 @@ int pd_sort_ex(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, 
       (unsigned)std::min<uint64_t>(pd_ceil_div(p.n, (uint64_t)RS_THREADS * 16), (uint64_t)ctx->sm_count * 4);
   {
     pd_launch_scope sc(ctx, PIMDAL_KERNEL_SORT_HIST, s);
-    k_sort_hist<<<hist_blocks ? hist_blocks : 1, RS_THREADS, 0, s>>>(p);
+    auto hk = key_mode == PD_KEY_HASH0 ? k_sort_hist<PD_KEY_HASH0>
+              : key_mode == PD_KEY_MULHASH ? k_sort_hist<PD_KEY_MULHASH> : k_sort_hist<PD_KEY_PLAIN>;
+    hk<<<hist_blocks ? hist_blocks : 1, RS_THREADS, 0, s>>>(p);
   }
   {
     pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
@@ -439,8 +512,11 @@ int pd_sort_ex(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, 
   }
   for (uint32_t q = 0; q < l.npasses; ++q) {
     pd_launch_scope sc(ctx, PIMDAL_KERNEL_SORT_PASS, s);
-    if (p.has_vals) k_sort_pass<true><<<(unsigned)l.tiles, RS_THREADS, 0, s>>>(p, q);
-    else k_sort_pass<false><<<(unsigned)l.tiles, RS_THREADS, 0, s>>>(p, q);
+    const uint32_t shift = p.begin_bit + q * RS_RADIX_BITS;
+    const uint32_t bits = std::min<uint32_t>(RS_RADIX_BITS, p.end_bit - shift);
+    const uint32_t mask = (1u << bits) - 1u;
+    auto k = pick_pass(p.has_vals != 0, key_mode);
+    k<<<(unsigned)l.tiles, RS_THREADS, 0, s>>>(p, q, shift, mask);
   }
   return pd_launch_status(ctx);
 }
@@ -452,6 +528,8 @@ extern "C" int pimdal_sort_kernel(pimdal_ctx_t *ctx, const pimdal_sort_arguments
   if (a->key_dtype != PIMDAL_I32 && a->key_dtype != PIMDAL_U32) return PIMDAL_ERR_ARG;
   if (a->nr_elements == 0) return PIMDAL_OK;
   if (!a->in || !a->out || a->in == a->out) return PIMDAL_ERR_ARG;
+  if (a->layout == PIMDAL_LAYOUT_PAIRS && (((uintptr_t)a->in | (uintptr_t)a->out) & 7u))
+    return PIMDAL_ERR_ARG;  // key_ptr32 pairs are accessed as 8-byte words
   if (a->layout == PIMDAL_LAYOUT_COLUMNS && a->out_ptr && a->in_ptr == a->out_ptr)
     return PIMDAL_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;

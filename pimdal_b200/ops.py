@@ -295,3 +295,31 @@ def hash_join(ctx: Context, build_key, build_payload, probe_key, probe_ptr=None,
     L.check(ctx.lib.pimdal_hash_join(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
             "pimdal_hash_join")
     return result, out_payload, out_row
+
+
+# ---------------------------------------------------------------------------
+# Group-by (group_kernel, pimdal/aggregate/aggregate.h:25)
+# ---------------------------------------------------------------------------
+def group_kernel(ctx: Context, keys, vals=None, *, method: int = L.GROUP_HASH,
+                 key_dtype: int = L.I32, expected_groups: int = 0, capacity: int | None = None,
+                 want=("sum", "count", "min", "max"), outs=None, result=None, stream=None):
+    """Group-by with exact int64 aggregates, groups ascending by key.
+    Returns (result, out_key, {name: column})."""
+    dev = keys.device
+    n = keys.numel()
+    if capacity is None:
+        capacity = max(1, min(n, expected_groups * 2 if expected_groups else n))
+    if outs is None:
+        outs = {w: torch.empty(capacity, dtype=torch.int64, device=dev) for w in want}
+        outs["key"] = torch.empty(capacity, dtype=torch.int32, device=dev)
+    if result is None:
+        result = torch.empty(1, dtype=torch.int64, device=dev)
+    a = L.AggrArguments(size=n, in_=_ptr(keys), in_val=_ptr(vals), out=_ptr(outs.get("key")),
+                        out_sum=_ptr(outs.get("sum")), out_count=_ptr(outs.get("count")),
+                        out_min=_ptr(outs.get("min")), out_max=_ptr(outs.get("max")),
+                        out_capacity=capacity, expected_groups=expected_groups,
+                        key_dtype=key_dtype, method=method)
+    _workspace(ctx, ctx.lib.pimdal_group_workspace_size, a)
+    L.check(ctx.lib.pimdal_group_kernel(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
+            "pimdal_group_kernel")
+    return result, outs
