@@ -196,6 +196,20 @@ int pimdal_sel_workspace_size(const pimdal_sel_arguments_t *args, size_t *bytes)
 int pimdal_sel_kernel(pimdal_ctx_t *ctx, const pimdal_sel_arguments_t *args,
                       pimdal_sel_results_t *d_result, pimdal_stream_t stream);
 
+/* Selection that allocates nothing -- no counterpart in the reference.  For
+ * callers that cannot call cudaMalloc (a host whose memory manager owns every
+ * device allocation, code running during stream capture, latency-critical
+ * paths): no context is needed, the caller passes only its own input, output
+ * and result buffers.  Same arguments and results as pimdal_sel_kernel, on
+ * the current device.  Scratch is a fixed 32 KiB device array inside the
+ * library, so at most 2^29 rows per call with 16-byte-aligned input (2^24
+ * otherwise); larger calls return PIMDAL_ERR_WORKSPACE.  The first call on a
+ * device sets that array up (do it before any stream capture).  Calls share
+ * the array: calls that overlap on the GPU race and must not be issued.  A
+ * device-side failure sets d_result->t_count to UINT64_MAX. */
+int pimdal_sel_kernel_noalloc(const pimdal_sel_arguments_t *args, pimdal_sel_results_t *d_result,
+                              pimdal_stream_t stream);
+
 /* ------------------------------------------------------------------------- */
 /* Sort.  Replaces sort_part_kernel + sort_kernel (pimdal/sort/sort.h:7-25,  */
 /* sort_keyval.c:114-179) and the CPU sort_kernel of                          */

@@ -145,6 +145,7 @@ SIGNATURES = {
     "pimdal_gen_column": (_I, [_VP, C.POINTER(GenSpec), _VP, _U64, _U64, _VP]),
     "pimdal_sel_workspace_size": (_I, [C.POINTER(SelArguments), C.POINTER(_SZ)]),
     "pimdal_sel_kernel": (_I, [_VP, C.POINTER(SelArguments), _VP, _VP]),
+    "pimdal_sel_kernel_noalloc": (_I, [C.POINTER(SelArguments), _VP, _VP]),
     "pimdal_sort_workspace_size": (_I, [C.POINTER(SortArguments), C.POINTER(_SZ)]),
     "pimdal_sort_kernel": (_I, [_VP, C.POINTER(SortArguments), _VP]),
     "pimdal_smj_merge_workspace_size": (_I, [C.POINTER(SmjMergeArguments), C.POINTER(_SZ)]),

@@ -17,6 +17,7 @@
 // stores.  The create_ptr / out_val glue is fused: row ids are generated
 // (ptr_base + index) unless a row-id column is given.
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -571,4 +572,155 @@ extern "C" int pimdal_sel_kernel(pimdal_ctx_t *ctx, const pimdal_sel_arguments_t
     k<<<(unsigned)tiles, SEL_THREADS, 0, s>>>(p);
   }
   return pd_launch_status(ctx);
+}
+
+// ---------------------------------------------------------------------------
+// pimdal_sel_kernel_noalloc: selection for callers that cannot allocate
+// device memory.
+//
+// Some hosts of this operator may not call cudaMalloc at all: code running
+// under a memory manager that owns every device allocation (a database
+// buffer pool or a framework's caching allocator), code called while a CUDA
+// graph is being captured, or a real-time path where an allocation could
+// block.  pimdal_sel_kernel needs a pimdal_ctx, and creating one allocates.
+// This entry point needs nothing but the caller's input, output and result
+// buffers: its scratch (look-back status words, the chunk claim counters and
+// an error word) is the file-scope device array below, which every GPU that
+// loads this library holds until the process exits.
+//
+// Limits and rules:
+//  * The scratch holds SEL_NA_STATUS_WORDS = 4096 look-back words, so a call
+//    handles at most 4096 tiles or chunks: up to 2^29 rows when the input
+//    (and row-id column) is 16-byte aligned, up to 2^24 rows otherwise.
+//    Larger inputs are rejected with PIMDAL_ERR_WORKSPACE before anything is
+//    launched.
+//  * The first call on a device looks up the array's device address
+//    (cudaGetSymbolAddress) and clears it; make that first call before any
+//    stream capture.
+//  * All calls on one device share the array and it keeps the last call's
+//    contents: the status words carry a per-call epoch, the counters reset
+//    themselves, and the error word is cleared after every call.  Calls that
+//    overlap on the GPU (different streams, no ordering between them) race on
+//    the array and must not be issued; calls ordered on one stream are fine.
+//  * A device-side failure (a bounded wait that gave up) is reported by
+//    writing UINT64_MAX into d_result->t_count.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr uint32_t SEL_NA_STATUS_WORDS = 4096;
+constexpr uint32_t SEL_NA_WORDS = SEL_NA_STATUS_WORDS + 8;  // + error word, claim counters
+static __device__ __align__(256) uint64_t g_sel_noalloc_scratch[SEL_NA_WORDS];
+
+struct SelNaDevice {
+  bool ready = false;
+  uint64_t *scratch = nullptr;  // device address of g_sel_noalloc_scratch
+  uint32_t epoch = 0;
+  int sm_count = 0;
+};
+constexpr int SEL_NA_MAX_DEVICES = 64;
+SelNaDevice g_sel_na[SEL_NA_MAX_DEVICES];
+std::mutex g_sel_na_mutex;
+
+// Turns a recorded device error into the UINT64_MAX count, then clears the
+// error word and the claim counters for the next call.
+__global__ void k_sel_na_finish(uint64_t *scratch, uint64_t *d_count) {
+  uint32_t *words = reinterpret_cast<uint32_t *>(scratch + SEL_NA_STATUS_WORDS);
+  if (words[0]) *d_count = ~0ull;
+  words[0] = 0;
+  words[2] = 0;
+  words[3] = 0;
+}
+}  // namespace
+
+extern "C" int pimdal_sel_kernel_noalloc(const pimdal_sel_arguments_t *a,
+                                         pimdal_sel_results_t *d_result, pimdal_stream_t stream) {
+  if (!a || !d_result) return PIMDAL_ERR_ARG;
+  if (a->layout != PIMDAL_LAYOUT_COLUMNS && a->layout != PIMDAL_LAYOUT_PAIRS) return PIMDAL_ERR_ARG;
+  if (a->key_dtype != PIMDAL_I32 && a->key_dtype != PIMDAL_U32) return PIMDAL_ERR_ARG;
+  if (a->size && (!a->in || !a->out)) return PIMDAL_ERR_ARG;
+  if (a->layout == PIMDAL_LAYOUT_PAIRS && (((uintptr_t)a->in | (uintptr_t)a->out) & 7u))
+    return PIMDAL_ERR_ARG;
+  SelParams p{};
+  int64_t lo, hi;
+  if (!pd_pred_interval(a->pred, &lo, &hi, &p.invert)) return PIMDAL_ERR_ARG;
+  const int64_t tmin = a->key_dtype == PIMDAL_I32 ? INT32_MIN : 0;
+  const int64_t tmax = a->key_dtype == PIMDAL_I32 ? INT32_MAX : (int64_t)UINT32_MAX;
+  lo = std::max(lo, tmin);
+  hi = std::min(hi, tmax);
+  if (lo > hi) {
+    p.lo32 = 0;
+    p.range32 = 0xFFFFFFFFu;
+    p.invert ^= 1u;
+  } else {
+    p.lo32 = (uint32_t)lo;
+    p.range32 = (uint32_t)(hi - lo);
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= SEL_NA_MAX_DEVICES)
+    return PIMDAL_ERR_CUDA;
+
+  std::lock_guard<std::mutex> lock(g_sel_na_mutex);
+  SelNaDevice &d = g_sel_na[dev];
+  if (!d.ready) {
+    // One-time set-up on this device (must not run inside stream capture).
+    void *addr = nullptr;
+    if (cudaGetSymbolAddress(&addr, g_sel_noalloc_scratch) != cudaSuccess || !addr) {
+      cudaGetLastError();
+      return PIMDAL_ERR_CUDA;
+    }
+    if (cudaDeviceGetAttribute(&d.sm_count, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+      return PIMDAL_ERR_CUDA;
+    PD_CHECK_CUDA(cudaMemsetAsync(addr, 0, sizeof(uint64_t) * SEL_NA_WORDS, s));
+    d.scratch = (uint64_t *)addr;
+    d.ready = true;
+  }
+  if (a->size == 0) {
+    PD_CHECK_CUDA(cudaMemsetAsync(d_result, 0, sizeof(uint64_t), s));
+    return PIMDAL_OK;
+  }
+  p.in = a->in;
+  p.in_ptr = a->layout == PIMDAL_LAYOUT_COLUMNS ? a->in_ptr : nullptr;
+  p.ptr_base = a->ptr_base;
+  p.out = a->out;
+  p.out_ptr = a->layout == PIMDAL_LAYOUT_COLUMNS ? a->out_ptr : nullptr;
+  p.n = a->size;
+  p.vec_ok = ((((uintptr_t)a->in) | (uintptr_t)(p.in_ptr)) & 15u) == 0;
+  p.status = d.scratch;
+  p.d_error = reinterpret_cast<uint32_t *>(d.scratch + SEL_NA_STATUS_WORDS);
+  p.d_count = &d_result->t_count;
+  const bool is_signed = a->key_dtype == PIMDAL_I32;
+  const bool chunked = p.vec_ok && a->size >= (1u << 20);
+  SlParams q{};
+  uint64_t words;
+  if (chunked) {
+    const uint64_t per_sm = pd_ceil_div(a->size, (uint64_t)d.sm_count);
+    q.chunk_elems = std::min<uint64_t>(SL_CHUNK_MAX, pd_align_up(per_sm, SL_TILE));
+    q.nchunks = pd_ceil_div(a->size, q.chunk_elems);
+    words = q.nchunks;
+  } else {
+    words = pd_ceil_div(a->size, SEL_TILE);
+  }
+  if (words > SEL_NA_STATUS_WORDS) return PIMDAL_ERR_WORKSPACE;  // beyond the fixed scratch
+
+  // Per-call epoch; stale status words are cleared when the 16-bit epoch wraps.
+  d.epoch = (d.epoch + 1) & 0xFFFFu;
+  if (d.epoch == 0) {
+    PD_CHECK_CUDA(cudaMemsetAsync(d.scratch, 0, sizeof(uint64_t) * SEL_NA_STATUS_WORDS, s));
+    d.epoch = 1;
+  }
+  p.epoch = d.epoch;
+  if (chunked) {
+    q.s = p;
+    q.claim = reinterpret_cast<uint32_t *>(d.scratch + SEL_NA_STATUS_WORDS) + 2;
+    const unsigned grid = (unsigned)std::min<uint64_t>(q.nchunks, (uint64_t)d.sm_count);
+    SlKernel k = pick_chunked(a->layout, is_signed, p.in_ptr != nullptr);
+    const int smem = SL_STAGES * SL_STAGE_BYTES;
+    PD_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k<<<grid, SL_THREADS, smem, s>>>(q);
+  } else {
+    SelKernel k = pick_kernel(a->layout, is_signed, p.in_ptr != nullptr);
+    k<<<(unsigned)words, SEL_THREADS, 0, s>>>(p);
+  }
+  k_sel_na_finish<<<1, 1, 0, s>>>(d.scratch, p.d_count);
+  return cudaGetLastError() == cudaSuccess ? PIMDAL_OK : PIMDAL_ERR_CUDA;
 }
