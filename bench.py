@@ -279,18 +279,50 @@ class SortSmjWorkload(Workload):
         self._run(self.ku, self.rows, self.kz, self.rk, self.rp, self.sk, self.sp)
 
     def step_e2e(self, stream):
-        for d, h in zip(self.d_in2, self.h_in):
-            d.copy_(h, non_blocking=True)
-        self._run(*self.d_in2)
-        for h, d in zip(self.h_out, (self.ou, self.oup, self.oz, self.ozp, self.ji, self.jo)):
-            h.copy_(d, non_blocking=True)
+        """Pinned host inputs -> device -> pinned host outputs through the public
+        API, pipelined over three streams ordered by events: the upload of an
+        operator's inputs, the previous operator's compute and the download of
+        an earlier operator's outputs overlap (PCIe is full duplex)."""
+        import torch
+        if not hasattr(self, "_streams"):
+            self._streams = [torch.cuda.Stream() for _ in range(3)]
+        up, comp, down = self._streams
+        ops, ctx, d = self.ops, self.ctx, self.d_in2
+        start = torch.cuda.Event()
+        start.record(stream)
+        for s in self._streams:
+            s.wait_event(start)
+        outs = (self.ou, self.oup, self.oz, self.ozp, self.ji, self.jo)
+        plan = [((0, 1), (0, 1)), ((2,), (2, 3)), ((3, 4, 5, 6), (4, 5))]
+        for g, (ins, outs_idx) in enumerate(plan):
+            with torch.cuda.stream(up):
+                for i in ins:
+                    d[i].copy_(self.h_in[i], non_blocking=True)
+            e_in = torch.cuda.Event()
+            e_in.record(up)
+            comp.wait_event(e_in)
+            if g == 0:
+                ops.sort_kernel(ctx, d[0], d[1], out=self.ou, out_ptr=self.oup, stream=comp)
+            elif g == 1:
+                ops.sort_kernel(ctx, d[2], d[1], out=self.oz, out_ptr=self.ozp, stream=comp)
+            else:
+                ops.sort_merge_join(ctx, d[3], d[4], d[5], d[6], out_inner=self.ji,
+                                    out_outer=self.jo, result=self.res, stream=comp)
+            e_c = torch.cuda.Event()
+            e_c.record(comp)
+            down.wait_event(e_c)
+            with torch.cuda.stream(down):
+                for o in outs_idx:
+                    self.h_out[o].copy_(outs[o], non_blocking=True)
+        end = torch.cuda.Event()
+        end.record(down)
+        stream.wait_event(end)
         h2d = sum(t.numel() * 4 for t in self.h_in)
         d2h = sum(t.numel() * 4 for t in self.h_out)
         return h2d, d2h
 
-    def roofline_bytes(self, launches: int) -> float:
+    def roofline_bytes(self, launches: int, steps: int) -> float:
         """Algorithmic bytes of all digit-pass launches of the timed region."""
-        steps = launches / 16  # 4 + 4 + 4 + 4 pass launches per step
         return self.pass_bytes * steps
 
     def algorithmic_bytes_per_launch(self):
@@ -328,7 +360,188 @@ class SortSmjWorkload(Workload):
                                  f"racy with >1 thread) on 2^21 x 8384000 keys, x{reps}")
 
 
-WORKLOADS = {"select": SelectWorkload, "sort_smj": SortSmjWorkload}
+class HashJoinWorkload(Workload):
+    """Hash join: build 2^25 unique int32 keys (a seeded sample of [0, 2^26))
+    with int32 payloads, probe 2^28 int32 keys at a 50% match rate, uniform
+    and Zipf(0.75) probe variants.  One step runs both joins."""
+    name = "hash_join"
+    NB = 1 << 25
+    NP = 1 << 28
+
+    def __init__(self):
+        from pimdal_b200 import _lib as L
+        from pimdal_b200 import gen
+        self.L = L
+        s = 0xB200 + 2
+        self.spec_bk = gen.Spec(L.GEN_PERM, L.I32, seed=s, perm_domain=2 * self.NB)
+        self.spec_bp = gen.Spec(L.GEN_UNIFORM, L.I32, seed=s, stream_id=1, lo=-2**31, hi=2**31 - 1)
+        self.spec_pu = gen.Spec(L.GEN_PROBE, L.I32, seed=s, stream_id=2, lo=self.NB,
+                                perm_domain=2 * self.NB, match_permille=500)
+        self.spec_pz = gen.Spec(L.GEN_PROBE, L.I32, seed=s, stream_id=3, lo=self.NB,
+                                perm_domain=2 * self.NB, match_permille=500)
+        self.config = {"workload": "hash join build 2^25 unique int32 keys + int32 payload, "
+                                   "probe 2^28 int32 keys at 50% match, uniform and Zipf(0.75)",
+                       "build_rows": self.NB, "probe_rows": self.NP,
+                       "l2": "inputs larger than L2; L2 also flushed between steps"}
+        self.rows_per_step = 2 * (self.NB + self.NP)
+        self.dominant = L.KERNEL_HJ_PROBE
+        self.dominant_name = "k_hj_probe"
+
+    def setup(self, ctx, dev):
+        import torch
+        from pimdal_b200 import gen, ops
+        self.ctx, self.ops = ctx, ops
+        self.spec_pz.cdf = gen.zipf_cdf(self.NB, 0.75)
+        g = lambda spec, n: ops.gen_column(ctx, spec, n)
+        self.bk, self.bp = g(self.spec_bk, self.NB), g(self.spec_bp, self.NB)
+        self.pu, self.pz = g(self.spec_pu, self.NP), g(self.spec_pz, self.NP)
+        e = lambda n: torch.empty(n, dtype=torch.int32, device=dev)
+        self.op, self.orow = e(self.NP), e(self.NP)
+        self.res = [torch.empty(1, dtype=torch.int64, device=dev) for _ in range(2)]
+        self.step()
+        ctx.sync()
+        self.matches = [int(r.item()) for r in self.res]
+        pin = lambda t: t.cpu().pin_memory()
+        self.h_in = [pin(t) for t in (self.bk, self.bp, self.pu, self.pz)]
+        self.d_in2 = [torch.empty_like(t) for t in (self.bk, self.bp, self.pu, self.pz)]
+        self.h_out = [torch.empty(self.NP, dtype=torch.int32).pin_memory() for _ in range(2)]
+
+    def _run(self, bk, bp, pu, pz):
+        for i, pk in enumerate((pu, pz)):
+            self.ops.hash_join(self.ctx, bk, bp, pk, capacity=self.NP, out_payload=self.op,
+                               out_row=self.orow, result=self.res[i])
+
+    def step(self):
+        self._run(self.bk, self.bp, self.pu, self.pz)
+
+    def step_e2e(self, stream):
+        for d, h in zip(self.d_in2, self.h_in):
+            d.copy_(h, non_blocking=True)
+        self._run(*self.d_in2)
+        k = self.matches[1]
+        self.h_out[0][:k].copy_(self.op[:k], non_blocking=True)
+        self.h_out[1][:k].copy_(self.orow[:k], non_blocking=True)
+        return sum(t.numel() * 4 for t in self.h_in), 8 * k + 16
+
+    def roofline_bytes(self, launches: int, steps: int) -> float:
+        # all probe launches of a step: 4 B per probe row + 8 B per match
+        return steps * sum(4 * self.NP + 8 * m for m in self.matches)
+
+    def algorithmic_bytes_per_launch(self):
+        return sum(4 * self.NP + 8 * m for m in self.matches)
+
+    def cpu_sample(self, ref, threads, budget_s):
+        from pimdal_b200 import gen
+        if not hasattr(self, "_cpu"):
+            nb, npr = self.NB // 16, self.NP // 16
+            bk = gen.generate_cpu(gen.Spec(self.L.GEN_PERM, self.L.I32, seed=9, perm_domain=2 * nb), nb)
+            bp = gen.generate_cpu(self.spec_bp, nb)
+            pk = gen.generate_cpu(gen.Spec(self.L.GEN_PROBE, self.L.I32, seed=9, stream_id=2, lo=nb,
+                                           perm_domain=2 * nb, match_permille=500), npr)
+            self._cpu = (bk, bp, pk, nb + npr)
+            ref.set_threads("hash_join", threads)
+        bk, bp, pk, rows = self._cpu
+        reps = 0
+        t0 = time.perf_counter()
+        while reps < 1 or time.perf_counter() - t0 < budget_s:
+            ref.hash_join(bk, bp, pk)
+            reps += 1
+        return rows * reps, time.perf_counter() - t0, (
+            f"reference partition + join_partitions (hash_join.cpp:57-157) on 2^21 build x "
+            f"2^24 probe rows (1/16 sample), x{reps}")
+
+
+class GroupByWorkload(Workload):
+    """Group-by over 2^28 rows (int32 key, int64 value U[100, 1e7]) at group
+    cardinality 16, 2^12 and 2^22, hash and sort methods: one step runs the
+    six group-bys."""
+    name = "group_by"
+    N = 1 << 28
+    CARDS = (16, 1 << 12, 1 << 22)
+
+    def __init__(self):
+        from pimdal_b200 import _lib as L
+        from pimdal_b200 import gen
+        self.L = L
+        s = 0xB200 + 3
+        self.spec_k = [gen.Spec(L.GEN_PERM_UNIFORM, L.I32, seed=s, stream_id=10 + i, lo=0, hi=c - 1,
+                                perm_domain=0) for i, c in enumerate(self.CARDS)]
+        self.spec_v = gen.Spec(L.GEN_UNIFORM, L.I64, seed=s, stream_id=1, lo=100, hi=10**7)
+        self.config = {"workload": "group-by 2^28 rows int32 key + int64 value U[100,1e7], "
+                                   "cardinality 16 / 2^12 / 2^22, hash and sort methods",
+                       "rows": self.N, "cardinalities": list(self.CARDS),
+                       "l2": "inputs larger than L2; L2 also flushed between steps"}
+        self.rows_per_step = 6 * self.N
+        self.dominant = L.KERNEL_GROUP
+        self.dominant_name = "k_gb_aggregate (hash method)"
+
+    def setup(self, ctx, dev):
+        import torch
+        from pimdal_b200 import gen, ops
+        self.ctx, self.ops = ctx, ops
+        self.keys = [ops.gen_column(ctx, sp, self.N) for sp in self.spec_k]
+        self.vals = ops.gen_column(ctx, self.spec_v, self.N)
+        cap = 2 * max(self.CARDS)
+        self.outs = {w: torch.empty(cap, dtype=torch.int64, device=dev)
+                     for w in ("sum", "count", "min", "max")}
+        self.outs["key"] = torch.empty(cap, dtype=torch.int32, device=dev)
+        self.res = torch.empty(1, dtype=torch.int64, device=dev)
+        self.step()
+        ctx.sync()
+        pin = lambda t: t.cpu().pin_memory()
+        self.h_in = [pin(t) for t in self.keys] + [pin(self.vals)]
+        self.d_in2 = [torch.empty_like(t) for t in self.keys] + [torch.empty_like(self.vals)]
+        self.h_cnt = torch.empty(1, dtype=torch.int64).pin_memory()
+        self.h_sum = torch.empty(max(self.CARDS), dtype=torch.int64).pin_memory()
+
+    def _run(self, keys, vals):
+        for k, c in zip(keys, self.CARDS):
+            for m in (self.L.GROUP_HASH, self.L.GROUP_SORT):
+                self.ops.group_kernel(self.ctx, k, vals, method=m, expected_groups=c,
+                                      capacity=2 * max(self.CARDS), outs=self.outs,
+                                      result=self.res)
+
+    def step(self):
+        self._run(self.keys, self.vals)
+
+    def step_e2e(self, stream):
+        for d, h in zip(self.d_in2, self.h_in):
+            d.copy_(h, non_blocking=True)
+        self._run(self.d_in2[:3], self.d_in2[3])
+        g = max(self.CARDS)
+        self.h_cnt.copy_(self.res, non_blocking=True)
+        self.h_sum[:g].copy_(self.outs["sum"][:g], non_blocking=True)
+        return sum(t.numel() * t.element_size() for t in self.h_in), 8 + 8 * g
+
+    def roofline_bytes(self, launches: int, steps: int) -> float:
+        # hash-method aggregation launches: 12 B per row (key + value)
+        return launches * 12 * self.N
+
+    def algorithmic_bytes_per_launch(self):
+        return 12 * self.N
+
+    def cpu_sample(self, ref, threads, budget_s):
+        from pimdal_b200 import gen
+        if not hasattr(self, "_cpu"):
+            n = self.N // 64
+            ks = [gen.generate_cpu(sp, n) for sp in self.spec_k]
+            v = gen.generate_cpu(self.spec_v, n)
+            self._cpu = (ks, v, 3 * n)
+            ref.set_threads("aggregate", threads)
+        ks, v, rows = self._cpu
+        reps = 0
+        t0 = time.perf_counter()
+        while reps < 1 or time.perf_counter() - t0 < budget_s:
+            for k in ks:
+                ref.group_by(k, v)
+            reps += 1
+        return rows * reps, time.perf_counter() - t0, (
+            f"reference hash_table_aggregate (aggregate.cpp:40-83) with int64 SUM/COUNT/MIN/MAX "
+            f"on 2^22 rows x 3 cardinalities (1/64 sample), x{reps}")
+
+
+WORKLOADS = {"select": SelectWorkload, "sort_smj": SortSmjWorkload,
+             "hash_join": HashJoinWorkload, "group_by": GroupByWorkload}
 DEFAULT_WORKLOAD = "sort_smj"
 
 
@@ -443,7 +656,7 @@ def run_ours(args) -> None:
     roof = None
     if k_launches:
         if hasattr(wl, "roofline_bytes"):
-            total_b = wl.roofline_bytes(k_launches)
+            total_b = wl.roofline_bytes(k_launches, args.steps)
         else:
             total_b = wl.algorithmic_bytes_per_launch() * k_launches
         ach = total_b / (k_ms / 1e3) / 1e9

@@ -21,10 +21,13 @@
 //    are partitioned, and partition by partition one table buffer (reused, so
 //    it stays L2-resident and is never written back) is cleared, built and
 //    probed.  All partition bounds live on the device; no host sync.
-//  * Probing: persistent CTAs claim 2048-row tiles; a thread walks its 8 rows
-//    4 at a time in lockstep, reading the table in 32-byte groups of 4 slots
-//    (one sector per step, 4 sector loads in flight per thread; with no
-//    duplicate build key a walk stops at its first match); match counts are scanned and the tile's output
+//  * Bucketized linear probing: a key hashes to a bucket of 4 slots (one
+//    32-byte sector) and takes the first free slot of the first bucket, from
+//    there on, that has one; a lookup reads one sector and is done when the
+//    key is found (no duplicate build key) or the bucket has a free slot.
+//  * Probing: persistent CTAs claim 4096-row tiles of warp-striped rows; a
+//    thread walks 2 rows at a time in lockstep (their bucket loads in flight
+//    together); match counts are scanned and the tile's output
 //    offset resolved by a block-wide decoupled look-back that chains across
 //    the per-partition launches, so the output is in probe order within each
 //    partition, partitions in order.
@@ -36,13 +39,16 @@ namespace {
 
 constexpr uint64_t HJ_EMPTY = ~0ull;
 constexpr int HJ_THREADS = 256;
-constexpr int HJ_ITEMS = 8;
-constexpr int HJ_TILE = HJ_THREADS * HJ_ITEMS;  // 2048 probe rows per tile
+constexpr int HJ_ITEMS = 16;
+constexpr int HJ_TILE = HJ_THREADS * HJ_ITEMS;  // 4096 probe rows per tile
+constexpr int HJ_BATCH = 2;
 constexpr uint32_t HJ_MIN_BITS = 10;
 
-__device__ __forceinline__ uint64_t slot_of(uint32_t key, uint32_t part_bits, uint32_t bits) {
+// Home bucket of a key: buckets are aligned groups of 4 slots (one 32-byte
+// sector); a table of 2^bits slots has 2^(bits-2) buckets.
+__device__ __forceinline__ uint64_t bucket_of(uint32_t key, uint32_t part_bits, uint32_t bits) {
   const uint64_t h = (uint64_t)key * PD_GOLDEN64;
-  return (h << part_bits) >> (64 - bits);
+  return (h << part_bits) >> (64 - (bits - 2));
 }
 
 struct JoinParams {
@@ -109,86 +115,87 @@ __global__ void __launch_bounds__(256) k_hj_build(JoinParams p) {
       atomicAdd(p.side_count, 1u);
       continue;
     }
-    uint64_t s = slot_of(k, p.part_bits, p.bits);
+    // Bucketized linear probing: the first free slot of the first bucket
+    // (from the home bucket on) that has one.  Every copy of a key therefore
+    // lies between its home bucket and the first bucket with a free slot.
+    const uint64_t gmask = mask >> 2;
+    uint64_t g = bucket_of(k, p.part_bits, p.bits);
     bool done = false;
     bool dup = false;
-    for (uint64_t t = 0; t <= mask; ++t) {
-      const unsigned long long old = atomicCAS(p.table + s, HJ_EMPTY, e);
-      if (old == HJ_EMPTY) {
-        done = true;
-        break;
+    for (uint64_t t = 0; t <= gmask && !done; ++t) {
+      unsigned long long *b = p.table + 4 * g;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (done) break;
+        const unsigned long long cur = b[j];
+        if (cur != HJ_EMPTY) {
+          dup |= (uint32_t)cur == k;
+          continue;
+        }
+        const unsigned long long old = atomicCAS(b + j, HJ_EMPTY, e);
+        if (old == HJ_EMPTY) done = true;
+        else dup |= (uint32_t)old == k;
       }
-      dup |= (uint32_t)old == k;  // an equal key always lies on this key's probe path
-      s = (s + 1) & mask;
+      g = (g + 1) & gmask;
     }
     if (dup) *p.dup_flag = 1;
     if (!done) atomicOr(p.d_error, PD_DEVERR_TABLE_FULL);
   }
 }
 
-// Match walk of HJ_BATCH probe rows in lockstep.  The table is read in
-// aligned groups of 4 slots (one 32-byte sector): the walk of a row starts at
-// its slot inside the first group and ends at the first empty slot (or, when
-// the build saw no duplicate key, at the first match).  The loads of all
-// rows of the batch are issued before any is inspected.
-constexpr int HJ_BATCH = 4;
-
-__device__ __forceinline__ void walk_batch(const JoinParams &p, const uint32_t *key,
-                                           const bool *valid, bool stop_first, uint64_t mask,
-                                           uint32_t *cnt, uint32_t *first) {
-  uint64_t g[HJ_BATCH];
-  uint32_t off[HJ_BATCH];
-  bool active[HJ_BATCH];
+// Resolves one bucket of a probe row: adds its matches to *c (first payload
+// in *first) and returns true when the walk ends here -- the bucket has a free
+// slot, or (no duplicate build key) a match was found.
+__device__ __forceinline__ bool resolve_bucket(ulonglong2 lo, ulonglong2 hi, uint32_t key,
+                                               bool stop_first, uint32_t *c, uint32_t *first) {
+  const unsigned long long e[4] = {lo.x, lo.y, hi.x, hi.y};
+  bool has_empty = false;
 #pragma unroll
-  for (int i = 0; i < HJ_BATCH; ++i) {
-    const uint64_t s = slot_of(key[i], p.part_bits, p.bits);
-    g[i] = s & ~3ull;
-    off[i] = (uint32_t)(s & 3);
-    active[i] = valid[i];
-    cnt[i] = 0;
-    first[i] = 0;
-  }
-  const bool early = stop_first;
-  for (uint64_t round = 0; round <= (mask >> 2); ++round) {
-    ulonglong2 lo[HJ_BATCH], hi[HJ_BATCH];
-    bool any = false;
-#pragma unroll
-    for (int i = 0; i < HJ_BATCH; ++i) {
-      if (active[i]) {
-        const ulonglong2 *q = reinterpret_cast<const ulonglong2 *>(p.table + g[i]);
-        lo[i] = q[0];
-        hi[i] = q[1];
-        any = true;
-      }
-    }
-    if (!any) break;
-#pragma unroll
-    for (int i = 0; i < HJ_BATCH; ++i) {
-      if (!active[i]) continue;
-      const unsigned long long e[4] = {lo[i].x, lo[i].y, hi[i].x, hi[i].y};
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        if (!active[i] || (uint32_t)j < off[i]) continue;
-        if (e[j] == HJ_EMPTY) {
-          active[i] = false;
-        } else if ((uint32_t)e[j] == key[i]) {
-          if (cnt[i] == 0) first[i] = (uint32_t)(e[j] >> 32);
-          ++cnt[i];
-          if (early && key[i] != 0xFFFFFFFFu) active[i] = false;
-        }
-      }
-      off[i] = 0;
-      g[i] = (g[i] + 4) & mask;
+  for (int j = 0; j < 4; ++j) {
+    if (e[j] == HJ_EMPTY) {
+      has_empty = true;
+    } else if ((uint32_t)e[j] == key) {
+      if (*c == 0) *first = (uint32_t)(e[j] >> 32);
+      ++*c;
     }
   }
+  return has_empty || (stop_first && *c);
 }
 
-__global__ void __launch_bounds__(HJ_THREADS) k_hj_probe(JoinParams p) {
+// Writes every match of key (bucket walk from its home bucket) from output
+// position w on; returns the number of matches.
+__device__ __noinline__ uint32_t emit_all(const JoinParams &p, uint32_t key, uint64_t mask,
+                                          uint64_t w, uint32_t row, bool *overflow, bool emit) {
+  const uint64_t gmask = mask >> 2;
+  uint64_t g = bucket_of(key, p.part_bits, p.bits);
+  uint32_t c = 0;
+  for (uint64_t t = 0; t <= gmask; ++t) {
+    bool has_empty = false;
+    for (int j = 0; j < 4; ++j) {
+      const unsigned long long e = p.table[4 * g + j];
+      if (e == HJ_EMPTY) {
+        has_empty = true;
+      } else if ((uint32_t)e == key) {
+        if (emit) {
+          if (w < p.cap) { p.out_pay[w] = (uint32_t)(e >> 32); p.out_row[w] = row; } else *overflow = true;
+        }
+        ++w;
+        ++c;
+      }
+    }
+    if (has_empty) break;
+    g = (g + 1) & gmask;
+  }
+  return c;
+}
+
+__global__ void __launch_bounds__(HJ_THREADS, 3) k_hj_probe(JoinParams p) {
   __shared__ uint32_t s_warp[HJ_THREADS / 32];
   __shared__ uint32_t s_flags[2 * (HJ_THREADS / 32)];
   __shared__ uint64_t s_sum[HJ_THREADS / 32 + 1];
   __shared__ int s_state;
   __shared__ uint64_t s_tile, s_prefix;
+  __shared__ uint32_t s_first[HJ_ITEMS][HJ_THREADS];  // first payload of each row
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   uint64_t lo, hi;
@@ -198,6 +205,7 @@ __global__ void __launch_bounds__(HJ_THREADS) k_hj_probe(JoinParams p) {
   const uint64_t mask = (1ull << p.bits) - 1;
   const uint32_t side = *p.side_count;
   const bool stop_first = *p.dup_flag == 0;
+  const uint32_t lt = (1u << lane) - 1u;
 
   while (true) {
     if (tid == 0) {
@@ -212,38 +220,71 @@ __global__ void __launch_bounds__(HJ_THREADS) k_hj_probe(JoinParams p) {
     const uint64_t tl = s_tile;
     if (tl >= tiles) break;
     const uint64_t gtile = gbase + tl;
-    const uint64_t r0 = lo + tl * HJ_TILE + (uint64_t)tid * HJ_ITEMS;
+    // Warp-striped rows: row k of this lane is wbase + 32k + lane.
+    const uint64_t wbase = lo + tl * HJ_TILE + (uint64_t)warp * (32 * HJ_ITEMS);
 
-    // This thread's 8 consecutive probe rows, walked 4 at a time.
-    uint32_t key[HJ_ITEMS], first[HJ_ITEMS];
-    uint32_t one = 0, many = 0, mine = 0;  // bit j: row j has 1 / several matches
-#pragma unroll
-    for (int j = 0; j < HJ_ITEMS; ++j) key[j] = (r0 + j < hi) ? __ldcs(p.pkey + r0 + j) : 0u;
+    // Phase 1: match counts (4 bits per row, 15 = "count again") and first payloads.
+    uint64_t cnt4 = 0;
+    uint32_t mine = 0;
 #pragma unroll
     for (int b = 0; b < HJ_ITEMS; b += HJ_BATCH) {
-      bool valid[HJ_BATCH];
-      uint32_t cnt[HJ_BATCH];
-#pragma unroll
-      for (int i = 0; i < HJ_BATCH; ++i) valid[i] = r0 + b + i < hi;
-      walk_batch(p, key + b, valid, stop_first, mask, cnt, first + b);
+      uint32_t key[HJ_BATCH], c[HJ_BATCH], fk[HJ_BATCH];
+      uint64_t g[HJ_BATCH];
+      bool active[HJ_BATCH];
 #pragma unroll
       for (int i = 0; i < HJ_BATCH; ++i) {
-        const int j = b + i;
-        uint32_t c = cnt[i];
-        if (valid[i] && key[j] == 0xFFFFFFFFu) c += side;
-        if (c == 1 && key[j] != 0xFFFFFFFFu) one |= 1u << j;
-        else if (c) many |= 1u << j;
-        mine += c;
+        const uint64_t r = wbase + (uint64_t)(b + i) * 32 + lane;
+        active[i] = r < hi;
+        key[i] = active[i] ? __ldcs(p.pkey + r) : 0u;
+        g[i] = bucket_of(key[i], p.part_bits, p.bits);
+        c[i] = 0;
+        fk[i] = 0;
+      }
+      // Lockstep bucket walks: all loads of a round are in flight together;
+      // almost every row resolves in its home bucket.
+      const uint64_t gmask = mask >> 2;
+      for (uint64_t round = 0; round <= gmask; ++round) {
+        ulonglong2 glo[HJ_BATCH], ghi[HJ_BATCH];
+        bool any = false;
+#pragma unroll
+        for (int i = 0; i < HJ_BATCH; ++i) {
+          if (active[i]) {
+            const ulonglong2 *q = reinterpret_cast<const ulonglong2 *>(p.table + 4 * g[i]);
+            glo[i] = q[0];
+            ghi[i] = q[1];
+            any = true;
+          }
+        }
+        if (!any) break;
+#pragma unroll
+        for (int i = 0; i < HJ_BATCH; ++i) {
+          if (!active[i]) continue;
+          if (resolve_bucket(glo[i], ghi[i], key[i], stop_first && key[i] != 0xFFFFFFFFu, &c[i],
+                             &fk[i]))
+            active[i] = false;
+          g[i] = (g[i] + 1) & gmask;
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < HJ_BATCH; ++i) {
+        const int k = b + i;
+        const uint64_t r = wbase + (uint64_t)k * 32 + lane;
+        uint32_t ci = c[i];
+        if (r < hi && key[i] == 0xFFFFFFFFu) ci += side;
+        s_first[k][tid] = fk[i];
+        mine += ci;
+        cnt4 |= (uint64_t)(ci < 15 ? ci : 15u) << (4 * k);
       }
     }
-    // Block exclusive scan of per-thread match counts.
+    // Block scan of per-thread totals; tile look-back.
     uint32_t inc = mine;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
       if (lane >= o) inc += t;
     }
-    if (lane == 31) s_warp[warp] = inc;
+    const uint32_t wtot = __shfl_sync(0xffffffffu, inc, 31);
+    if (lane == 0) s_warp[warp] = wtot;
     __syncthreads();
     uint32_t wpre = 0, total = 0;
 #pragma unroll
@@ -252,7 +293,6 @@ __global__ void __launch_bounds__(HJ_THREADS) k_hj_probe(JoinParams p) {
       if (w < warp) wpre += x;
       total += x;
     }
-    const uint32_t excl = wpre + inc - mine;
     if (gtile == 0) {
       if (tid == 0) {
         pd_store_relaxed_u64(p.status, pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, total));
@@ -270,32 +310,51 @@ __global__ void __launch_bounds__(HJ_THREADS) k_hj_probe(JoinParams p) {
       }
     }
     __syncthreads();
-    uint64_t w = s_prefix + excl;
+    // Phase 2: rows in order (k-major, then lane) -> consecutive output slots.
+    uint64_t w = s_prefix + wpre;
     bool overflow = false;
 #pragma unroll
-    for (int j = 0; j < HJ_ITEMS; ++j) {
-      if (!(((one | many) >> j) & 1u)) continue;
-      const uint32_t row = p.prow ? p.prow[r0 + j] : (uint32_t)(r0 + j);
-      if ((one >> j) & 1u) {
-        if (w < p.cap) { p.out_pay[w] = first[j]; p.out_row[w] = row; } else overflow = true;
-        ++w;
-        continue;
-      }
-      // several matches (or the side-counted row): walk the chain again
-      uint64_t s = slot_of(key[j], p.part_bits, p.bits);
-      unsigned long long e = p.table[s];
-      for (uint64_t t = 0; t <= mask && e != HJ_EMPTY; ++t) {
-        if ((uint32_t)e == key[j]) {
-          if (w < p.cap) { p.out_pay[w] = (uint32_t)(e >> 32); p.out_row[w] = row; } else overflow = true;
-          ++w;
+    for (int k = 0; k < HJ_ITEMS; ++k) {
+      const uint32_t c4 = (uint32_t)(cnt4 >> (4 * k)) & 15u;
+      const uint64_t r = wbase + (uint64_t)k * 32 + lane;
+      const bool simple = c4 <= 1;
+      if (__all_sync(0xffffffffu, simple)) {
+        const unsigned m = __ballot_sync(0xffffffffu, c4 == 1);
+        if (c4 == 1) {
+          const uint64_t pos = w + __popc(m & lt);
+          const uint32_t row = p.prow ? p.prow[r] : (uint32_t)r;
+          if (pos < p.cap) { p.out_pay[pos] = s_first[k][tid]; p.out_row[pos] = row; } else overflow = true;
         }
-        s = (s + 1) & mask;
-        e = p.table[s];
-      }
-      if (key[j] == 0xFFFFFFFFu) {
-        for (uint32_t m = 0; m < side; ++m, ++w) {
-          if (w < p.cap) { p.out_pay[w] = 0xFFFFFFFFu; p.out_row[w] = row; } else overflow = true;
+        w += __popc(m);
+      } else {
+        // some lane has several matches: exact counts by a second walk
+        uint32_t c = 0;
+        const uint32_t key = (r < hi && c4) ? p.pkey[r] : 0u;
+        if (c4 == 1) c = 1;
+        else if (c4 > 1) {
+          bool dummy = false;
+          c = emit_all(p, key, mask, 0, 0, &dummy, false);  // count only
+          if (key == 0xFFFFFFFFu) c += side;
         }
+        uint32_t ci = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          uint32_t t = __shfl_up_sync(0xffffffffu, ci, o);
+          if (lane >= o) ci += t;
+        }
+        const uint64_t pos = w + ci - c;
+        const uint32_t row = c ? (p.prow ? p.prow[r] : (uint32_t)r) : 0u;
+        if (c4 == 1) {
+          if (pos < p.cap) { p.out_pay[pos] = s_first[k][tid]; p.out_row[pos] = row; } else overflow = true;
+        } else if (c) {
+          uint64_t q = pos + emit_all(p, key, mask, pos, row, &overflow, true);
+          if (key == 0xFFFFFFFFu) {
+            for (uint32_t m2 = 0; m2 < side; ++m2, ++q) {
+              if (q < p.cap) { p.out_pay[q] = 0xFFFFFFFFu; p.out_row[q] = row; } else overflow = true;
+            }
+          }
+        }
+        w += __shfl_sync(0xffffffffu, ci, 31);
       }
     }
     if (overflow) atomicOr(p.d_error, PD_DEVERR_CAPACITY);
@@ -516,7 +575,7 @@ extern "C" int pimdal_hash_kernel(pimdal_ctx_t *ctx, const pimdal_hash_arguments
                                   pimdal_stream_t stream) {
   if (!ctx || !a || !a->table_ptr || ((uintptr_t)a->table_ptr & 31u)) return PIMDAL_ERR_ARG;
   if (a->size && !a->in_key) return PIMDAL_ERR_ARG;
-  if (a->table_size < 2 || (a->table_size & (a->table_size - 1)) || a->size > a->table_size)
+  if (a->table_size < 16 || (a->table_size & (a->table_size - 1)) || a->size > a->table_size)
     return PIMDAL_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   cudaSetDevice(ctx->device);
@@ -548,7 +607,7 @@ extern "C" int pimdal_hj_probe(pimdal_ctx_t *ctx, const pimdal_probe_arguments_t
   if (!ctx || !a || !d_result || !a->table_ptr || ((uintptr_t)a->table_ptr & 31u)) return PIMDAL_ERR_ARG;
   if (a->size && !a->in_key) return PIMDAL_ERR_ARG;
   if (a->out_capacity && (!a->out_inner || !a->out_outer)) return PIMDAL_ERR_ARG;
-  if (a->table_size < 2 || (a->table_size & (a->table_size - 1)) || a->size >= (1ull << 32))
+  if (a->table_size < 16 || (a->table_size & (a->table_size - 1)) || a->size >= (1ull << 32))
     return PIMDAL_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   cudaSetDevice(ctx->device);

@@ -228,11 +228,12 @@ __device__ __forceinline__ uint32_t sort_xform(uint32_t k, uint32_t flip) {
 // One digit pass.  FULL tiles take a path without bounds checks; indices
 // inside a tile are 32-bit; the digit is (xform(key) >> shift) & mask.
 template <bool HAS_VALS, int KEY_MODE>
-__global__ void __launch_bounds__(RS_THREADS, 3)
+__global__ void __launch_bounds__(RS_THREADS, 4)
 k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   __shared__ uint32_t s_keys[RS_TILE];
   __shared__ uint32_t s_vals[HAS_VALS ? RS_TILE : 1];
-  __shared__ uint32_t s_whist[RS_WARPS][RS_RADIX];
+  __shared__ uint32_t s_whist[RS_WARPS][RS_RADIX];  // warp digit counts -> warp offsets
+  __shared__ uint16_t s_wcnt[RS_WARPS][RS_RADIX];   // running counters of the ranking (< 512)
   __shared__ uint32_t s_dstart[RS_RADIX];
   __shared__ int32_t s_gdelta[RS_RADIX];
   __shared__ uint32_t s_warp[RS_WARPS];
@@ -248,7 +249,10 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_tile = atomicAdd(&p.counters[pass], 1u);
 #pragma unroll
-  for (int w = 0; w < RS_WARPS; ++w) s_whist[w][tid] = 0;
+  for (int w = 0; w < RS_WARPS; ++w) {
+    s_whist[w][tid] = 0;
+    s_wcnt[w][tid] = 0;
+  }
   __syncthreads();
   const uint64_t tile = s_tile;
   const uint64_t base = tile * (uint64_t)RS_TILE;
@@ -292,49 +296,15 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
     }
   }
 
-  // Warp-level stable ranking (match.any groups the lanes of one digit).
-  uint32_t rank[RS_ITEMS];
-  const uint32_t lt = (1u << lane) - 1u;
-  uint32_t *whist = s_whist[warp];
-  if (full) {
+  // Early counts: per-warp digit histograms (one shared atomic per key), so
+  // the tile's counts are published before the ranking, and successors'
+  // look-backs find them without waiting.
 #pragma unroll
-    for (int k = 0; k < RS_ITEMS; ++k) {
-      const uint32_t d = dig(key[k]);
-      const unsigned peers = __match_any_sync(0xffffffffu, d);
-      const int leader = __ffs(peers) - 1;
-      uint32_t old = 0;
-      if (lane == leader) {
-        old = whist[d];
-        whist[d] = old + __popc(peers);
-      }
-      old = __shfl_sync(0xffffffffu, old, leader);
-      rank[k] = old + __popc(peers & lt);
-      __syncwarp();
-    }
-  } else {
-#pragma unroll
-    for (int k = 0; k < RS_ITEMS; ++k) {
-      const bool valid = wl + 32u * k < tile_n;
-      const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-      rank[k] = 0;
-      if (valid) {
-        const uint32_t d = dig(key[k]);
-        const unsigned peers = __match_any_sync(vmask, d);
-        const int leader = __ffs(peers) - 1;
-        uint32_t old = 0;
-        if (lane == leader) {
-          old = whist[d];
-          whist[d] = old + __popc(peers);
-        }
-        old = __shfl_sync(vmask, old, leader);
-        rank[k] = old + __popc(peers & lt);
-      }
-      __syncwarp();
-    }
-  }
+  for (int k = 0; k < RS_ITEMS; ++k)
+    if (full || wl + 32u * k < tile_n) atomicAdd(&s_whist[warp][dig(key[k])], 1u);
   __syncthreads();
 
-  // Per digit (thread tid = digit): warp offsets, tile count, publish, look-back.
+  // Per digit (thread tid = digit): warp offsets, tile count, publish.
   const int d = tid;
   uint32_t run = 0;
 #pragma unroll
@@ -345,29 +315,88 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   }
   const uint32_t count = run;
   uint32_t *st = p.status + ((uint64_t)pass * p.tiles) * RS_RADIX + d;
-  if (tile == 0) pd_store_release_u32(st, RS_FLAG_INC | count);
-  else pd_store_release_u32(st + tile * RS_RADIX, RS_FLAG_AGG | count);
+  if (tile == 0) pd_store_relaxed_u32(st, RS_FLAG_INC | count);
+  else pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_AGG | count);
   const uint32_t dstart = block_exclusive_scan(count, s_warp, nullptr);
   s_dstart[d] = dstart;
 
+  // Warp-level stable ranking (match.any groups the lanes of one digit).
+  uint32_t rank2[RS_ITEMS / 2];  // two 16-bit warp-local ranks per register (< 512)
+#pragma unroll
+  for (int k = 0; k < RS_ITEMS / 2; ++k) rank2[k] = 0;
+  const uint32_t lt = (1u << lane) - 1u;
+  uint16_t *whist = s_wcnt[warp];
+  if (full) {
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+      const uint32_t d = dig(key[k]);
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const int leader = __ffs(peers) - 1;
+      uint32_t old = 0;
+      if (lane == leader) {
+        old = whist[d];
+        whist[d] = (uint16_t)(old + __popc(peers));
+      }
+      old = __shfl_sync(0xffffffffu, old, leader);
+      rank2[k >> 1] |= (old + __popc(peers & lt)) << (16 * (k & 1));
+      __syncwarp();
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+      const bool valid = wl + 32u * k < tile_n;
+      const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+      if (valid) {
+        const uint32_t d = dig(key[k]);
+        const unsigned peers = __match_any_sync(vmask, d);
+        const int leader = __ffs(peers) - 1;
+        uint32_t old = 0;
+        if (lane == leader) {
+          old = whist[d];
+          whist[d] = old + __popc(peers);
+        }
+        old = __shfl_sync(vmask, old, leader);
+        rank2[k >> 1] |= (old + __popc(peers & lt)) << (16 * (k & 1));
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+
+  // Look-back for digit d: four predecessor words per step (independent
+  // relaxed loads -- every word carries its own count, nothing else is read).
   uint32_t excl = 0;
   if (tile > 0) {
     int64_t t = (int64_t)tile - 1;
     uint32_t spins = 0;
     const uint64_t t0 = pd_globaltimer_ns();
     while (t >= 0) {
-      uint32_t w = pd_load_acquire_u32(st + (uint64_t)t * RS_RADIX);
-      uint32_t flag = w & ~RS_COUNT_MASK;
-      if (flag == 0) {
-        if (pd_wait_expired(p.d_error, t0, ++spins)) break;
-        __nanosleep(32);
-        continue;
+      uint32_t w[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        w[i] = (t - i >= 0) ? pd_load_relaxed_u32(st + (uint64_t)(t - i) * RS_RADIX) : RS_FLAG_INC;
+      int used = 0;
+      bool done = false, stalled = false;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        if (done || stalled) continue;
+        const uint32_t flag = w[i] & ~RS_COUNT_MASK;
+        if (flag == 0) {
+          stalled = true;
+          continue;
+        }
+        excl += w[i] & RS_COUNT_MASK;
+        ++used;
+        if (flag == RS_FLAG_INC) done = true;
       }
-      excl += w & RS_COUNT_MASK;
-      if (flag == RS_FLAG_INC) break;
-      --t;
+      if (done) break;
+      t -= used;
+      if (stalled) {
+        if (pd_wait_expired(p.d_error, t0, ++spins)) break;
+        __nanosleep(spins < 8 ? 64 : 256);
+      }
     }
-    pd_store_release_u32(st + tile * RS_RADIX, RS_FLAG_INC | ((excl + count) & RS_COUNT_MASK));
+    pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_INC | ((excl + count) & RS_COUNT_MASK));
   }
   s_gdelta[d] = (int32_t)(p.offsets[pass * RS_RADIX + d] + excl) - (int32_t)dstart;
   __syncthreads();
@@ -377,7 +406,7 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   for (int k = 0; k < RS_ITEMS; ++k) {
     if (full || wl + 32u * k < tile_n) {
       const uint32_t dg = dig(key[k]);
-      const uint32_t pos = s_dstart[dg] + whist[dg] + rank[k];
+      const uint32_t pos = s_dstart[dg] + s_whist[warp][dg] + ((rank2[k >> 1] >> (16 * (k & 1))) & 0xFFFFu);
       s_keys[pos] = key[k];
       if (HAS_VALS) s_vals[pos] = val[k];
     }
