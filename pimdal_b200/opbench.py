@@ -1,0 +1,132 @@
+"""Runs one operator on seeded device-resident inputs and prints its timing.
+
+    python -m pimdal_b200.opbench select    --rows 16777216 --iters 20
+    python -m pimdal_b200.opbench sort      --rows 67108864 [--zipf]
+    python -m pimdal_b200.opbench smj       --rows 67108864          (inner = rows / 4)
+    python -m pimdal_b200.opbench hash_join --rows 268435456         (build = rows / 8)
+    python -m pimdal_b200.opbench group     --rows 268435456 --card 4096 --method hash|sort
+
+The per-operator counterpart of the reference's benchmark programs
+(reference/db_operators/*.cpp main: generate, run the kernel a fixed number of
+times, print the mean).  It is also the program the committed ncu summaries
+profile: small row counts give captures that end in seconds.  Each iteration
+is timed with CUDA events on the launching stream; the inputs are generated on
+the device by the seeded generator (include/pimdal_gpu.h pimdal_gen_column).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import statistics
+
+import torch
+
+from . import _lib as L
+from . import gen, ops
+
+
+def _inputs(ctx: ops.Context, a) -> tuple:
+    g = lambda spec, n: ops.gen_column(ctx, spec, n)
+    n = a.rows
+    if a.op == "select":
+        return (g(gen.Spec(L.GEN_UNIFORM, L.I32, seed=a.seed, lo=0, hi=2**31 - 1), n),)
+    if a.op == "sort":
+        if a.zipf:
+            spec = gen.Spec(L.GEN_PERM_ZIPF, L.U32, seed=a.seed, stream_id=1, perm_domain=0,
+                            cdf=gen.zipf_cdf(1 << 24, 1.0))
+        else:
+            spec = gen.Spec(L.GEN_UNIFORM, L.U32, seed=a.seed, lo=0, hi=2**32 - 1)
+        return g(spec, n), torch.arange(n, dtype=torch.int32, device=f"cuda:{ctx.device}")
+    if a.op == "smj":
+        nr = max(n // 4, 1)
+        rk = g(gen.Spec(L.GEN_PERM, L.I32, seed=a.seed, perm_domain=nr), nr)
+        sk = g(gen.Spec(L.GEN_PERM_UNIFORM, L.I32, seed=a.seed, stream_id=3, lo=0, hi=nr - 1,
+                        perm_domain=nr), n)
+        return rk, sk
+    if a.op == "hash_join":
+        nb = max(n // 8, 1)
+        spec_p = gen.Spec(L.GEN_PROBE, L.I32, seed=a.seed, stream_id=2, lo=nb, perm_domain=2 * nb,
+                          match_permille=500,
+                          cdf=gen.zipf_cdf(nb, 0.75) if a.zipf else None)
+        return (g(gen.Spec(L.GEN_PERM, L.I32, seed=a.seed, perm_domain=2 * nb), nb),
+                g(gen.Spec(L.GEN_UNIFORM, L.I32, seed=a.seed, stream_id=1, lo=-2**31, hi=2**31 - 1), nb),
+                g(spec_p, n))
+    if a.op == "group":
+        keys = g(gen.Spec(L.GEN_PERM_UNIFORM, L.I32, seed=a.seed, stream_id=10, lo=0,
+                          hi=a.card - 1, perm_domain=0), n)
+        vals = g(gen.Spec(L.GEN_UNIFORM, L.I64, seed=a.seed, stream_id=1, lo=100, hi=10**7), n)
+        return keys, vals
+    raise SystemExit(f"unknown operator {a.op}")
+
+
+def _runner(ctx: ops.Context, a, inp):
+    n = a.rows
+    dev = f"cuda:{ctx.device}"
+    if a.op == "select":
+        pred = ops.make_pred(L.PRED_LT, 214748364)
+        out, ptr = torch.empty_like(inp[0]), torch.empty_like(inp[0])
+        res = torch.empty(1, dtype=torch.int64, device=dev)
+        return lambda: ops.sel_kernel(ctx, inp[0], pred, out=out, out_ptr=ptr, result=res)
+    if a.op == "sort":
+        out, ptr = torch.empty_like(inp[0]), torch.empty_like(inp[0])
+        return lambda: ops.sort_kernel(ctx, inp[0], inp[1], out=out, out_ptr=ptr)
+    if a.op == "smj":
+        oi = torch.empty(n, dtype=torch.int32, device=dev)
+        oo = torch.empty(n, dtype=torch.int32, device=dev)
+        res = torch.empty(1, dtype=torch.int64, device=dev)
+        return lambda: ops.sort_merge_join(ctx, inp[0], None, inp[1], None, out_inner=oi,
+                                           out_outer=oo, result=res)
+    if a.op == "hash_join":
+        op = torch.empty(n, dtype=torch.int32, device=dev)
+        orow = torch.empty(n, dtype=torch.int32, device=dev)
+        res = torch.empty(1, dtype=torch.int64, device=dev)
+        return lambda: ops.hash_join(ctx, inp[0], inp[1], inp[2], capacity=n, out_payload=op,
+                                     out_row=orow, result=res)
+    method = {"hash": L.GROUP_HASH, "sort": L.GROUP_SORT, "auto": L.GROUP_AUTO}[a.method]
+    cap = 2 * a.card
+    outs = {w: torch.empty(cap, dtype=torch.int64, device=dev) for w in ("sum", "count", "min", "max")}
+    outs["key"] = torch.empty(cap, dtype=torch.int32, device=dev)
+    res = torch.empty(1, dtype=torch.int64, device=dev)
+    return lambda: ops.group_kernel(ctx, inp[0], inp[1], method=method, expected_groups=a.card,
+                                    capacity=cap, outs=outs, result=res)
+
+
+def main(argv=None) -> None:
+    p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    p.add_argument("op", choices=["select", "sort", "smj", "hash_join", "group"])
+    p.add_argument("--rows", type=int, default=1 << 24)
+    p.add_argument("--iters", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=2)
+    p.add_argument("--seed", type=int, default=0xB200)
+    p.add_argument("--zipf", action="store_true", help="Zipf keys (sort: s=1.0, hash_join: s=0.75)")
+    p.add_argument("--card", type=int, default=4096, help="group cardinality")
+    p.add_argument("--method", default="hash", choices=["hash", "sort", "auto"])
+    p.add_argument("--device", type=int, default=0)
+    a = p.parse_args(argv)
+    torch.cuda.set_device(a.device)
+    ctx = ops.Context(a.device)
+    inp = _inputs(ctx, a)
+    run = _runner(ctx, a, inp)
+    for _ in range(a.warmup):
+        run()
+    ctx.sync()
+    stream = torch.cuda.current_stream()
+    times = []
+    for _ in range(a.iters):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        run()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ctx.sync()
+    med = statistics.median(times) if times else float("nan")
+    print(json.dumps({"op": a.op, "rows": a.rows, "iters": a.iters, "zipf": a.zipf,
+                      "card": a.card if a.op == "group" else None,
+                      "method": a.method if a.op == "group" else None,
+                      "ms_median": med, "ms_min": min(times) if times else None,
+                      "rows_per_s": a.rows / (med * 1e-3) if times else None}))
+
+
+if __name__ == "__main__":
+    main()
