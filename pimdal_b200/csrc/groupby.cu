@@ -14,14 +14,24 @@
 // This operator returns, ordered by key, every group's key and any of SUM,
 // COUNT, MIN, MAX of int64 values (all exact, int64 wrap-around sums).
 //
-// B200 design, hash method:
-//  1. persistent CTAs aggregate their rows into a 2048-group shared-memory
-//     table (64-bit atomicCAS on the tagged key, 64-bit shared atomics on the
-//     aggregates); a row whose group finds no slot within 16 probes goes to
-//     the global table directly; at the end each CTA merges its table into
-//     the global one (64-bit global atomics);
-//  2. the occupied global slots are compacted, sorted by key with K-SORT
-//     (element count read on the device) and gathered into the outputs.
+// B200 design, hash method.  A group lives in one 32-byte slot
+// {count << 32 | key, sum, min, max}: the claiming compare-and-swap carries
+// the first rows' count, and every later update of the group touches the same
+// sector.  Three aggregation modes, chosen from the expected group count:
+//  - GB_WARP (few groups): the lanes of a warp that hold the same key are
+//    found with match.any and combined with redux.sync (64-bit sums from four
+//    16-bit partial sums, 64-bit min/max from the high then the low word);
+//    one lane per distinct key updates the CTA's shared-memory table;
+//  - GB_SMEM (up to a few thousand groups): every row updates the CTA table
+//    (6144 slots, 192 KB, one 1024-thread CTA per SM); rows whose group finds
+//    no slot within 8 probes go to the global table;
+//  - GB_DIRECT (many groups): rows update the global table directly; when the
+//    table is larger than an L2 budget it is split into K sub-tables by the
+//    high hash bits and the rows are aggregated in K launches, each touching
+//    an L2-sized sub-table.
+// Shared tables are merged into the global table at the end of each CTA.
+// The occupied global slots are then compacted, sorted by key with K-SORT
+// (element count read on the device) and gathered into the outputs.
 // Sort method: K-SORT of (key, row id), then a reduce-by-key over the sorted
 // rows (see k_gb_segreduce).
 #include <algorithm>
@@ -30,125 +40,241 @@
 
 namespace {
 
-constexpr int GB_THREADS = 512;
-constexpr uint32_t GB_SMEM_SLOTS = 2048;
-constexpr uint32_t GB_SMEM_PROBES = 16;
-constexpr unsigned long long GB_TAG = 1ull << 32;  // occupied marker above the key
+constexpr int GB_THREADS = 1024;
+constexpr uint32_t GB_SMEM_SLOTS = 6144;
+constexpr uint32_t GB_SMEM_PROBES = 8;
+constexpr size_t GB_SMEM_BYTES = 32ull * GB_SMEM_SLOTS;      // 192 KB
+constexpr uint64_t GB_WARP_MAX_GROUPS = 512;                 // GB_WARP at or below
+constexpr uint64_t GB_SMEM_MAX_GROUPS = 2 * GB_SMEM_SLOTS;   // GB_SMEM at or below
+constexpr uint64_t GB_L2_BUDGET = 64ull << 20;               // bytes of one sub-table
+enum { GB_WARP = 0, GB_SMEM = 1, GB_DIRECT = 2 };
 
 struct GbParams {
   const uint32_t *key;
   const int64_t *val;  // NULL: every value is 1
   uint64_t n;
-  // global table (capacity 2^bits)
-  unsigned long long *gkey;
-  long long *gsum;
-  unsigned long long *gcnt;
-  long long *gmin, *gmax;
-  uint32_t bits;
+  int vec;             // key and val 16-byte aligned: 4 rows per vector load
+  // global table: npasses sub-tables of sub_cap 32-byte slots
+  unsigned long long *gtab;
+  uint32_t sub_cap, npasses;
   unsigned long long *ngroups;  // compacted group count (device)
   uint32_t *ckey, *cslot;
   uint32_t *d_error;
 };
 
-__device__ __forceinline__ uint32_t gb_hash(uint32_t key, uint32_t bits) {
-  return (uint32_t)(((uint64_t)key * PD_GOLDEN64) >> (64 - bits));
+__device__ __forceinline__ uint64_t gb_h(uint32_t key) { return pd_mix64(key); }
+__device__ __forceinline__ uint32_t gb_pass(uint64_t h, uint32_t k) {
+  return (uint32_t)(((h >> 32) * k) >> 32);
+}
+__device__ __forceinline__ uint32_t gb_slot(uint64_t h, uint32_t cap) {
+  return (uint32_t)(((h & 0xffffffffull) * cap) >> 32);
 }
 
 __global__ void __launch_bounds__(256) k_gb_init(GbParams p) {
-  const uint64_t cap = 1ull << p.bits;
+  const uint64_t slots = (uint64_t)p.sub_cap * p.npasses;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += stride) {
-    p.gkey[i] = 0;
-    p.gsum[i] = 0;
-    p.gcnt[i] = 0;
-    p.gmin[i] = INT64_MAX;
-    p.gmax[i] = INT64_MIN;
+  ulonglong2 *t = reinterpret_cast<ulonglong2 *>(p.gtab);
+  const ulonglong2 lo = make_ulonglong2(0ull, 0ull);
+  const ulonglong2 hi = make_ulonglong2((unsigned long long)INT64_MAX, (unsigned long long)INT64_MIN);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < slots; i += stride) {
+    t[2 * i] = lo;
+    t[2 * i + 1] = hi;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) *p.ngroups = 0;
 }
 
-__device__ __forceinline__ void global_add(const GbParams &p, uint32_t key, long long sum,
-                                           unsigned long long cnt, long long mn, long long mx) {
-  const uint64_t mask = (1ull << p.bits) - 1;
-  const unsigned long long tagged = GB_TAG | key;
-  uint64_t s = gb_hash(key, p.bits);
-  for (uint64_t t = 0; t <= mask; ++t) {
-    unsigned long long cur = p.gkey[s];
-    if (cur == 0) cur = atomicCAS(p.gkey + s, 0ull, tagged);
-    if (cur == 0 || cur == tagged) {
-      atomicAdd((unsigned long long *)(p.gsum + s), (unsigned long long)sum);
-      atomicAdd(p.gcnt + s, cnt);
-      atomicMin(p.gmin + s, mn);
-      atomicMax(p.gmax + s, mx);
+// Adds a partial aggregate of `key` to sub-table `pass` of the global table.
+__device__ void global_add(const GbParams &p, uint32_t key, uint64_t h, uint32_t pass,
+                           uint32_t cnt, long long sum, long long mn, long long mx) {
+  const uint32_t cap = p.sub_cap;
+  unsigned long long *base = p.gtab + (uint64_t)pass * cap * 4;
+  const unsigned long long mine = ((unsigned long long)cnt << 32) | key;
+  uint32_t s = gb_slot(h, cap);
+  for (uint32_t t = 0; t < cap; ++t) {
+    unsigned long long *slot = base + (uint64_t)s * 4;
+    unsigned long long w = __ldcg(slot);
+    bool claimed = false;
+    if (w == 0) {
+      w = atomicCAS(slot, 0ull, mine);
+      claimed = w == 0;
+    }
+    if (claimed || (uint32_t)w == key) {
+      if (!claimed) atomicAdd(slot, (unsigned long long)cnt << 32);
+      atomicAdd(slot + 1, (unsigned long long)sum);
+      long long *m = reinterpret_cast<long long *>(slot) + 2;
+      // min/max only move one way: a stale read can only cause a redundant atomic
+      if (mn < __ldcg(m)) atomicMin(m, mn);
+      if (mx > __ldcg(m + 1)) atomicMax(m + 1, mx);
       return;
     }
-    s = (s + 1) & mask;
+    s = (s + 1 == cap) ? 0 : s + 1;
   }
   atomicOr(p.d_error, PD_DEVERR_TABLE_FULL);
 }
 
-constexpr size_t GB_SMEM_BYTES = 40ull * GB_SMEM_SLOTS;
+struct SmemTable {
+  unsigned long long *w;  // count << 32 | key (0 = empty)
+  long long *sum, *mn, *mx;
+};
 
-__global__ void __launch_bounds__(GB_THREADS) k_gb_aggregate(GbParams p) {
-  extern __shared__ __align__(16) unsigned char gb_smem[];
-  unsigned long long *s_key = reinterpret_cast<unsigned long long *>(gb_smem);
-  long long *s_sum = reinterpret_cast<long long *>(s_key + GB_SMEM_SLOTS);
-  unsigned long long *s_cnt = reinterpret_cast<unsigned long long *>(s_sum + GB_SMEM_SLOTS);
-  long long *s_min = reinterpret_cast<long long *>(s_cnt + GB_SMEM_SLOTS);
-  long long *s_max = s_min + GB_SMEM_SLOTS;
-  for (uint32_t i = threadIdx.x; i < GB_SMEM_SLOTS; i += GB_THREADS) {
-    s_key[i] = 0;
-    s_sum[i] = 0;
-    s_cnt[i] = 0;
-    s_min[i] = INT64_MAX;
-    s_max[i] = INT64_MIN;
-  }
-  __syncthreads();
-  constexpr uint32_t SBITS = 11;  // log2(GB_SMEM_SLOTS)
-  const uint64_t stride = (uint64_t)gridDim.x * GB_THREADS;
-  for (uint64_t i = (uint64_t)blockIdx.x * GB_THREADS + threadIdx.x; i < p.n; i += stride) {
-    const uint32_t k = __ldcs(p.key + i);
-    const long long v = p.val ? (long long)__ldcs(p.val + i) : 1ll;
-    const unsigned long long tagged = GB_TAG | k;
-    uint32_t s = gb_hash(k, SBITS);
-    bool done = false;
-    for (uint32_t t = 0; t < GB_SMEM_PROBES; ++t) {
-      unsigned long long cur = s_key[s];
-      if (cur == 0) cur = atomicCAS(s_key + s, 0ull, tagged);
-      if (cur == 0 || cur == tagged) {
-        atomicAdd((unsigned long long *)(s_sum + s), (unsigned long long)v);
-        atomicAdd(s_cnt + s, 1ull);
-        atomicMin(s_min + s, v);
-        atomicMax(s_max + s, v);
-        done = true;
-        break;
-      }
-      s = (s + 1) & (GB_SMEM_SLOTS - 1);
+__device__ __forceinline__ bool smem_add(const SmemTable &t, uint32_t key, uint64_t h, uint32_t cnt,
+                                         long long sum, long long mn, long long mx) {
+  const unsigned long long mine = ((unsigned long long)cnt << 32) | key;
+  uint32_t s = gb_slot(h, GB_SMEM_SLOTS);
+#pragma unroll 1
+  for (uint32_t i = 0; i < GB_SMEM_PROBES; ++i) {
+    unsigned long long w = *(volatile unsigned long long *)(t.w + s);
+    bool claimed = false;
+    if (w == 0) {
+      w = atomicCAS(t.w + s, 0ull, mine);
+      claimed = w == 0;
     }
-    if (!done) global_add(p, k, v, 1ull, v, v);
+    if (claimed || (uint32_t)w == key) {
+      if (!claimed) atomicAdd(t.w + s, (unsigned long long)cnt << 32);
+      atomicAdd(reinterpret_cast<unsigned long long *>(t.sum) + s, (unsigned long long)sum);
+      if (mn < *(volatile long long *)(t.mn + s)) atomicMin(t.mn + s, mn);
+      if (mx > *(volatile long long *)(t.mx + s)) atomicMax(t.mx + s, mx);
+      return true;
+    }
+    s = (s + 1 == GB_SMEM_SLOTS) ? 0 : s + 1;
   }
-  __syncthreads();
-  for (uint32_t i = threadIdx.x; i < GB_SMEM_SLOTS; i += GB_THREADS) {
-    if (s_key[i])
-      global_add(p, (uint32_t)s_key[i], s_sum[i], s_cnt[i], s_min[i], s_max[i]);
+  return false;
+}
+
+// Aggregate of the lanes in `peers` (all holding the same key), exact in
+// 64-bit: the sum from four sums of 16-bit limbs (each < 2^21), min and max
+// from the signed high words, then the unsigned low words of the lanes that
+// hold the extreme high word.
+__device__ __forceinline__ void warp_combine(unsigned peers, long long v, long long &sum,
+                                             long long &mn, long long &mx) {
+  const unsigned long long u = (unsigned long long)v;
+  const unsigned long long s0 = __reduce_add_sync(peers, (unsigned)(u & 0xFFFFu));
+  const unsigned long long s1 = __reduce_add_sync(peers, (unsigned)((u >> 16) & 0xFFFFu));
+  const unsigned long long s2 = __reduce_add_sync(peers, (unsigned)((u >> 32) & 0xFFFFu));
+  const unsigned long long s3 = __reduce_add_sync(peers, (unsigned)(u >> 48));
+  sum = (long long)(s0 + (s1 << 16) + (s2 << 32) + (s3 << 48));
+  const int hi = (int)(u >> 32);
+  const unsigned lo = (unsigned)u;
+  const int mh = __reduce_min_sync(peers, hi);
+  const unsigned ml = __reduce_min_sync(peers, hi == mh ? lo : 0xFFFFFFFFu);
+  mn = (long long)(((unsigned long long)(unsigned)mh << 32) | ml);
+  const int xh = __reduce_max_sync(peers, hi);
+  const unsigned xl = __reduce_max_sync(peers, hi == xh ? lo : 0u);
+  mx = (long long)(((unsigned long long)(unsigned)xh << 32) | xl);
+}
+
+template <int MODE>
+__device__ __forceinline__ void gb_row(const GbParams &p, const SmemTable &t, uint32_t pass,
+                                       uint32_t k, long long v, bool valid, int lane) {
+  uint32_t cnt = 1;
+  long long sum = v, mn = v, mx = v;
+  if (MODE == GB_WARP) {
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+    if (!valid) return;
+    const unsigned peers = __match_any_sync(vmask, k);
+    if (peers != (1u << lane)) {
+      warp_combine(peers, v, sum, mn, mx);
+      if (lane != __ffs(peers) - 1) return;
+      cnt = __popc(peers);
+    }
+  } else if (!valid) {
+    return;
+  }
+  const uint64_t h = gb_h(k);
+  if (MODE == GB_DIRECT) {
+    if (p.npasses > 1 && gb_pass(h, p.npasses) != pass) return;
+    global_add(p, k, h, pass, cnt, sum, mn, mx);
+    return;
+  }
+  if (!smem_add(t, k, h, cnt, sum, mn, mx)) global_add(p, k, h, 0, cnt, sum, mn, mx);
+}
+
+// Persistent CTAs; each warp takes 128 consecutive rows per step (4 per lane,
+// one 16-byte key load and two 16-byte value loads when aligned).
+template <int MODE>
+__global__ void __launch_bounds__(GB_THREADS, MODE == GB_DIRECT ? 2 : 1)
+k_gb_aggregate(GbParams p, uint32_t pass) {
+  extern __shared__ __align__(16) unsigned char gb_smem[];
+  SmemTable t;
+  t.w = reinterpret_cast<unsigned long long *>(gb_smem);
+  t.sum = reinterpret_cast<long long *>(t.w + GB_SMEM_SLOTS);
+  t.mn = t.sum + GB_SMEM_SLOTS;
+  t.mx = t.mn + GB_SMEM_SLOTS;
+  if (MODE != GB_DIRECT) {
+    for (uint32_t i = threadIdx.x; i < GB_SMEM_SLOTS; i += GB_THREADS) {
+      t.w[i] = 0;
+      t.sum[i] = 0;
+      t.mn[i] = INT64_MAX;
+      t.mx[i] = INT64_MIN;
+    }
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31;
+  const uint64_t warps = (uint64_t)gridDim.x * (GB_THREADS / 32);
+  const uint64_t gw = (uint64_t)blockIdx.x * (GB_THREADS / 32) + (threadIdx.x >> 5);
+  uint64_t done = 0;
+  if (p.vec) {
+    const uint64_t nq = p.n / 4;  // quads of rows
+    const uint4 *k4 = reinterpret_cast<const uint4 *>(p.key);
+    const longlong2 *v2 = reinterpret_cast<const longlong2 *>(p.val);
+    for (uint64_t b = gw * 32; b < nq; b += warps * 32) {
+      const uint64_t q = b + lane;
+      const bool ok = q < nq;
+      uint4 k = make_uint4(0, 0, 0, 0);
+      longlong2 va = make_longlong2(1, 1), vb = make_longlong2(1, 1);
+      if (ok) {
+        k = __ldcs(k4 + q);
+        bool need = true;
+        if (MODE == GB_DIRECT && p.npasses > 1) {
+          need = gb_pass(gb_h(k.x), p.npasses) == pass || gb_pass(gb_h(k.y), p.npasses) == pass ||
+                 gb_pass(gb_h(k.z), p.npasses) == pass || gb_pass(gb_h(k.w), p.npasses) == pass;
+        }
+        if (p.val && need) {
+          va = __ldcs(v2 + 2 * q);
+          vb = __ldcs(v2 + 2 * q + 1);
+        }
+      }
+      gb_row<MODE>(p, t, pass, k.x, va.x, ok, lane);
+      gb_row<MODE>(p, t, pass, k.y, va.y, ok, lane);
+      gb_row<MODE>(p, t, pass, k.z, vb.x, ok, lane);
+      gb_row<MODE>(p, t, pass, k.w, vb.y, ok, lane);
+    }
+    done = nq * 4;
+  }
+  for (uint64_t b = done + gw * 32; b < p.n; b += warps * 32) {
+    const uint64_t i = b + lane;
+    const bool ok = i < p.n;
+    const uint32_t k = ok ? p.key[i] : 0u;
+    const long long v = (ok && p.val) ? (long long)p.val[i] : 1ll;
+    gb_row<MODE>(p, t, pass, k, v, ok, lane);
+  }
+  if (MODE != GB_DIRECT) {
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < GB_SMEM_SLOTS; i += GB_THREADS) {
+      const unsigned long long w = t.w[i];
+      if (w) {
+        const uint32_t k = (uint32_t)w;
+        global_add(p, k, gb_h(k), 0, (uint32_t)(w >> 32), t.sum[i], t.mn[i], t.mx[i]);
+      }
+    }
   }
 }
 
 // Occupied slots -> (key, slot) list (order is restored by the sort that follows).
 __global__ void __launch_bounds__(256) k_gb_compact(GbParams p) {
-  const uint64_t cap = 1ull << p.bits;
+  const uint64_t slots = (uint64_t)p.sub_cap * p.npasses;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   const int lane = threadIdx.x & 31;
-  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < cap; base += stride) {
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < slots; base += stride) {
     const uint64_t i = base + threadIdx.x;
-    const unsigned long long k = i < cap ? p.gkey[i] : 0ull;
-    const unsigned m = __ballot_sync(0xffffffffu, k != 0);
+    const unsigned long long w = i < slots ? __ldcs(p.gtab + 4 * i) : 0ull;
+    const unsigned m = __ballot_sync(0xffffffffu, w != 0);
     if (!m) continue;
     uint32_t pos = 0;
     if (lane == 0) pos = (uint32_t)atomicAdd(p.ngroups, (unsigned long long)__popc(m));
     pos = __shfl_sync(0xffffffffu, pos, 0) + __popc(m & ((1u << lane) - 1u));
-    if (k) {
-      p.ckey[pos] = (uint32_t)k;
+    if (w) {
+      p.ckey[pos] = (uint32_t)w;
       p.cslot[pos] = (uint32_t)i;
     }
   }
@@ -157,8 +283,7 @@ __global__ void __launch_bounds__(256) k_gb_compact(GbParams p) {
 struct GatherParams {
   const uint32_t *skey, *sslot;
   const unsigned long long *ngroups;
-  const long long *gsum, *gmin, *gmax;
-  const unsigned long long *gcnt;
+  const unsigned long long *gtab;
   uint32_t *out_key;
   int64_t *out_sum, *out_count, *out_min, *out_max;
   uint64_t cap;
@@ -174,13 +299,15 @@ __global__ void __launch_bounds__(256) k_gb_gather(GatherParams g) {
   }
   const uint64_t lim = min(n, g.cap);
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const ulonglong2 *t = reinterpret_cast<const ulonglong2 *>(g.gtab);
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < lim; i += stride) {
-    const uint32_t s = g.sslot[i];
+    const uint64_t s = g.sslot[i];
+    const ulonglong2 a = t[2 * s], b = t[2 * s + 1];
     if (g.out_key) g.out_key[i] = g.skey[i];
-    if (g.out_sum) g.out_sum[i] = g.gsum[s];
-    if (g.out_count) g.out_count[i] = (int64_t)g.gcnt[s];
-    if (g.out_min) g.out_min[i] = g.gmin[s];
-    if (g.out_max) g.out_max[i] = g.gmax[s];
+    if (g.out_sum) g.out_sum[i] = (int64_t)a.y;
+    if (g.out_count) g.out_count[i] = (int64_t)(a.x >> 32);
+    if (g.out_min) g.out_min[i] = (int64_t)b.x;
+    if (g.out_max) g.out_max[i] = (int64_t)b.y;
   }
 }
 
@@ -190,8 +317,10 @@ __global__ void __launch_bounds__(256) k_gb_gather(GatherParams g) {
 //  1. k_sr_heads: group heads per tile;
 //  2. k_sr_scan (one block): exclusive head prefix per tile, group count G;
 //  3. k_sr_init: outputs 0..G-1 set to the aggregate identities;
-//  4. k_gb_segreduce: a group inside one thread's rows is stored directly; a
-//     group cut by a thread boundary is merged with 64-bit global atomics.
+//  4. k_gb_segreduce: a group inside one thread's rows is stored directly;
+//     groups cut by thread boundaries are joined by a block-wide segmented
+//     scan and stored directly too; only the (at most two) groups of a tile
+//     that cross the tile's edges are merged with 64-bit global atomics.
 // ---------------------------------------------------------------------------
 constexpr int SR_THREADS = 256;
 constexpr int SR_ITEMS = 16;
@@ -276,96 +405,187 @@ __global__ void __launch_bounds__(256) k_sr_init(SegParams p) {
   }
 }
 
-__device__ __forceinline__ void sr_flush(const SegParams &p, uint64_t g, uint32_t key, bool whole,
-                                         long long sum, unsigned long long cnt, long long mn,
-                                         long long mx) {
-  if (g >= p.cap) return;  // reported by k_sr_scan
+struct SrAgg {
+  uint32_t cnt;  // rows inside one tile
+  long long sum, mn, mx;
+};
+
+__device__ __forceinline__ SrAgg sr_empty() { return SrAgg{0u, 0ll, INT64_MAX, INT64_MIN}; }
+
+__device__ __forceinline__ void sr_acc(SrAgg &a, long long v) {
+  ++a.cnt;
+  a.sum = (long long)((unsigned long long)a.sum + (unsigned long long)v);
+  a.mn = min(a.mn, v);
+  a.mx = max(a.mx, v);
+}
+
+__device__ __forceinline__ SrAgg sr_join(const SrAgg &a, const SrAgg &b) {
+  return SrAgg{a.cnt + b.cnt, (long long)((unsigned long long)a.sum + (unsigned long long)b.sum),
+               min(a.mn, b.mn), max(a.mx, b.mx)};
+}
+
+// Segmented-scan element: f = a group head lies in the covered rows; key and
+// agg describe the rows from the last such head (or all rows when f = 0).
+struct SrSeg {
+  uint32_t f, key;
+  SrAgg a;
+};
+
+__device__ __forceinline__ SrSeg sr_combine(const SrSeg &l, const SrSeg &r) {
+  if (r.f) return r;
+  return SrSeg{l.f, l.key, sr_join(l.a, r.a)};
+}
+
+__device__ __forceinline__ SrSeg sr_shfl_up(const SrSeg &x, int o) {
+  SrSeg y;
+  y.f = __shfl_up_sync(0xffffffffu, x.f, o);
+  y.key = __shfl_up_sync(0xffffffffu, x.key, o);
+  y.a.cnt = __shfl_up_sync(0xffffffffu, x.a.cnt, o);
+  y.a.sum = __shfl_up_sync(0xffffffffu, x.a.sum, o);
+  y.a.mn = __shfl_up_sync(0xffffffffu, x.a.mn, o);
+  y.a.mx = __shfl_up_sync(0xffffffffu, x.a.mx, o);
+  return y;
+}
+
+__device__ __forceinline__ void sr_store(const SegParams &p, uint64_t g, uint32_t key, bool whole,
+                                         const SrAgg &a) {
+  if (g >= p.cap || a.cnt == 0) return;  // overflow is reported by k_sr_scan
+  if (p.out_key) p.out_key[g] = key;     // every writer of a group stores the same key
   if (whole) {
-    if (p.out_key) p.out_key[g] = key;
-    if (p.out_sum) p.out_sum[g] = sum;
-    if (p.out_cnt) p.out_cnt[g] = cnt;
-    if (p.out_min) p.out_min[g] = mn;
-    if (p.out_max) p.out_max[g] = mx;
+    if (p.out_sum) p.out_sum[g] = a.sum;
+    if (p.out_cnt) p.out_cnt[g] = a.cnt;
+    if (p.out_min) p.out_min[g] = a.mn;
+    if (p.out_max) p.out_max[g] = a.mx;
   } else {
-    if (p.out_key) p.out_key[g] = key;  // every writer stores the same key
-    if (p.out_sum) atomicAdd((unsigned long long *)(p.out_sum + g), (unsigned long long)sum);
-    if (p.out_cnt) atomicAdd(p.out_cnt + g, cnt);
-    if (p.out_min) atomicMin(p.out_min + g, mn);
-    if (p.out_max) atomicMax(p.out_max + g, mx);
+    if (p.out_sum) atomicAdd((unsigned long long *)(p.out_sum + g), (unsigned long long)a.sum);
+    if (p.out_cnt) atomicAdd(p.out_cnt + g, (unsigned long long)a.cnt);
+    if (p.out_min) atomicMin(p.out_min + g, a.mn);
+    if (p.out_max) atomicMax(p.out_max + g, a.mx);
   }
 }
 
 __global__ void __launch_bounds__(SR_THREADS) k_gb_segreduce(SegParams p) {
-  __shared__ uint32_t s_warp[SR_THREADS / 32];
+  __shared__ uint32_t s_heads[SR_THREADS / 32];
+  __shared__ SrSeg s_seg[SR_THREADS / 32];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint64_t tile = blockIdx.x;
-  const uint64_t r0 = tile * SR_TILE + (uint64_t)tid * SR_ITEMS;
-  uint32_t key[SR_ITEMS];
-  uint32_t heads = 0, nh = 0;
+  const uint64_t t0 = tile * SR_TILE;
+  const uint64_t r0 = t0 + (uint64_t)tid * SR_ITEMS;
+  const bool full = t0 + SR_TILE <= p.n;
+  uint32_t key[SR_ITEMS], idx[SR_ITEMS];
+  if (full) {
+    const uint4 *k4 = reinterpret_cast<const uint4 *>(p.skey + r0);
+    const uint4 *i4 = reinterpret_cast<const uint4 *>(p.sidx + r0);
+#pragma unroll
+    for (int j = 0; j < SR_ITEMS / 4; ++j) {
+      const uint4 a = __ldcs(k4 + j), b = __ldcs(i4 + j);
+      key[4 * j] = a.x; key[4 * j + 1] = a.y; key[4 * j + 2] = a.z; key[4 * j + 3] = a.w;
+      idx[4 * j] = b.x; idx[4 * j + 1] = b.y; idx[4 * j + 2] = b.z; idx[4 * j + 3] = b.w;
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < SR_ITEMS; ++j) {
+      key[j] = (r0 + j < p.n) ? p.skey[r0 + j] : 0u;
+      idx[j] = (r0 + j < p.n) ? p.sidx[r0 + j] : 0u;
+    }
+  }
+  long long val[SR_ITEMS];
+#pragma unroll
+  for (int j = 0; j < SR_ITEMS; ++j)
+    val[j] = (p.val && (full || r0 + j < p.n)) ? (long long)__ldg(p.val + idx[j]) : 1ll;
   const uint32_t before = (r0 > 0 && r0 - 1 < p.n) ? p.skey[r0 - 1] : 0u;
+  uint32_t heads = 0, nh = 0;
 #pragma unroll
   for (int j = 0; j < SR_ITEMS; ++j) {
-    key[j] = (r0 + j < p.n) ? p.skey[r0 + j] : 0u;
     const uint32_t prev = j ? key[j - 1] : before;
-    const bool h = (r0 + j < p.n) && (r0 + j == 0 || key[j] != prev);
+    const bool h = (full || r0 + j < p.n) && (r0 + j == 0 || key[j] != prev);
     heads |= (uint32_t)h << j;
     nh += h;
   }
+  // heads strictly before this thread's first row (global group index)
   uint32_t inc = nh;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
-    uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
     if (lane >= o) inc += t;
   }
-  if (lane == 31) s_warp[warp] = inc;
+  if (lane == 31) s_heads[warp] = inc;
+  // rows: lead (before the first head), whole groups, tail (from the last head)
+  SrAgg lead = sr_empty(), cur = sr_empty();
   __syncthreads();
-  uint32_t wpre = 0;
+  uint32_t wpre = 0, btot = 0;
 #pragma unroll
-  for (int w = 0; w < SR_THREADS / 32; ++w)
-    if (w < warp) wpre += s_warp[w];
-  // heads strictly before this thread's first row
-  uint64_t g = p.tile_heads[tile] + wpre + inc - nh;
-  bool open_whole = false;  // the current segment began at a head in this thread
-  long long sum = 0, mn = INT64_MAX, mx = INT64_MIN;
-  unsigned long long cnt = 0;
+  for (int w = 0; w < SR_THREADS / 32; ++w) {
+    if (w < warp) wpre += s_heads[w];
+    btot += s_heads[w];
+  }
+  const uint64_t gfirst = p.tile_heads[tile] + wpre + inc - nh;
+  uint64_t g = gfirst;
   bool have = false;
   uint32_t cur_key = 0;
-  uint64_t cur_g = 0;
 #pragma unroll
   for (int j = 0; j < SR_ITEMS; ++j) {
-    if (r0 + j >= p.n) break;
+    if (!full && r0 + j >= p.n) break;
     if ((heads >> j) & 1u) {
-      if (have) sr_flush(p, cur_g, cur_key, open_whole, sum, cnt, mn, mx);
-      cur_g = g;
+      if (have) sr_store(p, g - 1, cur_key, true, cur);
+      else lead = cur;
+      have = true;
+      cur = sr_empty();
+      cur_key = key[j];
       ++g;
-      cur_key = key[j];
-      open_whole = true;
-      sum = 0; cnt = 0; mn = INT64_MAX; mx = INT64_MIN;
-      have = true;
-    } else if (!have) {
-      cur_g = g - 1;  // continues the group of the previous rows
-      cur_key = key[j];
-      open_whole = false;
-      have = true;
     }
-    const long long v = p.val ? (long long)p.val[p.sidx[r0 + j]] : 1ll;
-    sum = (long long)((unsigned long long)sum + (unsigned long long)v);
-    ++cnt;
-    mn = min(mn, v);
-    mx = max(mx, v);
+    sr_acc(cur, val[j]);
   }
+  if (!have) lead = cur;
+  // block-wide inclusive segmented scan of (have, tail)
+  SrSeg x{have ? 1u : 0u, have ? cur_key : key[0], have ? cur : lead};
+  SrSeg incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const SrSeg y = sr_shfl_up(incl, o);
+    if (lane >= o) incl = sr_combine(y, incl);
+  }
+  SrSeg wex = sr_shfl_up(incl, 1);
+  if (lane == 0) wex = SrSeg{0u, 0u, sr_empty()};
+  if (lane == 31) s_seg[warp] = incl;
+  __syncthreads();
+  SrSeg pre{0u, 0u, sr_empty()};
+  for (int w = 0; w < warp; ++w) pre = sr_combine(pre, s_seg[w]);
+  const SrSeg ex = sr_combine(pre, wex);
   if (have) {
-    // the last segment is whole only if the next row starts a new group
-    const uint64_t nx = r0 + SR_ITEMS;
-    const bool ends = nx >= p.n || p.skey[nx] != cur_key;
-    sr_flush(p, cur_g, cur_key, open_whole && ends, sum, cnt, mn, mx);
+    // the group that ends just before this thread's first head
+    const SrAgg tot = sr_join(ex.a, lead);
+    const uint32_t k = ex.f ? ex.key : (lead.cnt ? key[0] : before);
+    sr_store(p, gfirst - 1, k, ex.f != 0, tot);
+  }
+  if (tid == SR_THREADS - 1) {
+    const SrSeg all = sr_combine(pre, incl);
+    const uint64_t nx = t0 + SR_TILE;  // first row of the next tile
+    const bool ends = nx >= p.n || p.skey[nx] != p.skey[nx - 1];
+    if (all.f) {
+      sr_store(p, p.tile_heads[tile] + btot - 1, all.key, ends, all.a);
+    } else {
+      sr_store(p, p.tile_heads[tile] - 1, p.skey[t0], false, all.a);
+    }
   }
 }
 
 struct GbLayout {
-  uint32_t bits;
-  size_t gkey, gsum, gcnt, gmin, gmax, ngroups, ckey, cslot, skey, sslot, sort_ws, total;
+  int mode;
+  uint32_t sub_cap, npasses;
+  size_t gtab, ngroups, ckey, cslot, skey, sslot, sort_ws, total;
 };
+
+// Bytes of one global sub-table (an L2-sized slice of the table that one
+// aggregation launch updates); PIMDAL_GROUP_L2_BUDGET_MB overrides it.
+uint64_t gb_l2_budget() {
+  static const uint64_t b = [] {
+    const char *e = getenv("PIMDAL_GROUP_L2_BUDGET_MB");
+    const long long mb = e ? atoll(e) : 0;
+    return mb > 0 ? (uint64_t)mb << 20 : GB_L2_BUDGET;
+  }();
+  return b;
+}
 
 bool gb_layout(const pimdal_aggr_arguments_t *a, GbLayout *l) {
   const bool sort = a->method == PIMDAL_GROUP_SORT;
@@ -375,7 +595,8 @@ bool gb_layout(const pimdal_aggr_arguments_t *a, GbLayout *l) {
   if (sort) {
     sa.nr_elements = a->size;
     if (pimdal_sort_workspace_size(&sa, &w)) return false;
-    l->bits = 0;
+    l->mode = -1;
+    l->sub_cap = l->npasses = 0;
     l->ngroups = o; o += pd_align_up(8 * (pd_ceil_div(a->size, SR_TILE) + 1), 256);
     l->skey = o; o += pd_align_up(4 * a->size, 256);
     l->sslot = o; o += pd_align_up(4 * a->size, 256);
@@ -384,16 +605,18 @@ bool gb_layout(const pimdal_aggr_arguments_t *a, GbLayout *l) {
     return true;
   }
   uint64_t expect = a->expected_groups ? a->expected_groups : std::min<uint64_t>(a->size, 1ull << 22);
-  uint64_t cap = 2048;
-  while (cap < 2 * expect) cap <<= 1;
-  uint32_t bits = 0;
-  while ((1ull << bits) < cap) ++bits;
-  l->bits = bits;
-  l->gkey = o; o += pd_align_up(8 * cap, 256);
-  l->gsum = o; o += pd_align_up(8 * cap, 256);
-  l->gcnt = o; o += pd_align_up(8 * cap, 256);
-  l->gmin = o; o += pd_align_up(8 * cap, 256);
-  l->gmax = o; o += pd_align_up(8 * cap, 256);
+  expect = std::max<uint64_t>(expect, 1);
+  l->mode = expect <= GB_WARP_MAX_GROUPS ? GB_WARP : expect <= GB_SMEM_MAX_GROUPS ? GB_SMEM : GB_DIRECT;
+  // load factor 1/2 for the small tables, 3/4 for the large ones
+  uint64_t slots = l->mode == GB_DIRECT ? expect + expect / 3 + 1 : 2 * expect;
+  slots = std::max<uint64_t>(slots, 2048);
+  if (slots >= (1ull << 31)) return false;
+  uint64_t np = 1;
+  if (l->mode == GB_DIRECT) np = std::max<uint64_t>(1, pd_ceil_div(32 * slots, gb_l2_budget()));
+  l->npasses = (uint32_t)np;
+  l->sub_cap = (uint32_t)pd_ceil_div(slots, np);
+  const uint64_t cap = (uint64_t)l->sub_cap * np;
+  l->gtab = o; o += pd_align_up(32 * cap, 256);
   l->ngroups = o; o += 256;
   l->ckey = o; o += pd_align_up(4 * cap, 256);
   l->cslot = o; o += pd_align_up(4 * cap, 256);
@@ -485,29 +708,33 @@ extern "C" int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_argument
   p.key = (const uint32_t *)a->in;
   p.val = a->in_val;
   p.n = a->size;
-  p.gkey = (unsigned long long *)(ws + l.gkey);
-  p.gsum = (long long *)(ws + l.gsum);
-  p.gcnt = (unsigned long long *)(ws + l.gcnt);
-  p.gmin = (long long *)(ws + l.gmin);
-  p.gmax = (long long *)(ws + l.gmax);
-  p.bits = l.bits;
+  p.vec = ((uintptr_t)a->in & 15u) == 0 && ((uintptr_t)a->in_val & 15u) == 0;
+  p.gtab = (unsigned long long *)(ws + l.gtab);
+  p.sub_cap = l.sub_cap;
+  p.npasses = l.npasses;
   p.ngroups = (unsigned long long *)(ws + l.ngroups);
   p.ckey = (uint32_t *)(ws + l.ckey);
   p.cslot = (uint32_t *)(ws + l.cslot);
   p.d_error = ctx->d_error;
-  const uint64_t cap = 1ull << l.bits;
+  const uint64_t cap = (uint64_t)l.sub_cap * l.npasses;
   const unsigned init_grid = (unsigned)std::min<uint64_t>(pd_ceil_div(cap, 256), ctx->sm_count * 8ull);
   {
     pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
     k_gb_init<<<init_grid, 256, 0, s>>>(p);
   }
-  {
+  const uint64_t want = pd_ceil_div(a->size, (uint64_t)GB_THREADS * 4);
+  if (l.mode == GB_DIRECT) {
+    const unsigned grid = (unsigned)std::min<uint64_t>(want, (uint64_t)ctx->sm_count * 2);
+    for (uint32_t q = 0; q < l.npasses; ++q) {
+      pd_launch_scope sc(ctx, PIMDAL_KERNEL_GROUP, s);
+      k_gb_aggregate<GB_DIRECT><<<grid ? grid : 1, GB_THREADS, 0, s>>>(p, q);
+    }
+  } else {
     pd_launch_scope sc(ctx, PIMDAL_KERNEL_GROUP, s);
-    const unsigned grid = (unsigned)std::min<uint64_t>(pd_ceil_div(a->size, GB_THREADS * 8ull),
-                                                       (uint64_t)ctx->sm_count * 2);
-    PD_CHECK_CUDA(cudaFuncSetAttribute(k_gb_aggregate, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)GB_SMEM_BYTES));
-    k_gb_aggregate<<<grid ? grid : 1, GB_THREADS, GB_SMEM_BYTES, s>>>(p);
+    const unsigned grid = (unsigned)std::min<uint64_t>(want, (uint64_t)ctx->sm_count);
+    auto k = l.mode == GB_WARP ? k_gb_aggregate<GB_WARP> : k_gb_aggregate<GB_SMEM>;
+    PD_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GB_SMEM_BYTES));
+    k<<<grid ? grid : 1, GB_THREADS, GB_SMEM_BYTES, s>>>(p, 0);
   }
   {
     pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
@@ -525,10 +752,7 @@ extern "C" int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_argument
   g.skey = (const uint32_t *)(ws + l.skey);
   g.sslot = (const uint32_t *)(ws + l.sslot);
   g.ngroups = p.ngroups;
-  g.gsum = p.gsum;
-  g.gmin = p.gmin;
-  g.gmax = p.gmax;
-  g.gcnt = p.gcnt;
+  g.gtab = p.gtab;
   g.out_key = (uint32_t *)a->out;
   g.out_sum = a->out_sum;
   g.out_count = a->out_count;
