@@ -18,18 +18,22 @@
 // {count << 32 | key, sum, min, max}: the claiming compare-and-swap carries
 // the first rows' count, and every later update of the group touches the same
 // sector.  Three aggregation modes, chosen from the expected group count:
-//  - GB_WARP (few groups): the lanes of a warp that hold the same key are
-//    found with match.any and combined with redux.sync (64-bit sums from four
-//    16-bit partial sums, 64-bit min/max from the high then the low word);
-//    one lane per distinct key updates the CTA's shared-memory table;
-//  - GB_SMEM (up to a few thousand groups): every row updates the CTA table
-//    (6144 slots, 192 KB, one 1024-thread CTA per SM); rows whose group finds
-//    no slot within 8 probes go to the global table;
-//  - GB_DIRECT (many groups): rows update the global table directly; when the
-//    table is larger than an L2 budget it is split into K sub-tables by the
-//    high hash bits and the rows are aggregated in K launches, each touching
-//    an L2-sized sub-table.
-// Shared tables are merged into the global table at the end of each CTA.
+//  - GB_WARP (a few dozen groups): each warp owns a private shared-memory
+//    table of 192 slots (split in up to 4 replicas, each for a subset of the
+//    lanes), so only a few lanes of one warp ever contend;
+//  - GB_SMEM (up to a few thousand groups): every row updates the CTA's
+//    shared-memory table (6144 slots, 192 KB, one 1024-thread CTA per SM);
+//  - GB_DIRECT (many groups): rows update the global table directly.  When
+//    the table is larger than an L2 budget it can be split into K sub-tables
+//    by the high hash bits and aggregated in K launches, each touching an
+//    L2-sized sub-table (PIMDAL_GROUP_L2_BUDGET_MB; one pass by default).
+// Shared tables probe 4-slot buckets of 32-bit keys with one 16-byte load.
+// A row whose group finds no shared slot within 16 buckets goes to the global
+// table; shared tables are merged into the global table at the end of each
+// CTA.  A global update reads the slot's sector once (two 16-byte loads
+// issued together), claims an empty slot with one compare-and-swap, and adds
+// the count and sum with fire-and-forget reductions; min/max reductions are
+// issued only when the loaded value shows they change the slot.
 // The occupied global slots are then compacted, sorted by key with K-SORT
 // (element count read on the device) and gathered into the outputs.
 // Sort method: K-SORT of (key, row id), then a reduce-by-key over the sorted
@@ -41,12 +45,14 @@
 namespace {
 
 constexpr int GB_THREADS = 1024;
+constexpr int GB_WARPS = GB_THREADS / 32;
 constexpr uint32_t GB_SMEM_SLOTS = 6144;
-constexpr uint32_t GB_SMEM_PROBES = 8;
+constexpr uint32_t GB_WARP_SLOTS = GB_SMEM_SLOTS / GB_WARPS;  // 192 per warp
+constexpr uint32_t GB_SMEM_PROBES = 16;  // buckets
 constexpr size_t GB_SMEM_BYTES = 32ull * GB_SMEM_SLOTS;      // 192 KB
-constexpr uint64_t GB_WARP_MAX_GROUPS = 512;                 // GB_WARP at or below
-constexpr uint64_t GB_SMEM_MAX_GROUPS = 2 * GB_SMEM_SLOTS;   // GB_SMEM at or below
-constexpr uint64_t GB_L2_BUDGET = 64ull << 20;               // bytes of one sub-table
+constexpr uint64_t GB_WARP_MAX_GROUPS = 64;                  // GB_WARP at or below
+constexpr uint64_t GB_SMEM_MAX_GROUPS = 4608;                // GB_SMEM at or below (load 3/4)
+constexpr uint64_t GB_L2_BUDGET = 1ull << 40;                // one pass unless overridden
 enum { GB_WARP = 0, GB_SMEM = 1, GB_DIRECT = 2 };
 
 struct GbParams {
@@ -57,6 +63,7 @@ struct GbParams {
   // global table: npasses sub-tables of sub_cap 32-byte slots
   unsigned long long *gtab;
   uint32_t sub_cap, npasses;
+  uint32_t wrep;       // GB_WARP: private replicas per warp (1, 2 or 4)
   unsigned long long *ngroups;  // compacted group count (device)
   uint32_t *ckey, *cslot;
   uint32_t *d_error;
@@ -83,16 +90,22 @@ __global__ void __launch_bounds__(256) k_gb_init(GbParams p) {
   if (blockIdx.x == 0 && threadIdx.x == 0) *p.ngroups = 0;
 }
 
-// Adds a partial aggregate of `key` to sub-table `pass` of the global table.
-__device__ void global_add(const GbParams &p, uint32_t key, uint64_t h, uint32_t pass,
-                           uint32_t cnt, long long sum, long long mn, long long mx) {
+// Adds a partial aggregate of `key` to sub-table `pass` of the global table,
+// starting at slot s whose sector (a, b) the caller may already have loaded.
+__device__ void global_add_from(const GbParams &p, uint32_t key, uint32_t pass, uint32_t s,
+                                ulonglong2 a, ulonglong2 b, bool loaded, uint32_t cnt,
+                                long long sum, long long mn, long long mx) {
   const uint32_t cap = p.sub_cap;
   unsigned long long *base = p.gtab + (uint64_t)pass * cap * 4;
   const unsigned long long mine = ((unsigned long long)cnt << 32) | key;
-  uint32_t s = gb_slot(h, cap);
   for (uint32_t t = 0; t < cap; ++t) {
     unsigned long long *slot = base + (uint64_t)s * 4;
-    unsigned long long w = __ldcg(slot);
+    if (!loaded) {
+      a = __ldcg(reinterpret_cast<const ulonglong2 *>(slot));
+      b = __ldcg(reinterpret_cast<const ulonglong2 *>(slot) + 1);
+    }
+    loaded = false;
+    unsigned long long w = a.x;
     bool claimed = false;
     if (w == 0) {
       w = atomicCAS(slot, 0ull, mine);
@@ -101,10 +114,9 @@ __device__ void global_add(const GbParams &p, uint32_t key, uint64_t h, uint32_t
     if (claimed || (uint32_t)w == key) {
       if (!claimed) atomicAdd(slot, (unsigned long long)cnt << 32);
       atomicAdd(slot + 1, (unsigned long long)sum);
-      long long *m = reinterpret_cast<long long *>(slot) + 2;
-      // min/max only move one way: a stale read can only cause a redundant atomic
-      if (mn < __ldcg(m)) atomicMin(m, mn);
-      if (mx > __ldcg(m + 1)) atomicMax(m + 1, mx);
+      // min/max only move one way: a stale value can only cause a redundant reduction
+      if (mn < (long long)b.x) atomicMin(reinterpret_cast<long long *>(slot) + 2, mn);
+      if (mx > (long long)b.y) atomicMax(reinterpret_cast<long long *>(slot) + 3, mx);
       return;
     }
     s = (s + 1 == cap) ? 0 : s + 1;
@@ -112,106 +124,148 @@ __device__ void global_add(const GbParams &p, uint32_t key, uint64_t h, uint32_t
   atomicOr(p.d_error, PD_DEVERR_TABLE_FULL);
 }
 
+__device__ __forceinline__ void global_add(const GbParams &p, uint32_t key, uint64_t h, uint32_t pass,
+                                           uint32_t cnt, long long sum, long long mn, long long mx) {
+  global_add_from(p, key, pass, gb_slot(h, p.sub_cap), ulonglong2{}, ulonglong2{}, false, cnt, sum,
+                  mn, mx);
+}
+
+// Shared table: 4-slot buckets of 32-bit keys (empty = all ones), one 16-byte
+// load probes a bucket.  The all-ones key itself bypasses shared tables.
+constexpr uint32_t GB_EMPTY = 0xFFFFFFFFu;
+
 struct SmemTable {
-  unsigned long long *w;  // count << 32 | key (0 = empty)
-  long long *sum, *mn, *mx;
+  uint32_t *key;
+  uint32_t *cnt;
+  long long *sum;
+  longlong2 *mm;  // (min, max)
 };
 
-__device__ __forceinline__ bool smem_add(const SmemTable &t, uint32_t key, uint64_t h, uint32_t cnt,
-                                         long long sum, long long mn, long long mx) {
-  const unsigned long long mine = ((unsigned long long)cnt << 32) | key;
-  uint32_t s = gb_slot(h, GB_SMEM_SLOTS);
-#pragma unroll 1
-  for (uint32_t i = 0; i < GB_SMEM_PROBES; ++i) {
-    unsigned long long w = *(volatile unsigned long long *)(t.w + s);
-    bool claimed = false;
-    if (w == 0) {
-      w = atomicCAS(t.w + s, 0ull, mine);
-      claimed = w == 0;
+__device__ __forceinline__ int bucket_match(const uint4 &q, uint32_t key) {
+  return q.x == key ? 0 : q.y == key ? 1 : q.z == key ? 2 : q.w == key ? 3 : -1;
+}
+
+// Slot of `key` in buckets [base, base + nb) of a shared table, claiming an
+// empty slot when the key is absent; -1 when no bucket within the probe limit
+// has room (the row then goes to the global table).
+__device__ __noinline__ int smem_find(const SmemTable &t, uint32_t base, uint32_t nb, uint32_t key,
+                                      uint32_t b) {
+  for (uint32_t i = 0; i < GB_SMEM_PROBES;) {
+    const uint32_t s0 = 4 * (base + b);
+    // plain loads: a key never changes once set, so a stale bucket costs at
+    // most a failed compare-and-swap and another look
+    const uint4 q = *reinterpret_cast<const uint4 *>(t.key + s0);
+    const int hit = bucket_match(q, key);
+    if (hit >= 0) return (int)s0 + hit;
+    const int e = bucket_match(q, GB_EMPTY);
+    if (e < 0) {  // full bucket without the key: next bucket
+      b = (b + 1 == nb) ? 0 : b + 1;
+      ++i;
+      continue;
     }
-    if (claimed || (uint32_t)w == key) {
-      if (!claimed) atomicAdd(t.w + s, (unsigned long long)cnt << 32);
-      atomicAdd(reinterpret_cast<unsigned long long *>(t.sum) + s, (unsigned long long)sum);
-      if (mn < *(volatile long long *)(t.mn + s)) atomicMin(t.mn + s, mn);
-      if (mx > *(volatile long long *)(t.mx + s)) atomicMax(t.mx + s, mx);
-      return true;
-    }
-    s = (s + 1 == GB_SMEM_SLOTS) ? 0 : s + 1;
+    const uint32_t old = atomicCAS(t.key + s0 + e, GB_EMPTY, key);
+    if (old == GB_EMPTY || old == key) return (int)s0 + e;
+    // lost the slot to another key: look at the bucket again
   }
-  return false;
+  return -1;
 }
 
-// Aggregate of the lanes in `peers` (all holding the same key), exact in
-// 64-bit: the sum from four sums of 16-bit limbs (each < 2^21), min and max
-// from the signed high words, then the unsigned low words of the lanes that
-// hold the extreme high word.
-__device__ __forceinline__ void warp_combine(unsigned peers, long long v, long long &sum,
-                                             long long &mn, long long &mx) {
-  const unsigned long long u = (unsigned long long)v;
-  const unsigned long long s0 = __reduce_add_sync(peers, (unsigned)(u & 0xFFFFu));
-  const unsigned long long s1 = __reduce_add_sync(peers, (unsigned)((u >> 16) & 0xFFFFu));
-  const unsigned long long s2 = __reduce_add_sync(peers, (unsigned)((u >> 32) & 0xFFFFu));
-  const unsigned long long s3 = __reduce_add_sync(peers, (unsigned)(u >> 48));
-  sum = (long long)(s0 + (s1 << 16) + (s2 << 32) + (s3 << 48));
-  const int hi = (int)(u >> 32);
-  const unsigned lo = (unsigned)u;
-  const int mh = __reduce_min_sync(peers, hi);
-  const unsigned ml = __reduce_min_sync(peers, hi == mh ? lo : 0xFFFFFFFFu);
-  mn = (long long)(((unsigned long long)(unsigned)mh << 32) | ml);
-  const int xh = __reduce_max_sync(peers, hi);
-  const unsigned xl = __reduce_max_sync(peers, hi == xh ? lo : 0u);
-  mx = (long long)(((unsigned long long)(unsigned)xh << 32) | xl);
-}
-
+// Four rows of one lane: (A) bucket lookups with all four loads in flight,
+// the rare claims and full buckets on a slow path; (B) the updates as
+// straight-line predicated shared atomics.
 template <int MODE>
-__device__ __forceinline__ void gb_row(const GbParams &p, const SmemTable &t, uint32_t pass,
-                                       uint32_t k, long long v, bool valid, int lane) {
-  uint32_t cnt = 1;
-  long long sum = v, mn = v, mx = v;
-  if (MODE == GB_WARP) {
-    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-    if (!valid) return;
-    const unsigned peers = __match_any_sync(vmask, k);
-    if (peers != (1u << lane)) {
-      warp_combine(peers, v, sum, mn, mx);
-      if (lane != __ffs(peers) - 1) return;
-      cnt = __popc(peers);
+__device__ __forceinline__ void gb_rows4(const GbParams &p, const SmemTable &t, uint32_t pass,
+                                         const uint32_t (&k)[4], const long long (&v)[4],
+                                         uint32_t valid, uint32_t base, uint32_t nb) {
+  if constexpr (MODE == GB_DIRECT) {
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      if (!((valid >> r) & 1u)) continue;
+      const uint64_t h = gb_h(k[r]);
+      if (p.npasses > 1 && gb_pass(h, p.npasses) != pass) continue;
+      global_add(p, k[r], h, pass, 1u, v[r], v[r], v[r]);
     }
-  } else if (!valid) {
-    return;
+  } else {
+    // home and next bucket of every row, all eight loads in flight together
+    uint32_t b[4];
+    uint4 q[4], q2[4];
+    int slot[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      b[r] = gb_slot(gb_h(k[r]), nb);
+      const uint32_t b2 = b[r] + 1 == nb ? 0 : b[r] + 1;
+      q[r] = *reinterpret_cast<const uint4 *>(t.key + 4 * (base + b[r]));
+      q2[r] = *reinterpret_cast<const uint4 *>(t.key + 4 * (base + b2));
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      // the all-ones key equals the empty marker: it always takes the global path
+      const int hit = bucket_match(q[r], k[r]);
+      const bool home_full = bucket_match(q[r], GB_EMPTY) < 0;
+      const int hit2 = home_full ? bucket_match(q2[r], k[r]) : -1;
+      const uint32_t b2 = b[r] + 1 == nb ? 0 : b[r] + 1;
+      slot[r] = k[r] == GB_EMPTY ? -1
+              : hit >= 0         ? (int)(4 * (base + b[r])) + hit
+              : hit2 >= 0        ? (int)(4 * (base + b2)) + hit2
+                                 : -2;
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      if (!((valid >> r) & 1u)) slot[r] = -3;
+      else if (slot[r] == -2) slot[r] = smem_find(t, base, nb, k[r], b[r]);
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      if (slot[r] >= 0) {
+        atomicAdd(t.cnt + slot[r], 1u);
+        atomicAdd(reinterpret_cast<unsigned long long *>(t.sum) + slot[r], (unsigned long long)v[r]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      if (slot[r] >= 0) {
+        const longlong2 m = t.mm[slot[r]];
+        if (v[r] < m.x) atomicMin(&t.mm[slot[r]].x, v[r]);
+        if (v[r] > m.y) atomicMax(&t.mm[slot[r]].y, v[r]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+      if (slot[r] == -1) global_add(p, k[r], gb_h(k[r]), 0, 1u, v[r], v[r], v[r]);
   }
-  const uint64_t h = gb_h(k);
-  if (MODE == GB_DIRECT) {
-    if (p.npasses > 1 && gb_pass(h, p.npasses) != pass) return;
-    global_add(p, k, h, pass, cnt, sum, mn, mx);
-    return;
-  }
-  if (!smem_add(t, k, h, cnt, sum, mn, mx)) global_add(p, k, h, 0, cnt, sum, mn, mx);
 }
 
 // Persistent CTAs; each warp takes 128 consecutive rows per step (4 per lane,
-// one 16-byte key load and two 16-byte value loads when aligned).
+// one 16-byte key load and two 16-byte value loads when aligned).  In GB_WARP
+// mode each warp's 192 slots form p.wrep private replicas, one per group of
+// 32 / p.wrep lanes.
 template <int MODE>
 __global__ void __launch_bounds__(GB_THREADS, MODE == GB_DIRECT ? 2 : 1)
 k_gb_aggregate(GbParams p, uint32_t pass) {
   extern __shared__ __align__(16) unsigned char gb_smem[];
   SmemTable t;
-  t.w = reinterpret_cast<unsigned long long *>(gb_smem);
-  t.sum = reinterpret_cast<long long *>(t.w + GB_SMEM_SLOTS);
-  t.mn = t.sum + GB_SMEM_SLOTS;
-  t.mx = t.mn + GB_SMEM_SLOTS;
+  t.key = reinterpret_cast<uint32_t *>(gb_smem);
+  t.cnt = t.key + GB_SMEM_SLOTS;
+  t.sum = reinterpret_cast<long long *>(t.cnt + GB_SMEM_SLOTS);
+  t.mm = reinterpret_cast<longlong2 *>(t.sum + GB_SMEM_SLOTS);
   if (MODE != GB_DIRECT) {
     for (uint32_t i = threadIdx.x; i < GB_SMEM_SLOTS; i += GB_THREADS) {
-      t.w[i] = 0;
+      t.key[i] = GB_EMPTY;
+      t.cnt[i] = 0;
       t.sum[i] = 0;
-      t.mn[i] = INT64_MAX;
-      t.mx[i] = INT64_MIN;
+      t.mm[i] = make_longlong2(INT64_MAX, INT64_MIN);
     }
     __syncthreads();
   }
   const int lane = threadIdx.x & 31;
-  const uint64_t warps = (uint64_t)gridDim.x * (GB_THREADS / 32);
-  const uint64_t gw = (uint64_t)blockIdx.x * (GB_THREADS / 32) + (threadIdx.x >> 5);
+  // shared buckets this lane uses: its warp's replica (GB_WARP) or the CTA table
+  uint32_t base = 0, nb = GB_SMEM_SLOTS / 4;
+  if (MODE == GB_WARP) {
+    nb = GB_WARP_SLOTS / 4 / p.wrep;
+    base = (threadIdx.x >> 5) * (GB_WARP_SLOTS / 4) + (lane / (32 / p.wrep)) * nb;
+  }
+  const uint64_t warps = (uint64_t)gridDim.x * GB_WARPS;
+  const uint64_t gw = (uint64_t)blockIdx.x * GB_WARPS + (threadIdx.x >> 5);
   uint64_t done = 0;
   if (p.vec) {
     const uint64_t nq = p.n / 4;  // quads of rows
@@ -234,28 +288,33 @@ k_gb_aggregate(GbParams p, uint32_t pass) {
           vb = __ldcs(v2 + 2 * q + 1);
         }
       }
-      gb_row<MODE>(p, t, pass, k.x, va.x, ok, lane);
-      gb_row<MODE>(p, t, pass, k.y, va.y, ok, lane);
-      gb_row<MODE>(p, t, pass, k.z, vb.x, ok, lane);
-      gb_row<MODE>(p, t, pass, k.w, vb.y, ok, lane);
+      const uint32_t kk[4] = {k.x, k.y, k.z, k.w};
+      const long long vv[4] = {va.x, va.y, vb.x, vb.y};
+      gb_rows4<MODE>(p, t, pass, kk, vv, ok ? 0xFu : 0u, base, nb);
     }
     done = nq * 4;
   }
-  for (uint64_t b = done + gw * 32; b < p.n; b += warps * 32) {
-    const uint64_t i = b + lane;
-    const bool ok = i < p.n;
-    const uint32_t k = ok ? p.key[i] : 0u;
-    const long long v = (ok && p.val) ? (long long)p.val[i] : 1ll;
-    gb_row<MODE>(p, t, pass, k, v, ok, lane);
+  // unaligned input or the last rows: lane-striped groups of four rows
+  for (uint64_t b = done + gw * 128; b < p.n; b += warps * 128) {
+    uint32_t kk[4];
+    long long vv[4];
+    uint32_t valid = 0;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const uint64_t i = b + 32 * r + lane;
+      const bool in = i < p.n;
+      valid |= (uint32_t)in << r;
+      kk[r] = in ? p.key[i] : 0u;
+      vv[r] = (in && p.val) ? (long long)p.val[i] : 1ll;
+    }
+    gb_rows4<MODE>(p, t, pass, kk, vv, valid, base, nb);
   }
   if (MODE != GB_DIRECT) {
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < GB_SMEM_SLOTS; i += GB_THREADS) {
-      const unsigned long long w = t.w[i];
-      if (w) {
-        const uint32_t k = (uint32_t)w;
-        global_add(p, k, gb_h(k), 0, (uint32_t)(w >> 32), t.sum[i], t.mn[i], t.mx[i]);
-      }
+      const uint32_t k = t.key[i];
+      if (k != GB_EMPTY)
+        global_add(p, k, gb_h(k), 0, t.cnt[i], t.sum[i], t.mm[i].x, t.mm[i].y);
     }
   }
 }
@@ -572,7 +631,7 @@ __global__ void __launch_bounds__(SR_THREADS) k_gb_segreduce(SegParams p) {
 
 struct GbLayout {
   int mode;
-  uint32_t sub_cap, npasses;
+  uint32_t sub_cap, npasses, wrep;
   size_t gtab, ngroups, ckey, cslot, skey, sslot, sort_ws, total;
 };
 
@@ -596,7 +655,7 @@ bool gb_layout(const pimdal_aggr_arguments_t *a, GbLayout *l) {
     sa.nr_elements = a->size;
     if (pimdal_sort_workspace_size(&sa, &w)) return false;
     l->mode = -1;
-    l->sub_cap = l->npasses = 0;
+    l->sub_cap = l->npasses = l->wrep = 0;
     l->ngroups = o; o += pd_align_up(8 * (pd_ceil_div(a->size, SR_TILE) + 1), 256);
     l->skey = o; o += pd_align_up(4 * a->size, 256);
     l->sslot = o; o += pd_align_up(4 * a->size, 256);
@@ -607,6 +666,8 @@ bool gb_layout(const pimdal_aggr_arguments_t *a, GbLayout *l) {
   uint64_t expect = a->expected_groups ? a->expected_groups : std::min<uint64_t>(a->size, 1ull << 22);
   expect = std::max<uint64_t>(expect, 1);
   l->mode = expect <= GB_WARP_MAX_GROUPS ? GB_WARP : expect <= GB_SMEM_MAX_GROUPS ? GB_SMEM : GB_DIRECT;
+  // GB_WARP replicas: keep each replica's load at or below 1/3
+  l->wrep = expect <= 16 ? 4 : expect <= 32 ? 2 : 1;
   // load factor 1/2 for the small tables, 3/4 for the large ones
   uint64_t slots = l->mode == GB_DIRECT ? expect + expect / 3 + 1 : 2 * expect;
   slots = std::max<uint64_t>(slots, 2048);
@@ -712,6 +773,7 @@ extern "C" int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_argument
   p.gtab = (unsigned long long *)(ws + l.gtab);
   p.sub_cap = l.sub_cap;
   p.npasses = l.npasses;
+  p.wrep = l.wrep;
   p.ngroups = (unsigned long long *)(ws + l.ngroups);
   p.ckey = (uint32_t *)(ws + l.ckey);
   p.cslot = (uint32_t *)(ws + l.cslot);

@@ -31,7 +31,8 @@ constexpr int MJ_THREADS = 256;
 constexpr int MJ_WARPS = MJ_THREADS / 32;
 constexpr int MJ_ITEMS = 8;
 constexpr int MJ_TILE = MJ_THREADS * MJ_ITEMS;  // 2048 outer rows per tile
-constexpr int MJ_INNER_CAP = 4096;               // inner rows staged in shared memory
+constexpr int MJ_INNER_CAP = 3072;               // inner rows staged in shared memory
+constexpr int MJ_OUT_CAP = 2048;                 // output pairs staged in shared memory
 
 struct MergeParams {
   const uint32_t *ikey, *iptr;  // sorted inner (keys, payload / row id)
@@ -72,9 +73,23 @@ __global__ void __launch_bounds__(256) k_smj_bounds(MergeParams p) {
   p.bounds[2 * t + 1] = gsearch(p.ikey, 0, p.ni, kl, p.flip, true);
 }
 
+// First index in [lo, hi) of a staged (order-transformed) key array whose key
+// is >= v (upper = false) or > v (upper = true).
+__device__ __forceinline__ uint32_t ssearch(const uint32_t *k, uint32_t lo, uint32_t hi, uint32_t v,
+                                            bool upper) {
+  while (lo < hi) {
+    const uint32_t m = (lo + hi) >> 1;
+    const bool right = upper ? (k[m] <= v) : (k[m] < v);
+    if (right) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
 __global__ void __launch_bounds__(MJ_THREADS) k_smj_merge(MergeParams p) {
   __shared__ uint32_t s_ik[MJ_INNER_CAP];
   __shared__ uint32_t s_ip[MJ_INNER_CAP];
+  __shared__ uint32_t s_oo[MJ_OUT_CAP];  // staged output of the tile
+  __shared__ uint32_t s_oi[MJ_OUT_CAP];
   __shared__ uint32_t s_warp[MJ_WARPS];
   __shared__ uint32_t s_flags[2 * MJ_WARPS];
   __shared__ uint64_t s_sum[MJ_WARPS + 1];
@@ -97,33 +112,64 @@ __global__ void __launch_bounds__(MJ_THREADS) k_smj_merge(MergeParams p) {
     }
   }
   // Blocked arrangement: thread t owns outer rows o0 + 8t .. o0 + 8t + 7.
-  uint32_t lb[MJ_ITEMS], cnt[MJ_ITEMS];
-  uint32_t okey[MJ_ITEMS];
+  uint32_t okey[MJ_ITEMS], opay[MJ_ITEMS];
   const uint64_t r0 = o0 + (uint64_t)tid * MJ_ITEMS;
+  const bool vec = r0 + MJ_ITEMS <= o1 && (((uintptr_t)(p.okey + r0) | (uintptr_t)(p.optr + r0)) & 15u) == 0;
+  if (vec) {
+    const uint4 *k4 = reinterpret_cast<const uint4 *>(p.okey + r0);
+    const uint4 *p4 = reinterpret_cast<const uint4 *>(p.optr + r0);
 #pragma unroll
-  for (int j = 0; j < MJ_ITEMS; ++j) okey[j] = (r0 + j < o1) ? ord(p.okey[r0 + j], p.flip) : 0u;
-  __syncthreads();
-  uint32_t mine = 0;
-#pragma unroll
-  for (int j = 0; j < MJ_ITEMS; ++j) {
-    lb[j] = 0;
-    cnt[j] = 0;
-    if (r0 + j >= o1 || range == 0) continue;
-    uint64_t l, u;
-    if (staged) {
-      uint32_t lo = 0, hi = (uint32_t)range;
-      while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (s_ik[m] < okey[j]) lo = m + 1; else hi = m; }
-      l = lo;
-      hi = (uint32_t)range;
-      while (lo < hi) { uint32_t m = (lo + hi) >> 1; if (s_ik[m] <= okey[j]) lo = m + 1; else hi = m; }
-      u = lo;
-    } else {
-      l = gsearch(p.ikey, a0, a1, okey[j], p.flip, false) - a0;
-      u = gsearch(p.ikey, a0 + l, a1, okey[j], p.flip, true) - a0;
+    for (int h = 0; h < MJ_ITEMS / 4; ++h) {
+      const uint4 k = __ldcs(k4 + h), q = __ldcs(p4 + h);
+      okey[4 * h] = k.x; okey[4 * h + 1] = k.y; okey[4 * h + 2] = k.z; okey[4 * h + 3] = k.w;
+      opay[4 * h] = q.x; opay[4 * h + 1] = q.y; opay[4 * h + 2] = q.z; opay[4 * h + 3] = q.w;
     }
-    lb[j] = (uint32_t)l;
-    cnt[j] = (uint32_t)(u - l);
-    mine += cnt[j];
+  } else {
+#pragma unroll
+    for (int j = 0; j < MJ_ITEMS; ++j) {
+      okey[j] = r0 + j < o1 ? p.okey[r0 + j] : 0u;
+      opay[j] = r0 + j < o1 ? p.optr[r0 + j] : 0u;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < MJ_ITEMS; ++j) okey[j] = ord(okey[j], p.flip);
+  __syncthreads();
+  uint32_t lb[MJ_ITEMS], cnt[MJ_ITEMS];
+  uint32_t mine = 0;
+  if (staged) {
+    // The thread's keys ascend: one binary search, then short forward walks
+    // (a search again when a walk passes 8 keys).
+    const uint32_t rg = (uint32_t)range;
+    uint32_t lo = (r0 < o1 && rg) ? ssearch(s_ik, 0, rg, okey[0], false) : rg;
+#pragma unroll
+    for (int j = 0; j < MJ_ITEMS; ++j) {
+      lb[j] = 0;
+      cnt[j] = 0;
+      if (r0 + j >= o1) continue;
+      const uint32_t k = okey[j];
+      uint32_t steps = 0;
+      while (lo < rg && s_ik[lo] < k && steps < 8) { ++lo; ++steps; }
+      if (lo < rg && s_ik[lo] < k) lo = ssearch(s_ik, lo, rg, k, false);
+      uint32_t hi = lo;
+      steps = 0;
+      while (hi < rg && s_ik[hi] == k && steps < 8) { ++hi; ++steps; }
+      if (hi < rg && s_ik[hi] == k) hi = ssearch(s_ik, hi, rg, k, true);
+      lb[j] = lo;
+      cnt[j] = hi - lo;
+      mine += cnt[j];
+    }
+  } else {
+#pragma unroll
+    for (int j = 0; j < MJ_ITEMS; ++j) {
+      lb[j] = 0;
+      cnt[j] = 0;
+      if (r0 + j >= o1 || range == 0) continue;
+      const uint64_t l = gsearch(p.ikey, a0, a1, okey[j], p.flip, false) - a0;
+      const uint64_t u = gsearch(p.ikey, a0 + l, a1, okey[j], p.flip, true) - a0;
+      lb[j] = (uint32_t)l;
+      cnt[j] = (uint32_t)(u - l);
+      mine += cnt[j];
+    }
   }
   // Block exclusive scan of the per-thread match counts.
   uint32_t inc = mine;
@@ -162,17 +208,35 @@ __global__ void __launch_bounds__(MJ_THREADS) k_smj_merge(MergeParams p) {
   const uint64_t base = s_prefix;
   if (tile == p.tiles - 1 && tid == 0) *p.d_count = base + total;
 
-  // Emit (outer payload, inner payload) pairs.
+  if (staged && total <= MJ_OUT_CAP) {
+    // Stage the tile's pairs, then write them with coalesced stores.
+    uint32_t w = excl;
+#pragma unroll
+    for (int j = 0; j < MJ_ITEMS; ++j) {
+      for (uint32_t m = 0; m < cnt[j]; ++m, ++w) {
+        s_oo[w] = opay[j];
+        s_oi[w] = s_ip[lb[j] + m];
+      }
+    }
+    __syncthreads();
+    const uint32_t room = base >= p.cap ? 0u : (uint32_t)min((uint64_t)total, p.cap - base);
+    for (uint32_t i = tid; i < room; i += MJ_THREADS) {
+      p.out_outer[base + i] = s_oo[i];
+      p.out_inner[base + i] = s_oi[i];
+    }
+    if (tid == 0 && room < total) atomicOr(p.d_error, PD_DEVERR_CAPACITY);
+    return;
+  }
+  // Emit (outer payload, inner payload) pairs directly.
   uint64_t w = base + excl;
   bool overflow = false;
 #pragma unroll
   for (int j = 0; j < MJ_ITEMS; ++j) {
     if (!cnt[j]) continue;
-    const uint32_t op = p.optr[r0 + j];
     for (uint32_t m = 0; m < cnt[j]; ++m, ++w) {
       if (w >= p.cap) { overflow = true; continue; }
       const uint32_t ip = staged ? s_ip[lb[j] + m] : p.iptr[a0 + lb[j] + m];
-      p.out_outer[w] = op;
+      p.out_outer[w] = opay[j];
       p.out_inner[w] = ip;
     }
   }

@@ -225,6 +225,19 @@ __device__ __forceinline__ uint32_t sort_xform(uint32_t k, uint32_t flip) {
   return k ^ flip;
 }
 
+// Lanes of `members` whose digit equals this lane's: one ballot per digit
+// bit.  For 8-bit labels this is cheaper than the match.any instruction.
+__device__ __forceinline__ unsigned match_digit(uint32_t d, unsigned members) {
+  unsigned m = members;
+#pragma unroll
+  for (int b = 0; b < RS_RADIX_BITS; ++b) {
+    const bool bit = (d >> b) & 1u;
+    const unsigned v = __ballot_sync(members, bit);
+    m &= bit ? v : ~v;
+  }
+  return m;
+}
+
 // One digit pass.  FULL tiles take a path without bounds checks; indices
 // inside a tile are 32-bit; the digit is (xform(key) >> shift) & mask.
 template <bool HAS_VALS, int KEY_MODE>
@@ -330,7 +343,7 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
 #pragma unroll
     for (int k = 0; k < RS_ITEMS; ++k) {
       const uint32_t d = dig(key[k]);
-      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const unsigned peers = match_digit(d, 0xffffffffu);
       const int leader = __ffs(peers) - 1;
       uint32_t old = 0;
       if (lane == leader) {
@@ -348,7 +361,7 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
       const unsigned vmask = __ballot_sync(0xffffffffu, valid);
       if (valid) {
         const uint32_t d = dig(key[k]);
-        const unsigned peers = __match_any_sync(vmask, d);
+        const unsigned peers = match_digit(d, vmask);
         const int leader = __ffs(peers) - 1;
         uint32_t old = 0;
         if (lane == leader) {

@@ -102,6 +102,8 @@ def main(argv=None) -> None:
     p.add_argument("--card", type=int, default=4096, help="group cardinality")
     p.add_argument("--method", default="hash", choices=["hash", "sort", "auto"])
     p.add_argument("--device", type=int, default=0)
+    p.add_argument("--kernels", action="store_true",
+                   help="also print the mean time of each library kernel class")
     a = p.parse_args(argv)
     torch.cuda.set_device(a.device)
     ctx = ops.Context(a.device)
@@ -111,6 +113,11 @@ def main(argv=None) -> None:
         run()
     ctx.sync()
     stream = torch.cuda.current_stream()
+    names = {getattr(L, k): k[len("KERNEL_"):].lower() for k in dir(L) if k.startswith("KERNEL_")}
+    if a.kernels:
+        for k in names:
+            ctx.kernel_time(k)  # reset
+        ctx.set_profiling(True)
     times = []
     for _ in range(a.iters):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -120,12 +127,21 @@ def main(argv=None) -> None:
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
     ctx.sync()
+    kernels = None
+    if a.kernels:
+        ctx.set_profiling(False)
+        kernels = {}
+        for k, nm in sorted(names.items()):
+            n, ms = ctx.kernel_time(k)
+            if n:
+                kernels[nm] = {"launches_per_iter": n / max(a.iters, 1), "ms_per_iter": ms / max(a.iters, 1)}
     med = statistics.median(times) if times else float("nan")
     print(json.dumps({"op": a.op, "rows": a.rows, "iters": a.iters, "zipf": a.zipf,
                       "card": a.card if a.op == "group" else None,
                       "method": a.method if a.op == "group" else None,
                       "ms_median": med, "ms_min": min(times) if times else None,
-                      "rows_per_s": a.rows / (med * 1e-3) if times else None}))
+                      "rows_per_s": a.rows / (med * 1e-3) if times else None,
+                      "kernels": kernels}))
 
 
 if __name__ == "__main__":

@@ -92,3 +92,11 @@ def test_group_by_config3_full_size(ctx, card):
     kk = o1["key"][:g].cpu().numpy()
     assert np.all(np.diff(kk.astype(np.int64)) > 0)
     assert int(o1["min"][:g].min().item()) >= 100 and int(o1["max"][:g].max().item()) <= 10**7
+
+
+@pytest.mark.parametrize("expected", [4, 16, 32, 64, 1000])
+def test_group_by_all_ones_key_in_every_table_mode(ctx, expected):
+    # the all-ones key (-1) is the shared tables' empty marker: it must still aggregate
+    k, v = inputs(20000, min(expected, 8), 55)
+    k[::3] = -1
+    check(run(ctx, k, v, L.GROUP_HASH, expected=expected), oracle.group_by(k, v))
