@@ -413,6 +413,54 @@ int pimdal_group_workspace_size(const pimdal_aggr_arguments_t *args, size_t *byt
 int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_arguments_t *args,
                         pimdal_aggr_results_t *d_result, pimdal_stream_t stream);
 
+/* ------------------------------------------------------------------------- */
+/* Batched form: many independent group-by or hash-join instances, each phase */
+/* one persistent launch fed by a device work queue.  No reference counterpart */
+/* (the reference runs one operator instance per DPU launch, e.g. the        */
+/* dpu_launch loops of pimdal/main/aggregate/hash/host/host_aggregate_sync.cpp */
+/* and pimdal/main/join/hash/host/host_join_sync.cpp); every instance gets    */
+/* what pimdal_group_kernel / pimdal_hash_join (unpartitioned) return for the */
+/* same arguments.                                                           */
+/*                                                                           */
+/* A plan holds the instances' descriptors, the work items, the tables and   */
+/* the scratch in device memory allocated when it is created (not inside a   */
+/* stream capture).  pimdal_batch_run then launches a fixed kernel sequence  */
+/* that reads nothing from the host, so it can be captured into a CUDA graph */
+/* and replayed; the inputs are read and the outputs written at run time.    */
+/* ------------------------------------------------------------------------- */
+typedef struct pimdal_batch pimdal_batch_t;
+
+typedef struct {
+  uint32_t rows_per_item;   /* rows of one work item, a multiple of 128 (0 = 65536) */
+  uint32_t load_factor_pct; /* hash-table load factor in percent, 10..90 (0 = 50)   */
+  uint32_t reserved[2];
+} pimdal_batch_tuning_t;
+
+typedef enum { PIMDAL_BATCH_GROUP = 0, PIMDAL_BATCH_HASH_JOIN = 1 } pimdal_batch_kind_t;
+
+/* d_results: device array of count results (instance i -> d_results[i]). */
+int pimdal_group_batch_create(pimdal_ctx_t *ctx, const pimdal_aggr_arguments_t *args,
+                              uint32_t count, const pimdal_batch_tuning_t *tuning,
+                              pimdal_aggr_results_t *d_results, pimdal_batch_t **plan);
+int pimdal_hash_join_batch_create(pimdal_ctx_t *ctx, const pimdal_hash_join_arguments_t *args,
+                                  uint32_t count, const pimdal_batch_tuning_t *tuning,
+                                  pimdal_merge_results_t *d_results, pimdal_batch_t **plan);
+int pimdal_batch_run(pimdal_ctx_t *ctx, pimdal_batch_t *plan, pimdal_stream_t stream);
+int pimdal_batch_device_bytes(const pimdal_batch_t *plan, size_t *bytes);
+int pimdal_batch_destroy(pimdal_batch_t *plan);
+
+/* Autotuner: times the candidate work-item sizes and load factors on these  */
+/* instances (running them, so their outputs are written), returns the      */
+/* fastest and caches it in the context under the batch's shape (kind,      */
+/* count, row and group totals and maxima).  A later call for the same shape */
+/* returns the cached choice without running.  args is a                     */
+/* pimdal_aggr_arguments_t or pimdal_hash_join_arguments_t array; d_results  */
+/* as for the create call.  *cached tells whether the choice came from the   */
+/* cache.                                                                    */
+int pimdal_batch_autotune(pimdal_ctx_t *ctx, int kind, const void *args, uint32_t count,
+                          void *d_results, pimdal_batch_tuning_t *best, int *cached,
+                          pimdal_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -130,6 +130,13 @@ class AggrArguments(C.Structure):
     ]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("rows_per_item", C.c_uint32), ("load_factor_pct", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
+
+
+BATCH_GROUP, BATCH_HASH_JOIN = 0, 1
+
 # Exported symbols and their ctypes signatures.
 _VP, _SZ, _U64, _I = C.c_void_p, C.c_size_t, C.c_uint64, C.c_int
 SIGNATURES = {
@@ -161,6 +168,15 @@ SIGNATURES = {
     "pimdal_hash_join": (_I, [_VP, C.POINTER(HashJoinArguments), _VP, _VP]),
     "pimdal_group_workspace_size": (_I, [C.POINTER(AggrArguments), C.POINTER(_SZ)]),
     "pimdal_group_kernel": (_I, [_VP, C.POINTER(AggrArguments), _VP, _VP]),
+    "pimdal_group_batch_create": (_I, [_VP, C.POINTER(AggrArguments), C.c_uint32,
+                                       C.POINTER(BatchTuning), _VP, C.POINTER(_VP)]),
+    "pimdal_hash_join_batch_create": (_I, [_VP, C.POINTER(HashJoinArguments), C.c_uint32,
+                                           C.POINTER(BatchTuning), _VP, C.POINTER(_VP)]),
+    "pimdal_batch_run": (_I, [_VP, _VP, _VP]),
+    "pimdal_batch_device_bytes": (_I, [_VP, C.POINTER(_SZ)]),
+    "pimdal_batch_destroy": (_I, [_VP]),
+    "pimdal_batch_autotune": (_I, [_VP, _I, _VP, C.c_uint32, _VP, C.POINTER(BatchTuning),
+                                   C.POINTER(_I), _VP]),
 }
 
 _lib = None

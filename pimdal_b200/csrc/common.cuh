@@ -12,6 +12,7 @@
 #include <stdint.h>
 #include <stddef.h>
 
+#include <map>
 #include <vector>
 
 #include "../../include/pimdal_gpu.h"
@@ -62,6 +63,8 @@ struct pimdal_ctx {
   std::vector<cudaEvent_t> prof_free;
   uint64_t prof_launches[PIMDAL_KERNEL_COUNT] = {};
   double prof_ms[PIMDAL_KERNEL_COUNT] = {};
+  // batch autotuner: best tuning per batch shape
+  std::map<std::vector<uint64_t>, pimdal_batch_tuning_t> tune_cache;
 };
 
 // Brackets one launch with timing events when profiling is on.

@@ -40,7 +40,7 @@
 // rows (see k_gb_segreduce).
 #include <algorithm>
 
-#include "common.cuh"
+#include "batch.cuh"
 
 namespace {
 
@@ -138,7 +138,9 @@ struct SmemTable {
   uint32_t *key;
   uint32_t *cnt;
   long long *sum;
-  longlong2 *mm;  // (min, max)
+  longlong2 *mm;     // (min, max)
+  uint16_t *list;    // batched runs: slots claimed since the last flush
+  uint32_t *nlist;
 };
 
 __device__ __forceinline__ int bucket_match(const uint4 &q, uint32_t key) {
@@ -164,6 +166,7 @@ __device__ __noinline__ int smem_find(const SmemTable &t, uint32_t base, uint32_
       continue;
     }
     const uint32_t old = atomicCAS(t.key + s0 + e, GB_EMPTY, key);
+    if (old == GB_EMPTY && t.list) t.list[atomicAdd(t.nlist, 1u)] = (uint16_t)(s0 + e);
     if (old == GB_EMPTY || old == key) return (int)s0 + e;
     // lost the slot to another key: look at the bucket again
   }
@@ -235,45 +238,21 @@ __device__ __forceinline__ void gb_rows4(const GbParams &p, const SmemTable &t, 
   }
 }
 
-// Persistent CTAs; each warp takes 128 consecutive rows per step (4 per lane,
-// one 16-byte key load and two 16-byte value loads when aligned).  In GB_WARP
-// mode each warp's 192 slots form p.wrep private replicas, one per group of
-// 32 / p.wrep lanes.
+// Rows [r0, r1) of p by `warps` warps (this one is number gw): 128
+// consecutive rows per warp step, 4 per lane (one 16-byte key load and two
+// 16-byte value loads when aligned), then the unaligned rest.
 template <int MODE>
-__global__ void __launch_bounds__(GB_THREADS, MODE == GB_DIRECT ? 2 : 1)
-k_gb_aggregate(GbParams p, uint32_t pass) {
-  extern __shared__ __align__(16) unsigned char gb_smem[];
-  SmemTable t;
-  t.key = reinterpret_cast<uint32_t *>(gb_smem);
-  t.cnt = t.key + GB_SMEM_SLOTS;
-  t.sum = reinterpret_cast<long long *>(t.cnt + GB_SMEM_SLOTS);
-  t.mm = reinterpret_cast<longlong2 *>(t.sum + GB_SMEM_SLOTS);
-  if (MODE != GB_DIRECT) {
-    for (uint32_t i = threadIdx.x; i < GB_SMEM_SLOTS; i += GB_THREADS) {
-      t.key[i] = GB_EMPTY;
-      t.cnt[i] = 0;
-      t.sum[i] = 0;
-      t.mm[i] = make_longlong2(INT64_MAX, INT64_MIN);
-    }
-    __syncthreads();
-  }
-  const int lane = threadIdx.x & 31;
-  // shared buckets this lane uses: its warp's replica (GB_WARP) or the CTA table
-  uint32_t base = 0, nb = GB_SMEM_SLOTS / 4;
-  if (MODE == GB_WARP) {
-    nb = GB_WARP_SLOTS / 4 / p.wrep;
-    base = (threadIdx.x >> 5) * (GB_WARP_SLOTS / 4) + (lane / (32 / p.wrep)) * nb;
-  }
-  const uint64_t warps = (uint64_t)gridDim.x * GB_WARPS;
-  const uint64_t gw = (uint64_t)blockIdx.x * GB_WARPS + (threadIdx.x >> 5);
-  uint64_t done = 0;
-  if (p.vec) {
-    const uint64_t nq = p.n / 4;  // quads of rows
+__device__ __forceinline__ void gb_range(const GbParams &p, const SmemTable &t, uint32_t pass,
+                                         uint64_t r0, uint64_t r1, uint64_t gw, uint64_t warps,
+                                         int lane, uint32_t base, uint32_t nb) {
+  uint64_t done = r0;
+  if (p.vec && (r0 & 3u) == 0) {
+    const uint64_t q1 = r1 / 4;  // quads of rows
     const uint4 *k4 = reinterpret_cast<const uint4 *>(p.key);
     const longlong2 *v2 = reinterpret_cast<const longlong2 *>(p.val);
-    for (uint64_t b = gw * 32; b < nq; b += warps * 32) {
+    for (uint64_t b = r0 / 4 + gw * 32; b < q1; b += warps * 32) {
       const uint64_t q = b + lane;
-      const bool ok = q < nq;
+      const bool ok = q < q1;
       uint4 k = make_uint4(0, 0, 0, 0);
       longlong2 va = make_longlong2(1, 1), vb = make_longlong2(1, 1);
       if (ok) {
@@ -292,23 +271,70 @@ k_gb_aggregate(GbParams p, uint32_t pass) {
       const long long vv[4] = {va.x, va.y, vb.x, vb.y};
       gb_rows4<MODE>(p, t, pass, kk, vv, ok ? 0xFu : 0u, base, nb);
     }
-    done = nq * 4;
+    done = q1 * 4;
   }
   // unaligned input or the last rows: lane-striped groups of four rows
-  for (uint64_t b = done + gw * 128; b < p.n; b += warps * 128) {
+  for (uint64_t b = done + gw * 128; b < r1; b += warps * 128) {
     uint32_t kk[4];
     long long vv[4];
     uint32_t valid = 0;
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
       const uint64_t i = b + 32 * r + lane;
-      const bool in = i < p.n;
+      const bool in = i < r1;
       valid |= (uint32_t)in << r;
       kk[r] = in ? p.key[i] : 0u;
       vv[r] = (in && p.val) ? (long long)p.val[i] : 1ll;
     }
     gb_rows4<MODE>(p, t, pass, kk, vv, valid, base, nb);
   }
+}
+
+__device__ __forceinline__ SmemTable gb_smem_table(unsigned char *smem) {
+  SmemTable t;
+  t.key = reinterpret_cast<uint32_t *>(smem);
+  t.cnt = t.key + GB_SMEM_SLOTS;
+  t.sum = reinterpret_cast<long long *>(t.cnt + GB_SMEM_SLOTS);
+  t.mm = reinterpret_cast<longlong2 *>(t.sum + GB_SMEM_SLOTS);
+  t.list = nullptr;
+  t.nlist = nullptr;
+  return t;
+}
+
+__device__ __forceinline__ void gb_clear_slot(const SmemTable &t, uint32_t i) {
+  t.key[i] = GB_EMPTY;
+  t.cnt[i] = 0;
+  t.sum[i] = 0;
+  t.mm[i] = make_longlong2(INT64_MAX, INT64_MIN);
+}
+
+// Shared buckets of this lane: its warp's replica (GB_WARP) or the CTA table.
+__device__ __forceinline__ void gb_buckets(int mode, uint32_t wrep, uint32_t *base, uint32_t *nb) {
+  *base = 0;
+  *nb = GB_SMEM_SLOTS / 4;
+  if (mode == GB_WARP) {
+    const int lane = threadIdx.x & 31;
+    *nb = GB_WARP_SLOTS / 4 / wrep;
+    *base = (threadIdx.x >> 5) * (GB_WARP_SLOTS / 4) + (lane / (32 / wrep)) * *nb;
+  }
+}
+
+// Persistent CTAs over all rows.  In GB_WARP mode each warp's 192 slots form
+// p.wrep private replicas, one per group of 32 / p.wrep lanes.
+template <int MODE>
+__global__ void __launch_bounds__(GB_THREADS, MODE == GB_DIRECT ? 2 : 1)
+k_gb_aggregate(GbParams p, uint32_t pass) {
+  extern __shared__ __align__(16) unsigned char gb_smem[];
+  const SmemTable t = gb_smem_table(gb_smem);
+  if (MODE != GB_DIRECT) {
+    for (uint32_t i = threadIdx.x; i < GB_SMEM_SLOTS; i += GB_THREADS) gb_clear_slot(t, i);
+    __syncthreads();
+  }
+  uint32_t base, nb;
+  gb_buckets(MODE, p.wrep, &base, &nb);
+  const uint64_t warps = (uint64_t)gridDim.x * GB_WARPS;
+  const uint64_t gw = (uint64_t)blockIdx.x * GB_WARPS + (threadIdx.x >> 5);
+  gb_range<MODE>(p, t, pass, 0, p.n, gw, warps, threadIdx.x & 31, base, nb);
   if (MODE != GB_DIRECT) {
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < GB_SMEM_SLOTS; i += GB_THREADS) {
@@ -316,6 +342,185 @@ k_gb_aggregate(GbParams p, uint32_t pass) {
       if (k != GB_EMPTY)
         global_add(p, k, gb_h(k), 0, t.cnt[i], t.sum[i], t.mm[i].x, t.mm[i].y);
     }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Batched group-by (pd_gb_batch): persistent CTAs take (instance, row block)
+// work items from a device queue in instance-major order.  An item's rows go
+// through the CTA's shared table in the instance's mode; at the end of the
+// item the slots it claimed are merged into the instance's global table and
+// reset.  The instances' tables are then compacted together, sorted by key
+// and stably by instance, and gathered into each instance's outputs.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t gbb_inst_of_slot(const pd_gb_batch &b, uint64_t slot) {
+  uint32_t lo = 0, hi = b.count;  // last instance whose slot0 <= slot
+  while (hi - lo > 1) {
+    const uint32_t m = (lo + hi) >> 1;
+    if (b.slot0[m] <= slot) lo = m; else hi = m;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ GbParams gbb_params(const pd_gb_batch &b, const pd_gb_inst &in) {
+  GbParams p{};
+  p.key = in.key;
+  p.val = in.val;
+  p.n = in.n;
+  p.vec = ((uintptr_t)in.key & 15u) == 0 && ((uintptr_t)in.val & 15u) == 0;
+  p.gtab = b.gtab + 4 * in.slot0;
+  p.sub_cap = in.slots;
+  p.npasses = 1;
+  p.wrep = in.wrep;
+  p.d_error = b.d_error;
+  return p;
+}
+
+__global__ void __launch_bounds__(256) k_gbb_init(pd_gb_batch b) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  ulonglong2 *t = reinterpret_cast<ulonglong2 *>(b.gtab);
+  const ulonglong2 lo = make_ulonglong2(0ull, 0ull);
+  const ulonglong2 hi = make_ulonglong2((unsigned long long)INT64_MAX, (unsigned long long)INT64_MIN);
+  const uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint64_t i = i0; i < b.total_slots; i += stride) {
+    t[2 * i] = lo;
+    t[2 * i + 1] = hi;
+  }
+  for (uint64_t i = i0; i < b.count; i += stride) b.inst_groups[i] = 0;
+  if (i0 == 0) *b.ngroups = 0;
+}
+
+__global__ void __launch_bounds__(GB_THREADS, 1) k_gbb_aggregate(pd_gb_batch b) {
+  extern __shared__ __align__(16) unsigned char gb_smem[];
+  __shared__ uint32_t s_item, s_nlist;
+  SmemTable t = gb_smem_table(gb_smem);
+  t.list = reinterpret_cast<uint16_t *>(gb_smem + GB_SMEM_BYTES);
+  t.nlist = &s_nlist;
+  for (uint32_t i = threadIdx.x; i < GB_SMEM_SLOTS; i += GB_THREADS) gb_clear_slot(t, i);
+  if (threadIdx.x == 0) s_nlist = 0;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = threadIdx.x >> 5;
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const uint32_t it = atomicAdd(b.counters, 1u);
+      if (it >= b.nitems && atomicAdd(b.counters + 1, 1u) == gridDim.x - 1) {
+        b.counters[0] = 0;  // the last claimer of the launch resets the queue
+        b.counters[1] = 0;
+      }
+      s_item = it;
+    }
+    __syncthreads();
+    const uint32_t it = s_item;
+    if (it >= b.nitems) break;
+    const uint2 item = b.items[it];
+    const pd_gb_inst &in = b.inst[item.x];
+    const GbParams p = gbb_params(b, in);
+    const uint64_t r0 = item.y, r1 = min((uint64_t)item.y + b.rows_per_item, in.n);
+    const int mode = (int)in.mode;
+    uint32_t base, nb;
+    gb_buckets(mode, in.wrep, &base, &nb);
+    if (mode == GB_WARP) gb_range<GB_WARP>(p, t, 0, r0, r1, warp, GB_WARPS, lane, base, nb);
+    else if (mode == GB_SMEM) gb_range<GB_SMEM>(p, t, 0, r0, r1, warp, GB_WARPS, lane, base, nb);
+    else gb_range<GB_DIRECT>(p, t, 0, r0, r1, warp, GB_WARPS, lane, base, nb);
+    if (mode != GB_DIRECT) {
+      __syncthreads();
+      const uint32_t nl = s_nlist;
+      for (uint32_t i = threadIdx.x; i < nl; i += GB_THREADS) {
+        const uint32_t j = t.list[i];
+        const uint32_t k = t.key[j];
+        global_add(p, k, gb_h(k), 0, t.cnt[j], t.sum[j], t.mm[j].x, t.mm[j].y);
+        gb_clear_slot(t, j);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) s_nlist = 0;
+    }
+  }
+}
+
+// Occupied slots of every instance -> (order-transformed key, slot).
+__global__ void __launch_bounds__(256) k_gbb_compact(pd_gb_batch b) {
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const int lane = threadIdx.x & 31;
+  for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < b.total_slots; base += stride) {
+    const uint64_t i = base + threadIdx.x;
+    const unsigned long long w = i < b.total_slots ? __ldcs(b.gtab + 4 * i) : 0ull;
+    const unsigned m = __ballot_sync(0xffffffffu, w != 0);
+    if (!m) continue;
+    uint32_t pos = 0;
+    if (lane == 0) pos = (uint32_t)atomicAdd(b.ngroups, (unsigned long long)__popc(m));
+    pos = __shfl_sync(0xffffffffu, pos, 0) + __popc(m & ((1u << lane) - 1u));
+    if (w) {
+      const uint32_t inst = gbb_inst_of_slot(b, i);
+      atomicAdd(b.inst_groups + inst, 1u);
+      b.ckey[pos] = (uint32_t)w ^ b.inst[inst].flip;
+      b.cslot[pos] = (uint32_t)i;
+    }
+  }
+}
+
+// Key-ordered (key, slot) -> (instance, slot) for the stable sort by instance.
+__global__ void __launch_bounds__(256) k_gbb_inst(pd_gb_batch b) {
+  const uint64_t n = *b.ngroups;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t slot = b.sslot[i];
+    b.ikey[i] = gbb_inst_of_slot(b, slot);
+    b.islot[i] = slot;
+  }
+}
+
+// Per-instance first position and group count (one block).
+__global__ void __launch_bounds__(1024) k_gbb_start(pd_gb_batch b) {
+  __shared__ uint64_t s_w[32];
+  __shared__ uint64_t s_carry;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) s_carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < b.count; base += 1024) {
+    const uint32_t i = base + tid;
+    const uint64_t v = i < b.count ? b.inst_groups[i] : 0;
+    uint64_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    if (lane == 31) s_w[warp] = inc;
+    __syncthreads();
+    uint64_t pre = 0, tot = 0;
+    for (int w = 0; w < 32; ++w) {
+      if (w < warp) pre += s_w[w];
+      tot += s_w[w];
+    }
+    if (i < b.count) {
+      b.inst_start[i] = s_carry + pre + inc - v;
+      const pd_gb_inst &in = b.inst[i];
+      *in.d_count = v;
+      if (v > in.out_cap) atomicOr(b.d_error, PD_DEVERR_CAPACITY);
+    }
+    __syncthreads();
+    if (tid == 0) s_carry += tot;
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) k_gbb_gather(pd_gb_batch b) {
+  const uint64_t n = *b.ngroups;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const ulonglong2 *t = reinterpret_cast<const ulonglong2 *>(b.gtab);
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const uint32_t inst = b.ckey[i];
+    const uint64_t s = b.cslot[i];
+    const pd_gb_inst &in = b.inst[inst];
+    const uint64_t j = i - b.inst_start[inst];
+    if (j >= in.out_cap) continue;
+    const ulonglong2 x = t[2 * s], y = t[2 * s + 1];
+    if (in.out_key) in.out_key[j] = (uint32_t)x.x;
+    if (in.out_sum) in.out_sum[j] = (int64_t)x.y;
+    if (in.out_count) in.out_count[j] = (int64_t)(x.x >> 32);
+    if (in.out_min) in.out_min[j] = (int64_t)y.x;
+    if (in.out_max) in.out_max[j] = (int64_t)y.y;
   }
 }
 
@@ -691,6 +896,65 @@ bool gb_layout(const pimdal_aggr_arguments_t *a, GbLayout *l) {
 }
 
 }  // namespace
+
+void pd_gb_mode(uint64_t expect, uint32_t *mode, uint32_t *wrep) {
+  expect = std::max<uint64_t>(expect, 1);
+  *mode = expect <= GB_WARP_MAX_GROUPS ? GB_WARP : expect <= GB_SMEM_MAX_GROUPS ? GB_SMEM : GB_DIRECT;
+  *wrep = expect <= 16 ? 4 : expect <= 32 ? 2 : 1;
+}
+
+size_t pd_gb_batch_shared_bytes() { return GB_SMEM_BYTES + 2 * GB_SMEM_SLOTS; }
+
+int pd_gb_batch_run(pimdal_ctx *ctx, const pd_gb_batch &b, cudaStream_t s) {
+  const unsigned grid = (unsigned)std::min<uint64_t>(pd_ceil_div(std::max<uint64_t>(b.total_slots, 1), 256),
+                                                     ctx->sm_count * 8ull);
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_gbb_init<<<grid, 256, 0, s>>>(b);
+  }
+  if (b.nitems) {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_GROUP, s);
+    const size_t smem = pd_gb_batch_shared_bytes();
+    PD_CHECK_CUDA(cudaFuncSetAttribute(k_gbb_aggregate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_gbb_aggregate<<<std::min<unsigned>(ctx->sm_count, b.nitems), GB_THREADS, smem, s>>>(b);
+  }
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_gbb_compact<<<grid, 256, 0, s>>>(b);
+  }
+  int st;
+  pimdal_sort_arguments_t sa{};
+  sa.key_dtype = PIMDAL_U32;
+  sa.layout = PIMDAL_LAYOUT_COLUMNS;
+  sa.nr_elements = std::max<uint64_t>(b.total_slots, 1);
+  sa.in = b.ckey;
+  sa.in_ptr = b.cslot;
+  sa.out = b.skey;
+  sa.out_ptr = b.sslot;
+  if ((st = pd_sort_ex2(ctx, &sa, PD_KEY_PLAIN, b.sort_ws, s, nullptr, (const uint64_t *)b.ngroups)))
+    return st;
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_gbb_inst<<<grid, 256, 0, s>>>(b);
+  }
+  sa.in = b.ikey;
+  sa.in_ptr = b.islot;
+  sa.out = b.ckey;
+  sa.out_ptr = b.cslot;
+  sa.begin_bit = 0;
+  sa.end_bit = b.inst_bits;
+  if ((st = pd_sort_ex2(ctx, &sa, PD_KEY_PLAIN, b.sort_ws, s, nullptr, (const uint64_t *)b.ngroups)))
+    return st;
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_gbb_start<<<1, 1024, 0, s>>>(b);
+  }
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_gbb_gather<<<grid, 256, 0, s>>>(b);
+  }
+  return pd_launch_status(ctx);
+}
 
 extern "C" int pimdal_group_workspace_size(const pimdal_aggr_arguments_t *a, size_t *bytes) {
   if (!a || !bytes) return PIMDAL_ERR_ARG;

@@ -33,7 +33,7 @@
 //    partition, partitions in order.
 #include <algorithm>
 
-#include "common.cuh"
+#include "batch.cuh"
 
 namespace {
 
@@ -43,6 +43,19 @@ constexpr int HJ_ITEMS = 16;
 constexpr int HJ_TILE = HJ_THREADS * HJ_ITEMS;  // 4096 probe rows per tile
 constexpr int HJ_BATCH = 2;
 constexpr uint32_t HJ_MIN_BITS = 10;
+
+}  // namespace
+
+// log2 of the slots of a table for nb build rows at load_pct percent.
+uint32_t pd_hj_table_bits(uint64_t nb, uint32_t load_pct) {
+  uint64_t cap = 1ull << HJ_MIN_BITS;
+  while (cap * load_pct < nb * 100) cap <<= 1;
+  uint32_t bits = 0;
+  while ((1ull << bits) < cap) ++bits;
+  return bits;
+}
+
+namespace {
 
 // Home bucket of a key: buckets are aligned groups of 4 slots (one 32-byte
 // sector); a table of 2^bits slots has 2^(bits-2) buckets.
@@ -102,45 +115,47 @@ __global__ void __launch_bounds__(256) k_hj_clear(JoinParams p) {
   }
 }
 
+// Inserts one build row (bucketized linear probing: the first free slot of the
+// first bucket, from the home bucket on, that has one; every copy of a key
+// therefore lies between its home bucket and the first bucket with a free
+// slot).  The one row whose slot word would equal the empty word is counted
+// on the side.
+__device__ __forceinline__ void hj_insert(const JoinParams &p, uint32_t k, uint32_t v) {
+  const unsigned long long e = ((unsigned long long)v << 32) | k;
+  if (e == HJ_EMPTY) {
+    atomicAdd(p.side_count, 1u);
+    return;
+  }
+  const uint64_t gmask = ((1ull << p.bits) - 1) >> 2;
+  uint64_t g = bucket_of(k, p.part_bits, p.bits);
+  bool done = false;
+  bool dup = false;
+  for (uint64_t t = 0; t <= gmask && !done; ++t) {
+    unsigned long long *b = p.table + 4 * g;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (done) break;
+      const unsigned long long cur = b[j];
+      if (cur != HJ_EMPTY) {
+        dup |= (uint32_t)cur == k;
+        continue;
+      }
+      const unsigned long long old = atomicCAS(b + j, HJ_EMPTY, e);
+      if (old == HJ_EMPTY) done = true;
+      else dup |= (uint32_t)old == k;
+    }
+    g = (g + 1) & gmask;
+  }
+  if (dup) *p.dup_flag = 1;
+  if (!done) atomicOr(p.d_error, PD_DEVERR_TABLE_FULL);
+}
+
 __global__ void __launch_bounds__(256) k_hj_build(JoinParams p) {
   uint64_t lo, hi;
   part_range(p.boff, p.part, p.nb, &lo, &hi);
-  const uint64_t mask = (1ull << p.bits) - 1;
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-  for (uint64_t i = lo + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < hi; i += stride) {
-    const uint32_t k = p.bkey[i];
-    const uint32_t v = p.bpay ? p.bpay[i] : (uint32_t)i;
-    const unsigned long long e = ((unsigned long long)v << 32) | k;
-    if (e == HJ_EMPTY) {
-      atomicAdd(p.side_count, 1u);
-      continue;
-    }
-    // Bucketized linear probing: the first free slot of the first bucket
-    // (from the home bucket on) that has one.  Every copy of a key therefore
-    // lies between its home bucket and the first bucket with a free slot.
-    const uint64_t gmask = mask >> 2;
-    uint64_t g = bucket_of(k, p.part_bits, p.bits);
-    bool done = false;
-    bool dup = false;
-    for (uint64_t t = 0; t <= gmask && !done; ++t) {
-      unsigned long long *b = p.table + 4 * g;
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        if (done) break;
-        const unsigned long long cur = b[j];
-        if (cur != HJ_EMPTY) {
-          dup |= (uint32_t)cur == k;
-          continue;
-        }
-        const unsigned long long old = atomicCAS(b + j, HJ_EMPTY, e);
-        if (old == HJ_EMPTY) done = true;
-        else dup |= (uint32_t)old == k;
-      }
-      g = (g + 1) & gmask;
-    }
-    if (dup) *p.dup_flag = 1;
-    if (!done) atomicOr(p.d_error, PD_DEVERR_TABLE_FULL);
-  }
+  for (uint64_t i = lo + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < hi; i += stride)
+    hj_insert(p, p.bkey[i], p.bpay ? p.bpay[i] : (uint32_t)i);
 }
 
 // Resolves one bucket of a probe row: adds its matches to *c (first payload
@@ -189,24 +204,172 @@ __device__ __noinline__ uint32_t emit_all(const JoinParams &p, uint32_t key, uin
   return c;
 }
 
-__global__ void __launch_bounds__(HJ_THREADS, 3) k_hj_probe(JoinParams p) {
+// One probe tile: rows [row0, min(row0 + HJ_TILE, hi)) of p, tile index gtile
+// in p.status (the tile with index 0 starts the chain).  When count_last,
+// the tile also stores the inclusive match count in *p.d_count.
+__device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0, uint64_t hi,
+                                              uint64_t gtile, uint32_t side, bool stop_first,
+                                              bool count_last) {
   __shared__ uint32_t s_warp[HJ_THREADS / 32];
   __shared__ uint32_t s_flags[2 * (HJ_THREADS / 32)];
   __shared__ uint64_t s_sum[HJ_THREADS / 32 + 1];
   __shared__ int s_state;
-  __shared__ uint64_t s_tile, s_prefix;
+  __shared__ uint64_t s_prefix;
   __shared__ uint32_t s_first[HJ_ITEMS][HJ_THREADS];  // first payload of each row
-
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t mask = (1ull << p.bits) - 1;
+  const uint32_t lt = (1u << lane) - 1u;
+  // Warp-striped rows: row k of this lane is wbase + 32k + lane.
+  const uint64_t wbase = row0 + (uint64_t)warp * (32 * HJ_ITEMS);
+
+  // Phase 1: match counts (4 bits per row, 15 = "count again") and first payloads.
+  uint64_t cnt4 = 0;
+  uint32_t mine = 0;
+#pragma unroll
+  for (int b = 0; b < HJ_ITEMS; b += HJ_BATCH) {
+    uint32_t key[HJ_BATCH], c[HJ_BATCH], fk[HJ_BATCH];
+    uint64_t g[HJ_BATCH];
+    bool active[HJ_BATCH];
+#pragma unroll
+    for (int i = 0; i < HJ_BATCH; ++i) {
+      const uint64_t r = wbase + (uint64_t)(b + i) * 32 + lane;
+      active[i] = r < hi;
+      key[i] = active[i] ? __ldcs(p.pkey + r) : 0u;
+      g[i] = bucket_of(key[i], p.part_bits, p.bits);
+      c[i] = 0;
+      fk[i] = 0;
+    }
+    // Lockstep bucket walks: all loads of a round are in flight together;
+    // almost every row resolves in its home bucket.
+    const uint64_t gmask = mask >> 2;
+    for (uint64_t round = 0; round <= gmask; ++round) {
+      ulonglong2 glo[HJ_BATCH], ghi[HJ_BATCH];
+      bool any = false;
+#pragma unroll
+      for (int i = 0; i < HJ_BATCH; ++i) {
+        if (active[i]) {
+          const ulonglong2 *q = reinterpret_cast<const ulonglong2 *>(p.table + 4 * g[i]);
+          glo[i] = q[0];
+          ghi[i] = q[1];
+          any = true;
+        }
+      }
+      if (!any) break;
+#pragma unroll
+      for (int i = 0; i < HJ_BATCH; ++i) {
+        if (!active[i]) continue;
+        if (resolve_bucket(glo[i], ghi[i], key[i], stop_first && key[i] != 0xFFFFFFFFu, &c[i],
+                           &fk[i]))
+          active[i] = false;
+        g[i] = (g[i] + 1) & gmask;
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < HJ_BATCH; ++i) {
+      const int k = b + i;
+      const uint64_t r = wbase + (uint64_t)k * 32 + lane;
+      uint32_t ci = c[i];
+      if (r < hi && key[i] == 0xFFFFFFFFu) ci += side;
+      s_first[k][tid] = fk[i];
+      mine += ci;
+      cnt4 |= (uint64_t)(ci < 15 ? ci : 15u) << (4 * k);
+    }
+  }
+  // Block scan of per-thread totals; tile look-back.
+  uint32_t inc = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += t;
+  }
+  const uint32_t wtot = __shfl_sync(0xffffffffu, inc, 31);
+  if (lane == 0) s_warp[warp] = wtot;
+  __syncthreads();
+  uint32_t wpre = 0, total = 0;
+#pragma unroll
+  for (int w = 0; w < HJ_THREADS / 32; ++w) {
+    uint32_t x = s_warp[w];
+    if (w < warp) wpre += x;
+    total += x;
+  }
+  if (gtile == 0) {
+    if (tid == 0) {
+      pd_store_relaxed_u64(p.status, pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, total));
+      s_prefix = 0;
+    }
+  } else {
+    if (tid == 0)
+      pd_store_relaxed_u64(p.status + gtile, pd_pack_status(p.epoch, PD_FLAG_AGGREGATE, total));
+    uint64_t pre = pd_block_lookback<HJ_THREADS>(p.status, (int64_t)gtile, p.epoch, p.d_error,
+                                                 s_flags, s_sum, &s_state);
+    if (tid == 0) {
+      pd_store_relaxed_u64(p.status + gtile,
+                           pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, pre + total));
+      s_prefix = pre;
+    }
+  }
+  __syncthreads();
+  // Phase 2: rows in order (k-major, then lane) -> consecutive output slots.
+  uint64_t w = s_prefix + wpre;
+  bool overflow = false;
+#pragma unroll
+  for (int k = 0; k < HJ_ITEMS; ++k) {
+    const uint32_t c4 = (uint32_t)(cnt4 >> (4 * k)) & 15u;
+    const uint64_t r = wbase + (uint64_t)k * 32 + lane;
+    const bool simple = c4 <= 1;
+    if (__all_sync(0xffffffffu, simple)) {
+      const unsigned m = __ballot_sync(0xffffffffu, c4 == 1);
+      if (c4 == 1) {
+        const uint64_t pos = w + __popc(m & lt);
+        const uint32_t row = p.prow ? p.prow[r] : (uint32_t)r;
+        if (pos < p.cap) { p.out_pay[pos] = s_first[k][tid]; p.out_row[pos] = row; } else overflow = true;
+      }
+      w += __popc(m);
+    } else {
+      // some lane has several matches: exact counts by a second walk
+      uint32_t c = 0;
+      const uint32_t key = (r < hi && c4) ? p.pkey[r] : 0u;
+      if (c4 == 1) c = 1;
+      else if (c4 > 1) {
+        bool dummy = false;
+        c = emit_all(p, key, mask, 0, 0, &dummy, false);  // count only
+        if (key == 0xFFFFFFFFu) c += side;
+      }
+      uint32_t ci = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, ci, o);
+        if (lane >= o) ci += t;
+      }
+      const uint64_t pos = w + ci - c;
+      const uint32_t row = c ? (p.prow ? p.prow[r] : (uint32_t)r) : 0u;
+      if (c4 == 1) {
+        if (pos < p.cap) { p.out_pay[pos] = s_first[k][tid]; p.out_row[pos] = row; } else overflow = true;
+      } else if (c) {
+        uint64_t q = pos + emit_all(p, key, mask, pos, row, &overflow, true);
+        if (key == 0xFFFFFFFFu) {
+          for (uint32_t m2 = 0; m2 < side; ++m2, ++q) {
+            if (q < p.cap) { p.out_pay[q] = 0xFFFFFFFFu; p.out_row[q] = row; } else overflow = true;
+          }
+        }
+      }
+      w += __shfl_sync(0xffffffffu, ci, 31);
+    }
+  }
+  if (overflow) atomicOr(p.d_error, PD_DEVERR_CAPACITY);
+  if (count_last && tid == 0) *p.d_count = s_prefix + total;
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(HJ_THREADS, 3) k_hj_probe(JoinParams p) {
+  __shared__ uint64_t s_tile;
+  const int tid = threadIdx.x;
   uint64_t lo, hi;
   part_range(p.poff, p.part, p.np, &lo, &hi);
   const uint64_t tiles = pd_ceil_div(hi - lo, HJ_TILE);
   const uint64_t gbase = p.tilebase ? p.tilebase[p.part] : 0;
-  const uint64_t mask = (1ull << p.bits) - 1;
   const uint32_t side = *p.side_count;
   const bool stop_first = *p.dup_flag == 0;
-  const uint32_t lt = (1u << lane) - 1u;
-
   while (true) {
     if (tid == 0) {
       uint64_t t = atomicAdd(p.claim, 1u);
@@ -219,146 +382,7 @@ __global__ void __launch_bounds__(HJ_THREADS, 3) k_hj_probe(JoinParams p) {
     __syncthreads();
     const uint64_t tl = s_tile;
     if (tl >= tiles) break;
-    const uint64_t gtile = gbase + tl;
-    // Warp-striped rows: row k of this lane is wbase + 32k + lane.
-    const uint64_t wbase = lo + tl * HJ_TILE + (uint64_t)warp * (32 * HJ_ITEMS);
-
-    // Phase 1: match counts (4 bits per row, 15 = "count again") and first payloads.
-    uint64_t cnt4 = 0;
-    uint32_t mine = 0;
-#pragma unroll
-    for (int b = 0; b < HJ_ITEMS; b += HJ_BATCH) {
-      uint32_t key[HJ_BATCH], c[HJ_BATCH], fk[HJ_BATCH];
-      uint64_t g[HJ_BATCH];
-      bool active[HJ_BATCH];
-#pragma unroll
-      for (int i = 0; i < HJ_BATCH; ++i) {
-        const uint64_t r = wbase + (uint64_t)(b + i) * 32 + lane;
-        active[i] = r < hi;
-        key[i] = active[i] ? __ldcs(p.pkey + r) : 0u;
-        g[i] = bucket_of(key[i], p.part_bits, p.bits);
-        c[i] = 0;
-        fk[i] = 0;
-      }
-      // Lockstep bucket walks: all loads of a round are in flight together;
-      // almost every row resolves in its home bucket.
-      const uint64_t gmask = mask >> 2;
-      for (uint64_t round = 0; round <= gmask; ++round) {
-        ulonglong2 glo[HJ_BATCH], ghi[HJ_BATCH];
-        bool any = false;
-#pragma unroll
-        for (int i = 0; i < HJ_BATCH; ++i) {
-          if (active[i]) {
-            const ulonglong2 *q = reinterpret_cast<const ulonglong2 *>(p.table + 4 * g[i]);
-            glo[i] = q[0];
-            ghi[i] = q[1];
-            any = true;
-          }
-        }
-        if (!any) break;
-#pragma unroll
-        for (int i = 0; i < HJ_BATCH; ++i) {
-          if (!active[i]) continue;
-          if (resolve_bucket(glo[i], ghi[i], key[i], stop_first && key[i] != 0xFFFFFFFFu, &c[i],
-                             &fk[i]))
-            active[i] = false;
-          g[i] = (g[i] + 1) & gmask;
-        }
-      }
-#pragma unroll
-      for (int i = 0; i < HJ_BATCH; ++i) {
-        const int k = b + i;
-        const uint64_t r = wbase + (uint64_t)k * 32 + lane;
-        uint32_t ci = c[i];
-        if (r < hi && key[i] == 0xFFFFFFFFu) ci += side;
-        s_first[k][tid] = fk[i];
-        mine += ci;
-        cnt4 |= (uint64_t)(ci < 15 ? ci : 15u) << (4 * k);
-      }
-    }
-    // Block scan of per-thread totals; tile look-back.
-    uint32_t inc = mine;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
-      if (lane >= o) inc += t;
-    }
-    const uint32_t wtot = __shfl_sync(0xffffffffu, inc, 31);
-    if (lane == 0) s_warp[warp] = wtot;
-    __syncthreads();
-    uint32_t wpre = 0, total = 0;
-#pragma unroll
-    for (int w = 0; w < HJ_THREADS / 32; ++w) {
-      uint32_t x = s_warp[w];
-      if (w < warp) wpre += x;
-      total += x;
-    }
-    if (gtile == 0) {
-      if (tid == 0) {
-        pd_store_relaxed_u64(p.status, pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, total));
-        s_prefix = 0;
-      }
-    } else {
-      if (tid == 0)
-        pd_store_relaxed_u64(p.status + gtile, pd_pack_status(p.epoch, PD_FLAG_AGGREGATE, total));
-      uint64_t pre = pd_block_lookback<HJ_THREADS>(p.status, (int64_t)gtile, p.epoch, p.d_error,
-                                                   s_flags, s_sum, &s_state);
-      if (tid == 0) {
-        pd_store_relaxed_u64(p.status + gtile,
-                             pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, pre + total));
-        s_prefix = pre;
-      }
-    }
-    __syncthreads();
-    // Phase 2: rows in order (k-major, then lane) -> consecutive output slots.
-    uint64_t w = s_prefix + wpre;
-    bool overflow = false;
-#pragma unroll
-    for (int k = 0; k < HJ_ITEMS; ++k) {
-      const uint32_t c4 = (uint32_t)(cnt4 >> (4 * k)) & 15u;
-      const uint64_t r = wbase + (uint64_t)k * 32 + lane;
-      const bool simple = c4 <= 1;
-      if (__all_sync(0xffffffffu, simple)) {
-        const unsigned m = __ballot_sync(0xffffffffu, c4 == 1);
-        if (c4 == 1) {
-          const uint64_t pos = w + __popc(m & lt);
-          const uint32_t row = p.prow ? p.prow[r] : (uint32_t)r;
-          if (pos < p.cap) { p.out_pay[pos] = s_first[k][tid]; p.out_row[pos] = row; } else overflow = true;
-        }
-        w += __popc(m);
-      } else {
-        // some lane has several matches: exact counts by a second walk
-        uint32_t c = 0;
-        const uint32_t key = (r < hi && c4) ? p.pkey[r] : 0u;
-        if (c4 == 1) c = 1;
-        else if (c4 > 1) {
-          bool dummy = false;
-          c = emit_all(p, key, mask, 0, 0, &dummy, false);  // count only
-          if (key == 0xFFFFFFFFu) c += side;
-        }
-        uint32_t ci = c;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          uint32_t t = __shfl_up_sync(0xffffffffu, ci, o);
-          if (lane >= o) ci += t;
-        }
-        const uint64_t pos = w + ci - c;
-        const uint32_t row = c ? (p.prow ? p.prow[r] : (uint32_t)r) : 0u;
-        if (c4 == 1) {
-          if (pos < p.cap) { p.out_pay[pos] = s_first[k][tid]; p.out_row[pos] = row; } else overflow = true;
-        } else if (c) {
-          uint64_t q = pos + emit_all(p, key, mask, pos, row, &overflow, true);
-          if (key == 0xFFFFFFFFu) {
-            for (uint32_t m2 = 0; m2 < side; ++m2, ++q) {
-              if (q < p.cap) { p.out_pay[q] = 0xFFFFFFFFu; p.out_row[q] = row; } else overflow = true;
-            }
-          }
-        }
-        w += __shfl_sync(0xffffffffu, ci, 31);
-      }
-    }
-    if (overflow) atomicOr(p.d_error, PD_DEVERR_CAPACITY);
-    __syncthreads();
+    hj_probe_tile(p, lo + tl * HJ_TILE, hi, gbase + tl, side, stop_first, false);
   }
 }
 
@@ -393,6 +417,94 @@ __global__ void k_hj_offsets(const uint32_t *boffs, const uint32_t *poffs, uint3
   tilebase[parts] = (uint32_t)t;
 }
 
+// ---------------------------------------------------------------------------
+// Batched hash join (pd_hj_batch): every instance has its own table (never
+// partitioned).  Build: CTAs take (instance, row block) items.  Probe:
+// persistent CTAs claim probe tiles in instance-major order; each instance's
+// tiles form their own look-back chain (status words from the instance's
+// first tile), so every instance's output is in probe order, exactly as its
+// plain unpartitioned join.  The look-back epoch lives on the device and is
+// advanced by the run itself, so a captured run can be replayed.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ JoinParams hjb_params(const pd_hj_batch &b, const pd_hj_inst &in) {
+  JoinParams p{};
+  p.table = in.table;
+  p.bits = in.bits;
+  p.part_bits = 0;
+  p.side_count = in.header;
+  p.dup_flag = in.header + 2;
+  p.bkey = in.bkey;
+  p.bpay = in.bpay;
+  p.nb = in.nb;
+  p.pkey = in.pkey;
+  p.prow = in.prow;
+  p.np = in.np;
+  p.out_pay = in.out_pay;
+  p.out_row = in.out_row;
+  p.cap = in.cap;
+  p.status = b.status + in.tile0;
+  p.d_error = b.d_error;
+  p.d_count = in.d_count;
+  return p;
+}
+
+// Advances the device epoch (1..65535); instances without probe rows get a
+// zero count (no tile of theirs will write it).
+__global__ void k_hjb_begin(pd_hj_batch b) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == 0) *b.epoch = *b.epoch % 65535u + 1u;
+  if (i < b.count && b.tile0[i + 1] == b.tile0[i]) *b.inst[i].d_count = 0;
+}
+
+// After a wrap of the epoch, stale words could carry the new epoch: clear them.
+__global__ void __launch_bounds__(256) k_hjb_status_clear(pd_hj_batch b) {
+  if (*b.epoch != 1u) return;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < b.total_tiles; i += stride)
+    b.status[i] = 0;
+}
+
+__global__ void __launch_bounds__(256) k_hjb_build(pd_hj_batch b) {
+  for (uint32_t it = blockIdx.x; it < b.nbitems; it += gridDim.x) {
+    const uint2 item = b.bitems[it];
+    const pd_hj_inst &in = b.inst[item.x];
+    const JoinParams p = hjb_params(b, in);
+    const uint64_t r1 = min((uint64_t)item.y + b.build_rows_per_item, in.nb);
+    for (uint64_t i = item.y + threadIdx.x; i < r1; i += blockDim.x)
+      hj_insert(p, p.bkey[i], p.bpay ? p.bpay[i] : (uint32_t)i);
+  }
+}
+
+__global__ void __launch_bounds__(HJ_THREADS, 3) k_hjb_probe(pd_hj_batch b) {
+  __shared__ uint64_t s_tile;
+  const int tid = threadIdx.x;
+  const uint32_t epoch = *b.epoch;
+  while (true) {
+    if (tid == 0) {
+      const uint64_t t = atomicAdd(b.counters, 1u);
+      if (t >= b.total_tiles && atomicAdd(b.counters + 1, 1u) == gridDim.x - 1) {
+        b.counters[0] = 0;  // the last claimer of the launch resets the queue
+        b.counters[1] = 0;
+      }
+      s_tile = t;
+    }
+    __syncthreads();
+    const uint64_t t = s_tile;
+    if (t >= b.total_tiles) break;
+    uint32_t lo = 0, hi = b.count;  // the instance whose tiles contain t
+    while (hi - lo > 1) {
+      const uint32_t m = (lo + hi) >> 1;
+      if (b.tile0[m] <= t) lo = m; else hi = m;
+    }
+    const pd_hj_inst &in = b.inst[lo];
+    JoinParams p = hjb_params(b, in);
+    p.epoch = epoch;
+    const uint64_t tl = t - in.tile0;
+    const uint64_t tiles = pd_ceil_div(in.np, HJ_TILE);
+    hj_probe_tile(p, tl * HJ_TILE, in.np, tl, *p.side_count, *p.dup_flag == 0, tl == tiles - 1);
+  }
+}
+
 int probe_grid(pimdal_ctx *ctx) {
   static int per_sm = 0;
   if (!per_sm) {
@@ -408,12 +520,9 @@ struct HjLayout {
 };
 
 bool hj_layout(const pimdal_hash_join_arguments_t *a, HjLayout *l) {
-  uint64_t cap = 1ull << HJ_MIN_BITS;
   const uint32_t load_pct = a->load_factor_pct ? a->load_factor_pct : 50;
   if (load_pct > 90) return false;
-  while (cap * load_pct < a->size_build * 100) cap <<= 1;
-  uint32_t bits = 0;
-  while ((1ull << bits) < cap) ++bits;
+  const uint32_t bits = pd_hj_table_bits(a->size_build, load_pct);
   uint64_t budget = a->l2_budget_bytes ? a->l2_budget_bytes : (48ull << 20);
   uint32_t pb = a->partition_bits;
   if (pb == 0xFFFFFFFFu) pb = 0;  // explicit "no partitioning"
@@ -448,6 +557,37 @@ bool hj_layout(const pimdal_hash_join_arguments_t *a, HjLayout *l) {
 }
 
 }  // namespace
+
+uint32_t pd_hj_tile_rows() { return HJ_TILE; }
+
+int pd_hj_batch_run(pimdal_ctx *ctx, const pd_hj_batch &b, cudaStream_t s) {
+  if (b.table_words) PD_CHECK_CUDA(cudaMemsetAsync(b.tables, 0xFF, 8 * b.table_words, s));
+  PD_CHECK_CUDA(cudaMemsetAsync(b.headers, 0, 32ull * b.count, s));
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_hjb_begin<<<(b.count + 255) / 256, 256, 0, s>>>(b);
+  }
+  if (b.total_tiles) {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    const unsigned g = (unsigned)std::min<uint64_t>(pd_ceil_div(b.total_tiles, 256), ctx->sm_count * 4ull);
+    k_hjb_status_clear<<<g, 256, 0, s>>>(b);
+  }
+  if (b.nbitems) {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_HJ_BUILD, s);
+    k_hjb_build<<<std::min<unsigned>(b.nbitems, ctx->sm_count * 8), 256, 0, s>>>(b);
+  }
+  if (b.total_tiles) {
+    static int per_sm = 0;
+    if (!per_sm) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hjb_probe, HJ_THREADS, 0);
+      if (per_sm <= 0) per_sm = 1;
+    }
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_HJ_PROBE, s);
+    const unsigned g = (unsigned)std::min<uint64_t>(b.total_tiles, (uint64_t)per_sm * ctx->sm_count);
+    k_hjb_probe<<<g, HJ_THREADS, 0, s>>>(b);
+  }
+  return pd_launch_status(ctx);
+}
 
 // ---------------------------------------------------------------------------
 // pimdal_hash_join

@@ -323,3 +323,89 @@ def group_kernel(ctx: Context, keys, vals=None, *, method: int = L.GROUP_HASH,
     L.check(ctx.lib.pimdal_group_kernel(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
             "pimdal_group_kernel")
     return result, outs
+
+
+# ---------------------------------------------------------------------------
+# Batched form (pimdal_group_batch_create / pimdal_hash_join_batch_create)
+# ---------------------------------------------------------------------------
+def group_args(keys, vals, outs, *, expected_groups: int = 0, capacity: int | None = None,
+               key_dtype: int = L.I32, method: int = L.GROUP_HASH) -> L.AggrArguments:
+    """Argument struct of one group-by instance (outputs: dict as group_kernel)."""
+    n = keys.numel()
+    if capacity is None:
+        capacity = outs["key"].numel() if "key" in outs else max(n, 1)
+    return L.AggrArguments(size=n, in_=_ptr(keys), in_val=_ptr(vals), out=_ptr(outs.get("key")),
+                           out_sum=_ptr(outs.get("sum")), out_count=_ptr(outs.get("count")),
+                           out_min=_ptr(outs.get("min")), out_max=_ptr(outs.get("max")),
+                           out_capacity=capacity, expected_groups=expected_groups,
+                           key_dtype=key_dtype, method=method)
+
+
+def hash_join_args(build_key, build_payload, probe_key, probe_ptr, out_payload, out_row, *,
+                   capacity: int | None = None, load_factor_pct: int = 0) -> L.HashJoinArguments:
+    """Argument struct of one (unpartitioned) hash-join instance."""
+    if capacity is None:
+        capacity = out_payload.numel()
+    return L.HashJoinArguments(build_key=_ptr(build_key), build_payload=_ptr(build_payload),
+                               size_build=build_key.numel(), probe_key=_ptr(probe_key),
+                               probe_ptr=_ptr(probe_ptr), size_probe=probe_key.numel(),
+                               out_build_payload=_ptr(out_payload), out_probe_ptr=_ptr(out_row),
+                               out_capacity=capacity, partition_bits=0xFFFFFFFF,
+                               load_factor_pct=load_factor_pct, l2_budget_bytes=0)
+
+
+class Batch:
+    """A plan of many instances of one operator, run by one persistent launch
+    per phase.  results: int64 device tensor of the per-instance counts."""
+
+    def __init__(self, ctx: Context, kind: int, args: list, *, tuning: L.BatchTuning | None = None):
+        self.ctx = ctx
+        self.kind = kind
+        n = len(args)
+        self.results = torch.zeros(max(n, 1), dtype=torch.int64, device=f"cuda:{ctx.device}")
+        typ = L.AggrArguments if kind == L.BATCH_GROUP else L.HashJoinArguments
+        self._args = (typ * max(n, 1))(*args)
+        self.count = n
+        h = C.c_void_p()
+        fn = (ctx.lib.pimdal_group_batch_create if kind == L.BATCH_GROUP
+              else ctx.lib.pimdal_hash_join_batch_create)
+        L.check(fn(ctx.handle, self._args, n, C.byref(tuning) if tuning is not None else None,
+                   self.results.data_ptr(), C.byref(h)), fn.__name__)
+        self.handle = h
+
+    @staticmethod
+    def autotune(ctx: Context, kind: int, args: list, results=None, stream=None):
+        """(best tuning, came from the cache).  Runs the instances while timing."""
+        n = len(args)
+        typ = L.AggrArguments if kind == L.BATCH_GROUP else L.HashJoinArguments
+        arr = (typ * max(n, 1))(*args)
+        if results is None:
+            results = torch.zeros(max(n, 1), dtype=torch.int64, device=f"cuda:{ctx.device}")
+        best = L.BatchTuning()
+        cached = C.c_int()
+        L.check(ctx.lib.pimdal_batch_autotune(ctx.handle, kind, C.cast(arr, C.c_void_p), n,
+                                              results.data_ptr(), C.byref(best), C.byref(cached),
+                                              _stream(stream)), "pimdal_batch_autotune")
+        return best, bool(cached.value)
+
+    def run(self, stream=None) -> None:
+        L.check(self.ctx.lib.pimdal_batch_run(self.ctx.handle, self.handle, _stream(stream)),
+                "pimdal_batch_run")
+
+    @property
+    def device_bytes(self) -> int:
+        b = C.c_size_t()
+        L.check(self.ctx.lib.pimdal_batch_device_bytes(self.handle, C.byref(b)),
+                "pimdal_batch_device_bytes")
+        return int(b.value)
+
+    def close(self) -> None:
+        if self.handle:
+            self.ctx.lib.pimdal_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -46,3 +46,17 @@ def test_argument_errors_need_no_gpu():
     assert lib.pimdal_ctx_destroy(None) == 1
     sz = ctypes.c_size_t(7)
     assert lib.pimdal_sel_workspace_size(None, ctypes.byref(sz)) == 1
+
+
+def test_batch_argument_errors_need_no_gpu():
+    lib = L.lib()
+    plan = ctypes.c_void_p()
+    # null context, plan pointer or instance arrays are rejected before any CUDA call
+    assert lib.pimdal_group_batch_create(None, None, 0, None, None, ctypes.byref(plan)) == 1
+    assert lib.pimdal_hash_join_batch_create(None, None, 0, None, None, ctypes.byref(plan)) == 1
+    assert lib.pimdal_batch_run(None, None, None) == 1
+    assert lib.pimdal_batch_destroy(None) == 0
+    sz = ctypes.c_size_t(7)
+    assert lib.pimdal_batch_device_bytes(None, ctypes.byref(sz)) == 1
+    best = L.BatchTuning()
+    assert lib.pimdal_batch_autotune(None, 0, None, 0, None, ctypes.byref(best), None, None) == 1
