@@ -775,9 +775,154 @@ class BatchWorkload(Workload):
             f"(hash_join.cpp:57-157) over the batch's first 8 group-by and 8 join instances, x{reps}")
 
 
+class ServeWorkload(Workload):
+    """Served form: filter -> join -> group-by pipelines over a resident
+    lineitem-shaped fact table (about 6e7 rows: orderkey with 1-7 rows per
+    order over 1.5e7 orders, partkey U[1,2e6], suppkey U[1,1e5], quantity,
+    price cents U[90000,10500000], discount U[0,10], date over 2557 days, two
+    flags) and two dimensions (1.5e7 orders, 2e6 parts), request row ranges
+    log-uniform in [1e5, 6e7], date selectivity 1-50%, 8 concurrency slots
+    under a 150 GB HBM budget.  A step is one saturated stream of 200 requests
+    (all arrived at the start); the same stream run serially (one request at a
+    time) and a Poisson stream at 70% of the serial throughput are measured
+    beside it."""
+    name = "serve"
+    R = 200
+    SLOTS = 8
+    metric_name = "queries/s"
+    unit = "queries/s"
+
+    def __init__(self):
+        from pimdal_b200 import _lib as L
+        self.L = L
+        self.config = {"workload": "served filter->join->group-by pipelines (SUM(price*(100-discount)), "
+                                   "COUNT by 1-2 keys) over a 6e7-row fact table + 1.5e7 / 2e6-row "
+                                   "dimensions, ranges log-U[1e5,6e7], selectivity U[1%,50%]",
+                       "requests_per_step": self.R, "slots": self.SLOTS, "hbm_budget_gb": 150,
+                       "l2": "inputs (resident tables, GBs) larger than L2"}
+        self.units_per_step = self.R
+        self.dominant = L.KERNEL_SELECT
+        self.dominant_name = "k_select (date-range selection)"
+
+    def setup(self, ctx, dev):
+        import torch
+        from pimdal_b200 import serve
+        self.serve = serve
+        self.tables = serve.Tables(ctx)
+        self.server = serve.Server(self.tables, device=ctx.device, slots=self.SLOTS)
+        self.server.warm()
+        self.reqs = serve.make_requests(self.R, self.tables.n, rate=None, seed=0xB206)
+        self.rows_per_step = sum(r.n for r in self.reqs)
+        self.config["fact_rows"] = self.tables.n
+        self._runs = []
+
+    def step(self):
+        import torch
+        l0 = sum(sl.ctx.launches for sl in self.server.slots)
+        st = self.server.run(self.reqs)
+        # kernels of this step (the slots launch through their own contexts)
+        self.launches_per_step = sum(sl.ctx.launches for sl in self.server.slots) - l0
+        cur = torch.cuda.current_stream()
+        for sl in self.server.slots:
+            cur.wait_stream(sl.stream)
+        self._runs.append(st)
+
+    def dominant_timing(self):
+        """(launches, ms) of the selection kernel over one served run (profiled)."""
+        for sl in self.server.slots:
+            sl.ctx.kernel_time(self.L.KERNEL_SELECT)
+            sl.ctx.set_profiling(True)
+        st = self.server.run(self.reqs)
+        n = ms = 0
+        for sl in self.server.slots:
+            sl.ctx.sync(sl.stream)
+            sl.ctx.set_profiling(False)
+            a, b = sl.ctx.kernel_time(self.L.KERNEL_SELECT)
+            n += a
+            ms += b
+        self._sel_rows = sum(r.n for r in self.reqs)
+        return n, ms
+
+    def roofline_bytes(self, launches: int, steps: int) -> float:
+        # the date column of every request's range (4 B per row); outputs are small
+        return 4.0 * self._sel_rows * steps
+
+    def algorithmic_bytes_per_launch(self):
+        return 4.0 * self.rows_per_step / self.R
+
+    def extra(self) -> dict:
+        serve = self.serve
+        served = self._runs[-1]
+        serial = self.server.run(self.reqs, serial=True)
+        ser = serial.summary()
+        rate = 0.7 * ser["queries_per_s"]
+        pois = serve.make_requests(self.R, self.tables.n, rate=rate, seed=0xB207)
+        p_served = self.server.run(pois).summary()
+        p_serial = self.server.run(pois, serial=True).summary()
+        same = serve.same_results(served, serial)
+        return {"served_saturated": served.summary(), "serial_saturated": ser,
+                "poisson": {"rate_per_s": round(rate, 2), "served": p_served, "serial": p_serial},
+                "served_equals_serial": same,
+                "speedup_vs_serial": round(served.summary()["queries_per_s"] / ser["queries_per_s"], 3)}
+
+    def step_e2e(self, stream):
+        """A served run: request parameters in kernel arguments, each result
+        (groups) copied to pinned host memory; the tables stay resident."""
+        import torch
+        st = self.server.run(self.reqs)
+        for sl in self.server.slots:
+            stream.wait_stream(sl.stream)
+        d2h = sum(r.keys.nbytes + r.sums.nbytes + r.counts.nbytes + 24 for r in st.results.values())
+        return 0, d2h
+
+    def cpu_sample(self, ref, threads, budget_s):
+        """The reference's CPU operators composed per request: select over the
+        date range (select.cpp), hash join of the selected join keys against
+        the dimension (hash_join.cpp), hash aggregation (aggregate.cpp); the
+        gathers between them in numpy."""
+        serve = self.serve if hasattr(self, "serve") else __import__("pimdal_b200.serve").serve
+        if not hasattr(self, "_cpu"):
+            import torch
+            from pimdal_b200 import ops
+            ctx = ops.Context(0) if torch.cuda.is_available() else None
+            t = self.tables if hasattr(self, "tables") else serve.Tables(ctx)
+            c = lambda x: x.cpu().numpy()
+            self._cpu = dict(date=c(t.l_date), okey=c(t.l_orderkey), pkey=c(t.l_partkey),
+                             price=c(t.l_price), disc=c(t.l_discount), rflag=c(t.l_rflag),
+                             lstat=c(t.l_lstatus), o_key=c(t.o_key), o_prio=c(t.o_prio),
+                             p_key=c(t.p_key), p_cat=c(t.p_cat), n=t.n)
+            self._cpu_reqs = serve.make_requests(64, t.n, rate=None, seed=0xB208)
+            for lib in ("select", "hash_join", "aggregate"):
+                ref.set_threads(lib, threads)
+        d = self._cpu
+        done = rows = 0
+        t0 = time.perf_counter()
+        for r in self._cpu_reqs:
+            if done and time.perf_counter() - t0 >= budget_s:
+                break
+            dates = d["date"][r.r0:r.r0 + r.n]
+            ref.select(dates, r.d0, r.d1)  # the reference's filter (values only)
+            rows_sel = r.r0 + np.flatnonzero((dates >= r.d0) & (dates <= r.d1))
+            if r.dim == 0:
+                jk, bk, bp, flag, nf = d["okey"][rows_sel], d["o_key"], d["o_prio"], d["rflag"], 3
+            else:
+                jk, bk, bp, flag, nf = d["pkey"][rows_sel], d["p_key"], d["p_cat"], d["lstat"], 2
+            pay, prow = ref.hash_join(bk, bp, jk.astype(np.int32))
+            sel = rows_sel[prow.astype(np.int64)]
+            key = pay.astype(np.int64) * (nf if r.two_keys else 1) + (flag[sel] if r.two_keys else 0)
+            val = d["price"][sel] * (100 - d["disc"][sel].astype(np.int64))
+            ref.group_by(key.astype(np.int32), val)
+            done += 1
+            rows += r.n
+        return done, time.perf_counter() - t0, (
+            f"reference select (select.cpp:77-100), partition + join (hash_join.cpp:57-157) and "
+            f"hash_table_aggregate (aggregate.cpp:40-83) composed per request, numpy gathers "
+            f"between them, {done} requests of the served mix")
+
+
 WORKLOADS = {"select": SelectWorkload, "sort_smj": SortSmjWorkload,
              "hash_join": HashJoinWorkload, "group_by": GroupByWorkload,
-             "batch": BatchWorkload}
+             "batch": BatchWorkload, "serve": ServeWorkload}
 DEFAULT_WORKLOAD = "sort_smj"
 
 
@@ -890,7 +1035,8 @@ def run_ours(args) -> None:
     e2e_ms = reduce_max(e0.elapsed_time(e1), world)
     ctx.sync()
 
-    rows_total = reduce_sum(float(wl.rows_per_step * args.steps), world)
+    units = getattr(wl, "units_per_step", wl.rows_per_step)
+    rows_total = reduce_sum(float(units * args.steps), world)
     value = rows_total / (total_ms / 1e3)
     e2e_value = rows_total / (e2e_ms / 1e3)
 
@@ -915,13 +1061,13 @@ def run_ours(args) -> None:
 
     if rank == 0:
         line = {
-            "metric": "rows/s", "value": round(value, 1), "unit": "rows/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "metric": getattr(wl, "metric_name", "rows/s"), "value": round(value, 1),
+            "unit": getattr(wl, "unit", "rows/s"), "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(total_ms / args.steps, 5), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "int32/uint32 keys, int64 sums",
             "data": "synthetic (seeded counter-based generator)",
             "config": dict(wl.config, parallelism=f"replicas x{world}"),
-            "e2e": {"value": round(e2e_value, 1), "unit": "rows/s",
+            "e2e": {"value": round(e2e_value, 1), "unit": getattr(wl, "unit", "rows/s"),
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": round(e2e_ms / args.steps, 4)},
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
@@ -949,7 +1095,7 @@ def cpu_baseline(wl) -> dict | None:
         return {"value": None, "unavailable": "oracle/_ref not built"}
     threads = host_threads()
     rows, secs, desc = wl.cpu_sample(oracle.Ref(), threads, 15.0)
-    return {"value": round(rows / secs, 1), "unit": "rows/s", "cores": threads,
+    return {"value": round(rows / secs, 1), "unit": getattr(wl, "unit", "rows/s"), "cores": threads,
             "kind": "reference", "sample": desc}
 
 
@@ -976,16 +1122,18 @@ def run_reference(args) -> None:
         rows += r
         secs += s
     value = rows / secs
+    unit = getattr(wl, "unit", "rows/s")
+    per_step = getattr(wl, "units_per_step", wl.rows_per_step)
     print(json.dumps({
-        "metric": "rows/s", "value": round(value, 1), "unit": "rows/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": round(wl.rows_per_step / value * 1e3, 3),
+        "metric": getattr(wl, "metric_name", "rows/s"), "value": round(value, 1), "unit": unit,
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(per_step / value * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32/uint32 keys, int64 sums", "data": "synthetic (seeded counter-based generator)",
         "config": dict(wl.config, parallelism="host CPU"), "impl": "reference",
-        "cpu_baseline": {"value": round(value, 1), "unit": "rows/s", "cores": threads,
+        "cpu_baseline": {"value": round(value, 1), "unit": unit, "cores": threads,
                          "kind": "reference", "sample": desc},
-        "e2e": {"value": round(value, 1), "unit": "rows/s", "h2d_bytes_per_step": 0,
+        "e2e": {"value": round(value, 1), "unit": unit, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
 

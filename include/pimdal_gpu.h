@@ -414,6 +414,34 @@ int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_arguments_t *args,
                         pimdal_aggr_results_t *d_result, pimdal_stream_t stream);
 
 /* ------------------------------------------------------------------------- */
+/* Pipeline glue between operators.  Replaces the separate DPU passes of     */
+/* arithmetic_kernel (pimdal/general/arithmetic.c:35-67), the reduce chains  */
+/* (pimdal/general/reduce.c:42-77) and the column <-> pair conversions of    */
+/* the query pipelines (pimdal/main/tpc_h/query6/dpu/kernel_q6.c:112-156)    */
+/* with fused single-pass gathers.                                           */
+/* ------------------------------------------------------------------------- */
+/* out[i] = col[idx[i]] for i < n. */
+int pimdal_gather_u32(pimdal_ctx_t *ctx, const uint32_t *col, const uint32_t *idx, uint64_t n,
+                      uint32_t *out, pimdal_stream_t stream);
+
+typedef struct {
+  uint64_t size;               /* joined rows                                   */
+  const uint32_t *match_row;   /* per joined row: index into sel_rows           */
+  const uint32_t *match_attr;  /* per joined row: the dimension attribute       */
+  const uint32_t *sel_rows;    /* selected fact rows (NULL: match_row is the row) */
+  const int64_t *price;        /* fact columns, indexed by fact row             */
+  const int32_t *discount;     /* percent, 0..100                               */
+  const uint8_t *flag;         /* second group column (NULL: none)              */
+  uint32_t attr_mult;          /* key = attr * attr_mult + flag[row]            */
+  uint32_t pad;
+  uint32_t *out_key;           /* group key per joined row                      */
+  int64_t *out_val;            /* price * (100 - discount) per joined row       */
+} pimdal_revenue_arguments_t;
+
+int pimdal_revenue_keys(pimdal_ctx_t *ctx, const pimdal_revenue_arguments_t *args,
+                        pimdal_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
 /* Batched form: many independent group-by or hash-join instances, each phase */
 /* one persistent launch fed by a device work queue.  No reference counterpart */
 /* (the reference runs one operator instance per DPU launch, e.g. the        */

@@ -130,6 +130,15 @@ class AggrArguments(C.Structure):
     ]
 
 
+class RevenueArguments(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint64), ("match_row", C.c_void_p), ("match_attr", C.c_void_p),
+        ("sel_rows", C.c_void_p), ("price", C.c_void_p), ("discount", C.c_void_p),
+        ("flag", C.c_void_p), ("attr_mult", C.c_uint32), ("pad", C.c_uint32),
+        ("out_key", C.c_void_p), ("out_val", C.c_void_p),
+    ]
+
+
 class BatchTuning(C.Structure):
     _fields_ = [("rows_per_item", C.c_uint32), ("load_factor_pct", C.c_uint32),
                 ("reserved", C.c_uint32 * 2)]
@@ -168,6 +177,8 @@ SIGNATURES = {
     "pimdal_hash_join": (_I, [_VP, C.POINTER(HashJoinArguments), _VP, _VP]),
     "pimdal_group_workspace_size": (_I, [C.POINTER(AggrArguments), C.POINTER(_SZ)]),
     "pimdal_group_kernel": (_I, [_VP, C.POINTER(AggrArguments), _VP, _VP]),
+    "pimdal_gather_u32": (_I, [_VP, _VP, _VP, _U64, _VP, _VP]),
+    "pimdal_revenue_keys": (_I, [_VP, C.POINTER(RevenueArguments), _VP]),
     "pimdal_group_batch_create": (_I, [_VP, C.POINTER(AggrArguments), C.c_uint32,
                                        C.POINTER(BatchTuning), _VP, C.POINTER(_VP)]),
     "pimdal_hash_join_batch_create": (_I, [_VP, C.POINTER(HashJoinArguments), C.c_uint32,

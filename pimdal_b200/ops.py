@@ -326,6 +326,30 @@ def group_kernel(ctx: Context, keys, vals=None, *, method: int = L.GROUP_HASH,
 
 
 # ---------------------------------------------------------------------------
+# Pipeline glue (pimdal_gather_u32, pimdal_revenue_keys)
+# ---------------------------------------------------------------------------
+def gather_u32(ctx: Context, col, idx, n: int | None = None, out=None, stream=None):
+    """out[i] = col[idx[i]] for the first n indices."""
+    n = idx.numel() if n is None else n
+    if out is None:
+        out = torch.empty(max(n, 1), dtype=torch.int32, device=idx.device)
+    L.check(ctx.lib.pimdal_gather_u32(ctx.handle, _ptr(col), _ptr(idx), n, _ptr(out), _stream(stream)),
+            "pimdal_gather_u32")
+    return out
+
+
+def revenue_keys(ctx: Context, n: int, match_row, match_attr, sel_rows, price, discount, flag,
+                 attr_mult: int, out_key, out_val, stream=None) -> None:
+    """key = attr * attr_mult + flag[row], value = price[row] * (100 - discount[row])
+    for the first n joined rows (row = sel_rows[match_row[i]])."""
+    a = L.RevenueArguments(size=n, match_row=_ptr(match_row), match_attr=_ptr(match_attr),
+                           sel_rows=_ptr(sel_rows), price=_ptr(price), discount=_ptr(discount),
+                           flag=_ptr(flag), attr_mult=attr_mult, out_key=_ptr(out_key),
+                           out_val=_ptr(out_val))
+    L.check(ctx.lib.pimdal_revenue_keys(ctx.handle, C.byref(a), _stream(stream)), "pimdal_revenue_keys")
+
+
+# ---------------------------------------------------------------------------
 # Batched form (pimdal_group_batch_create / pimdal_hash_join_batch_create)
 # ---------------------------------------------------------------------------
 def group_args(keys, vals, outs, *, expected_groups: int = 0, capacity: int | None = None,
