@@ -243,11 +243,11 @@ __device__ __forceinline__ unsigned match_digit(uint32_t d, unsigned members) {
 template <bool HAS_VALS, int KEY_MODE>
 __global__ void __launch_bounds__(RS_THREADS, 4)
 k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
-  __shared__ uint32_t s_keys[RS_TILE];
-  __shared__ uint32_t s_vals[HAS_VALS ? RS_TILE : 1];
-  __shared__ uint32_t s_whist[RS_WARPS][RS_RADIX];  // warp digit counts -> warp offsets
+  // the tile staged in digit order: (key, value) words, or keys alone
+  __shared__ uint2 s_kv[HAS_VALS ? RS_TILE : 1];
+  __shared__ uint32_t s_k[HAS_VALS ? 1 : RS_TILE];
+  __shared__ uint32_t s_whist[RS_WARPS][RS_RADIX];  // warp digit counts -> tile offsets
   __shared__ uint16_t s_wcnt[RS_WARPS][RS_RADIX];   // running counters of the ranking (< 512)
-  __shared__ uint32_t s_dstart[RS_RADIX];
   __shared__ int32_t s_gdelta[RS_RADIX];
   __shared__ uint32_t s_warp[RS_WARPS];
   __shared__ uint32_t s_tile;
@@ -331,7 +331,9 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   if (tile == 0) pd_store_relaxed_u32(st, RS_FLAG_INC | count);
   else pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_AGG | count);
   const uint32_t dstart = block_exclusive_scan(count, s_warp, nullptr);
-  s_dstart[d] = dstart;
+  // each warp's first position of digit d in the staged tile
+#pragma unroll
+  for (int w = 0; w < RS_WARPS; ++w) s_whist[w][d] += dstart;
 
   // Warp-level stable ranking (match.any groups the lanes of one digit).
   uint32_t rank2[RS_ITEMS / 2];  // two 16-bit warp-local ranks per register (< 512)
@@ -419,9 +421,9 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   for (int k = 0; k < RS_ITEMS; ++k) {
     if (full || wl + 32u * k < tile_n) {
       const uint32_t dg = dig(key[k]);
-      const uint32_t pos = s_dstart[dg] + s_whist[warp][dg] + ((rank2[k >> 1] >> (16 * (k & 1))) & 0xFFFFu);
-      s_keys[pos] = key[k];
-      if (HAS_VALS) s_vals[pos] = val[k];
+      const uint32_t pos = s_whist[warp][dg] + ((rank2[k >> 1] >> (16 * (k & 1))) & 0xFFFFu);
+      if (HAS_VALS) s_kv[pos] = make_uint2(key[k], val[k]);
+      else s_k[pos] = key[k];
     }
   }
   __syncthreads();
@@ -431,13 +433,13 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   uint2 *dkey64 = reinterpret_cast<uint2 *>(dkey);
 #pragma unroll 4
   for (uint32_t i = tid; i < tile_n; i += RS_THREADS) {
-    const uint32_t k = s_keys[i];
-    const uint32_t g = (uint32_t)(s_gdelta[dig(k)] + (int32_t)i);
+    const uint2 e = HAS_VALS ? s_kv[i] : make_uint2(s_k[i], 0u);
+    const uint32_t g = (uint32_t)(s_gdelta[dig(e.x)] + (int32_t)i);
     if (dst_pairs) {
-      dkey64[g] = make_uint2(k, HAS_VALS ? s_vals[i] : 0u);
+      dkey64[g] = e;
     } else {
-      dkey32[g] = k;
-      if (HAS_VALS) dval[g] = s_vals[i];
+      dkey32[g] = e.x;
+      if (HAS_VALS) dval[g] = e.y;
     }
   }
 }
