@@ -216,6 +216,7 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
   __shared__ int s_state;
   __shared__ uint64_t s_prefix;
   __shared__ uint32_t s_first[HJ_ITEMS][HJ_THREADS];  // first payload of each row
+  __shared__ uint32_t s_row[HJ_ITEMS][HJ_THREADS];    // probe row id of each row (p.prow)
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint64_t mask = (1ull << p.bits) - 1;
   const uint32_t lt = (1u << lane) - 1u;
@@ -227,7 +228,7 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
   uint32_t mine = 0;
 #pragma unroll
   for (int b = 0; b < HJ_ITEMS; b += HJ_BATCH) {
-    uint32_t key[HJ_BATCH], c[HJ_BATCH], fk[HJ_BATCH];
+    uint32_t key[HJ_BATCH], c[HJ_BATCH], fk[HJ_BATCH], rowv[HJ_BATCH];
     uint64_t g[HJ_BATCH];
     bool active[HJ_BATCH];
 #pragma unroll
@@ -235,6 +236,9 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
       const uint64_t r = wbase + (uint64_t)(b + i) * 32 + lane;
       active[i] = r < hi;
       key[i] = active[i] ? __ldcs(p.pkey + r) : 0u;
+      // row ids are loaded here, with the keys, so the output phase reads them
+      // from shared memory instead of waiting on a load per row
+      rowv[i] = (p.prow && active[i]) ? __ldcs(p.prow + r) : (uint32_t)r;
       g[i] = bucket_of(key[i], p.part_bits, p.bits);
       c[i] = 0;
       fk[i] = 0;
@@ -271,6 +275,7 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
       uint32_t ci = c[i];
       if (r < hi && key[i] == 0xFFFFFFFFu) ci += side;
       s_first[k][tid] = fk[i];
+      s_row[k][tid] = rowv[i];
       mine += ci;
       cnt4 |= (uint64_t)(ci < 15 ? ci : 15u) << (4 * k);
     }
@@ -321,7 +326,7 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
       const unsigned m = __ballot_sync(0xffffffffu, c4 == 1);
       if (c4 == 1) {
         const uint64_t pos = w + __popc(m & lt);
-        const uint32_t row = p.prow ? p.prow[r] : (uint32_t)r;
+        const uint32_t row = s_row[k][tid];
         if (pos < p.cap) { p.out_pay[pos] = s_first[k][tid]; p.out_row[pos] = row; } else overflow = true;
       }
       w += __popc(m);
@@ -342,7 +347,7 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
         if (lane >= o) ci += t;
       }
       const uint64_t pos = w + ci - c;
-      const uint32_t row = c ? (p.prow ? p.prow[r] : (uint32_t)r) : 0u;
+      const uint32_t row = c ? s_row[k][tid] : 0u;
       if (c4 == 1) {
         if (pos < p.cap) { p.out_pay[pos] = s_first[k][tid]; p.out_row[pos] = row; } else overflow = true;
       } else if (c) {

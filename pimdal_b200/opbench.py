@@ -81,7 +81,8 @@ def _runner(ctx: ops.Context, a, inp):
         orow = torch.empty(n, dtype=torch.int32, device=dev)
         res = torch.empty(1, dtype=torch.int64, device=dev)
         return lambda: ops.hash_join(ctx, inp[0], inp[1], inp[2], capacity=n, out_payload=op,
-                                     out_row=orow, result=res)
+                                     out_row=orow, result=res, partition_bits=a.partition_bits,
+                                     load_factor_pct=a.load_factor)
     method = {"hash": L.GROUP_HASH, "sort": L.GROUP_SORT, "auto": L.GROUP_AUTO}[a.method]
     cap = 2 * a.card
     outs = {w: torch.empty(cap, dtype=torch.int64, device=dev) for w in ("sum", "count", "min", "max")}
@@ -101,6 +102,9 @@ def main(argv=None) -> None:
     p.add_argument("--zipf", action="store_true", help="Zipf keys (sort: s=1.0, hash_join: s=0.75)")
     p.add_argument("--card", type=int, default=4096, help="group cardinality")
     p.add_argument("--method", default="hash", choices=["hash", "sort", "auto"])
+    p.add_argument("--partition-bits", type=int, default=0,
+                   help="hash join: 0 = auto, 4294967295 = never partition, else 1..8")
+    p.add_argument("--load-factor", type=int, default=0, help="hash join table load factor, percent")
     p.add_argument("--device", type=int, default=0)
     p.add_argument("--kernels", action="store_true",
                    help="also print the mean time of each library kernel class")
