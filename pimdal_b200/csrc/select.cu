@@ -448,6 +448,242 @@ __global__ void __launch_bounds__(SL_THREADS, 1) k_select_chunked(SlParams q) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Shapes and loads of the cooperative selection kernel below.
+// ---------------------------------------------------------------------------
+constexpr int SC_THREADS = 512;
+constexpr int SC_WARPS = SC_THREADS / 32;
+constexpr int SC_TILE_BYTES = 64 * 1024;
+
+template <int LAYOUT, int SUB_ = SC_TILE_BYTES / 16 / SC_THREADS>
+struct ScShape {
+  static constexpr int EB = LAYOUT == PIMDAL_LAYOUT_PAIRS ? 8 : 4;  // bytes per element
+  static constexpr int EPV = 16 / EB;                                // elements per 16-byte load
+  static constexpr int SUB = SUB_;                                   // loads per thread
+  static constexpr int EPT = SUB * EPV;                              // elements per thread
+  static constexpr int TE = SC_THREADS * EPT;                        // elements per tile
+};
+
+// Striped (coalesced) loads: load k of thread t covers tile elements
+// (k * SC_THREADS + t) * EPV + j.  key[k * EPV + j]; *valid has a bit per
+// element inside the input.
+template <int LAYOUT, int SUB_ = SC_TILE_BYTES / 16 / SC_THREADS>
+__device__ __forceinline__ void sc_load_keys(const SelParams &p, uint64_t tile, uint32_t *key,
+                                             uint32_t *valid) {
+  using S = ScShape<LAYOUT, SUB_>;
+  const uint64_t t0 = tile * S::TE;
+  const uint4 *src = reinterpret_cast<const uint4 *>(reinterpret_cast<const char *>(p.in) + t0 * S::EB);
+  *valid = 0;
+#pragma unroll
+  for (int k = 0; k < S::SUB; ++k) {
+    const uint64_t e = t0 + ((uint64_t)k * SC_THREADS + threadIdx.x) * S::EPV;
+    if (e + S::EPV <= p.n) {
+      const uint4 v = src[k * SC_THREADS + threadIdx.x];
+      if (LAYOUT == PIMDAL_LAYOUT_PAIRS) {
+        key[2 * k] = v.x;
+        key[2 * k + 1] = v.z;
+      } else {
+        key[4 * k] = v.x; key[4 * k + 1] = v.y; key[4 * k + 2] = v.z; key[4 * k + 3] = v.w;
+      }
+      *valid |= ((1u << S::EPV) - 1u) << (k * S::EPV);
+    } else {
+#pragma unroll
+      for (int j = 0; j < S::EPV; ++j) {
+        const bool ok = e + j < p.n;
+        *valid |= (uint32_t)ok << (k * S::EPV + j);
+        key[k * S::EPV + j] = !ok ? 0u
+                              : LAYOUT == PIMDAL_LAYOUT_PAIRS
+                                  ? reinterpret_cast<const pimdal_key_ptr32_t *>(p.in)[e + j].key
+                                  : reinterpret_cast<const uint32_t *>(p.in)[e + j];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Large aligned inputs (pimdal_sel_kernel): one cooperative launch (all CTAs
+// co-resident, no look-back): each CTA counts a contiguous run of 64 KB tiles, a grid barrier (bounded wait) publishes the
+// per-CTA counts, each CTA adds up the counts before it, then re-reads its
+// tiles (L2 hits while the input fits in L2) and writes the selected
+// elements in order with a running offset.
+// ---------------------------------------------------------------------------
+constexpr int CO_SUB = 8;  // 16-byte loads per thread per tile (tile = 64 KB)
+
+// Grid-wide barrier for a cooperative launch: bar[0] arrivals (reset by the
+// last arrival), bar[1] generation.  A wait that exceeds the bounded-wait
+// limit sets PD_DEVERR_TIMEOUT; returns false (in every thread) when the
+// device error word has that bit, so the caller writes nothing.
+__device__ __forceinline__ bool co_grid_barrier(uint32_t *bar, uint32_t *d_error) {
+  __shared__ bool s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t gen = pd_load_acquire_u32(bar + 1);
+    __threadfence();
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      bar[0] = 0;
+      __threadfence();
+      pd_store_release_u32(bar + 1, gen + 1);
+    } else {
+      uint32_t spins = 0;
+      const uint64_t t0 = pd_globaltimer_ns();
+      while (pd_load_acquire_u32(bar + 1) == gen) {
+        if (pd_wait_expired(d_error, t0, ++spins)) break;
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+    s_ok = !(*(volatile uint32_t *)d_error & PD_DEVERR_TIMEOUT);
+  }
+  __syncthreads();
+  return s_ok;
+}
+
+template <int LAYOUT, bool SIGNED, bool HAS_PTR>
+__global__ void __launch_bounds__(SC_THREADS) k_select_coop(SelParams p, uint64_t *counts,
+                                                            uint32_t *bar, uint64_t tiles_per_cta) {
+  using S = ScShape<LAYOUT, CO_SUB>;
+  constexpr int E = S::SUB * SC_WARPS;  // (load, warp) entries of a tile, load major
+  __shared__ uint32_t s_off[E];
+  __shared__ uint32_t s_red[SC_WARPS];
+  __shared__ uint64_t s_base;
+  __shared__ uint32_t s_total;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t ntiles = pd_ceil_div(p.n, (uint64_t)S::TE);
+  const uint64_t t0 = min(ntiles, (uint64_t)blockIdx.x * tiles_per_cta);
+  const uint64_t t1 = min(ntiles, t0 + tiles_per_cta);
+
+  // 1. count this CTA's tiles
+  uint32_t c = 0;
+  for (uint64_t t = t0; t < t1; ++t) {
+    uint32_t key[S::EPT], valid, m = 0;
+    sc_load_keys<LAYOUT, CO_SUB>(p, t, key, &valid);
+#pragma unroll
+    for (int j = 0; j < S::EPT; ++j) m |= (uint32_t)sel_pred<SIGNED>(key[j], p) << j;
+    c += __popc(m & valid);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if (lane == 0) s_red[warp] = c;
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t t = 0;
+#pragma unroll
+    for (int w = 0; w < SC_WARPS; ++w) t += s_red[w];
+    counts[blockIdx.x] = t;
+  }
+  // 2. every CTA's count is published
+  if (!co_grid_barrier(bar, p.d_error)) return;
+  // 3. this CTA's first output row: the counts of the CTAs before it
+  {
+    uint64_t pre = 0, all = 0;
+    for (uint32_t i = tid; i < gridDim.x; i += SC_THREADS) {
+      const uint64_t v = __ldcg(counts + i);
+      all += v;
+      if (i < blockIdx.x) pre += v;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      pre += __shfl_xor_sync(0xffffffffu, pre, o);
+      all += __shfl_xor_sync(0xffffffffu, all, o);
+    }
+    __shared__ uint64_t s_pre[SC_WARPS], s_all[SC_WARPS];
+    if (lane == 0) {
+      s_pre[warp] = pre;
+      s_all[warp] = all;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      uint64_t a = 0, b = 0;
+      for (int w = 0; w < SC_WARPS; ++w) {
+        a += s_pre[w];
+        b += s_all[w];
+      }
+      s_base = a;
+      if (blockIdx.x == 0) *p.d_count = b;
+    }
+    __syncthreads();
+  }
+  // 4. re-read the tiles, rank and write
+  uint64_t base = s_base;
+  for (uint64_t t = t0; t < t1; ++t) {
+    uint32_t key[S::EPT], valid, m = 0;
+    sc_load_keys<LAYOUT, CO_SUB>(p, t, key, &valid);
+#pragma unroll
+    for (int j = 0; j < S::EPT; ++j) m |= (uint32_t)sel_pred<SIGNED>(key[j], p) << j;
+    m &= valid;
+    static_assert(S::SUB <= 8, "one byte per load in 64 bits");
+    uint64_t packed = 0;  // per load: count (<= 4) in one byte; per warp < 256
+#pragma unroll
+    for (int k = 0; k < S::SUB; ++k)
+      packed |= (uint64_t)__popc((m >> (k * S::EPV)) & ((1u << S::EPV) - 1u)) << (8 * k);
+    uint64_t inc = packed;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t x = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += x;
+    }
+    const uint64_t excl = inc - packed;
+    if (lane == 31) {
+#pragma unroll
+      for (int k = 0; k < S::SUB; ++k) s_off[k * SC_WARPS + warp] = (uint32_t)(inc >> (8 * k)) & 0xFFu;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t carry = 0;
+#pragma unroll
+      for (int i0 = 0; i0 < E; i0 += 32) {
+        const int i = i0 + lane;
+        const uint32_t v = i < E ? s_off[i] : 0u;
+        uint32_t x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+          if (lane >= o) x += y;
+        }
+        if (i < E) s_off[i] = carry + x - v;
+        carry += __shfl_sync(0xffffffffu, x, 31);
+      }
+      if (lane == 0) s_total = carry;
+    }
+    __syncthreads();
+    if (m) {
+      const uint64_t te = t * S::TE;
+#pragma unroll
+      for (int k = 0; k < S::SUB; ++k) {
+        uint64_t o = base + s_off[k * SC_WARPS + warp] + ((excl >> (8 * k)) & 0xFFu);
+        const uint64_t e = te + ((uint64_t)k * SC_THREADS + tid) * S::EPV;
+#pragma unroll
+        for (int j = 0; j < S::EPV; ++j) {
+          if ((m >> (k * S::EPV + j)) & 1u) {
+            if (LAYOUT == PIMDAL_LAYOUT_PAIRS) {
+              const uint32_t ptr = reinterpret_cast<const pimdal_key_ptr32_t *>(p.in)[e + j].ptr;
+              reinterpret_cast<uint2 *>(p.out)[o] = make_uint2(key[k * S::EPV + j], ptr);
+            } else {
+              reinterpret_cast<uint32_t *>(p.out)[o] = key[k * S::EPV + j];
+              if (p.out_ptr) p.out_ptr[o] = HAS_PTR ? p.in_ptr[e + j] : (uint32_t)(p.ptr_base + e + j);
+            }
+            ++o;
+          }
+        }
+      }
+    }
+    base += s_total;
+    __syncthreads();  // s_off / s_total are rewritten by the next tile
+  }
+}
+
+using CoKernel = void (*)(SelParams, uint64_t *, uint32_t *, uint64_t);
+CoKernel pick_coop(int layout, bool is_signed, bool has_ptr) {
+  if (layout == PIMDAL_LAYOUT_PAIRS)
+    return is_signed ? k_select_coop<PIMDAL_LAYOUT_PAIRS, true, true>
+                     : k_select_coop<PIMDAL_LAYOUT_PAIRS, false, true>;
+  if (is_signed)
+    return has_ptr ? k_select_coop<PIMDAL_LAYOUT_COLUMNS, true, true>
+                   : k_select_coop<PIMDAL_LAYOUT_COLUMNS, true, false>;
+  return has_ptr ? k_select_coop<PIMDAL_LAYOUT_COLUMNS, false, true>
+                 : k_select_coop<PIMDAL_LAYOUT_COLUMNS, false, false>;
+}
+
 using SelKernel = void (*)(SelParams);
 using SlKernel = void (*)(SlParams);
 
@@ -554,18 +790,24 @@ extern "C" int pimdal_sel_kernel(pimdal_ctx_t *ctx, const pimdal_sel_arguments_t
   p.d_count = &d_result->t_count;
   const bool is_signed = a->key_dtype == PIMDAL_I32;
   if (p.vec_ok && a->size >= (1u << 20)) {
-    SlParams q{};
-    q.s = p;
-    const uint64_t per_sm = pd_ceil_div(a->size, (uint64_t)ctx->sm_count);
-    q.chunk_elems = std::min<uint64_t>(SL_CHUNK_MAX, pd_align_up(per_sm, SL_TILE));
-    q.nchunks = pd_ceil_div(a->size, q.chunk_elems);
-    q.claim = ctx->d_counters + PD_COUNTER_SELECT;
-    const unsigned grid = (unsigned)std::min<uint64_t>(q.nchunks, (uint64_t)ctx->sm_count);
-    SlKernel k = pick_chunked(a->layout, is_signed, p.in_ptr != nullptr);
-    const int smem = SL_STAGES * SL_STAGE_BYTES;
-    PD_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    CoKernel k = pick_coop(a->layout, is_signed, p.in_ptr != nullptr);
+    static int per_sm[2] = {0, 0};
+    int &occ = per_sm[a->layout == PIMDAL_LAYOUT_PAIRS];
+    if (!occ) {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, SC_THREADS, 0);
+      if (occ <= 0) occ = 1;
+    }
+    const uint64_t te = (uint64_t)SC_THREADS * CO_SUB * (a->layout == PIMDAL_LAYOUT_PAIRS ? 2 : 4);
+    const uint64_t ntiles = pd_ceil_div(a->size, te);
+    const uint64_t want = std::min<uint64_t>(ntiles, (uint64_t)occ * ctx->sm_count);
+    uint64_t tpc = pd_ceil_div(ntiles, want);
+    unsigned grid = (unsigned)pd_ceil_div(ntiles, tpc);
+    uint64_t *counts = ctx->d_status;  // per-CTA counts (epoch 0 words: never a live status)
+    uint32_t *bar = ctx->d_counters + PD_COUNTER_SELECT;
+    SelParams pp = p;
+    void *args[] = {&pp, &counts, &bar, &tpc};
     pd_launch_scope scope(ctx, PIMDAL_KERNEL_SELECT, s);
-    k<<<grid, SL_THREADS, smem, s>>>(q);
+    PD_CHECK_CUDA(cudaLaunchCooperativeKernel((const void *)k, dim3(grid), dim3(SC_THREADS), args, 0, s));
   } else {
     SelKernel k = pick_kernel(a->layout, is_signed, p.in_ptr != nullptr);
     pd_launch_scope scope(ctx, PIMDAL_KERNEL_SELECT, s);

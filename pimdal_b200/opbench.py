@@ -10,8 +10,10 @@ The per-operator counterpart of the reference's benchmark programs
 (reference/db_operators/*.cpp main: generate, run the kernel a fixed number of
 times, print the mean).  It is also the program the committed ncu summaries
 profile: small row counts give captures that end in seconds.  Each iteration
-is timed with CUDA events on the launching stream; the inputs are generated on
-the device by the seeded generator (include/pimdal_gpu.h pimdal_gen_column).
+is timed with CUDA events on the launching stream, all of them enqueued
+behind a GPU sleep so that host-side launch overhead is not timed; the inputs
+are generated on the device by the seeded generator (include/pimdal_gpu.h
+pimdal_gen_column).
 """
 from __future__ import annotations
 
@@ -122,15 +124,17 @@ def main(argv=None) -> None:
         for k in names:
             ctx.kernel_time(k)  # reset
         ctx.set_profiling(True)
-    times = []
-    for _ in range(a.iters):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # All iterations are enqueued behind a GPU sleep, so the host's launch
+    # path (Python, ctypes) never leaves the GPU idle inside a timed region.
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(a.iters)]
+    torch.cuda._sleep(int(2e8))
+    for e0, e1 in evs:
         e0.record(stream)
         run()
         e1.record(stream)
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
     ctx.sync()
+    times = [e0.elapsed_time(e1) for e0, e1 in evs]
     kernels = None
     if a.kernels:
         ctx.set_profiling(False)
