@@ -29,9 +29,17 @@ namespace {
 
 constexpr int RS_THREADS = 256;
 constexpr int RS_WARPS = RS_THREADS / 32;
-constexpr int RS_ITEMS = 16;
-constexpr int RS_WARP_TILE = 32 * RS_ITEMS;        // 512
-constexpr int RS_TILE = RS_THREADS * RS_ITEMS;     // 4096
+#ifndef PD_RS_ITEMS
+#define PD_RS_ITEMS 20  // keys per thread of a digit-pass tile (measured best with 3 CTAs per SM)
+#endif
+#ifndef PD_RS_MIN_CTAS
+#define PD_RS_MIN_CTAS 3  // CTAs per SM the pass is compiled for (register budget)
+#endif
+constexpr int RS_ITEMS = PD_RS_ITEMS;
+constexpr int RS_WARP_TILE = 32 * RS_ITEMS;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+constexpr int RS_MIN_CTAS = PD_RS_MIN_CTAS;
+static_assert(RS_ITEMS % 2 == 0 && RS_WARP_TILE <= 65535, "16-bit packed ranks");
 constexpr int RS_RADIX_BITS = 8;
 constexpr int RS_RADIX = 1 << RS_RADIX_BITS;       // 256 (== RS_THREADS)
 constexpr int RS_MAX_PASSES = 4;
@@ -241,13 +249,14 @@ __device__ __forceinline__ unsigned match_digit(uint32_t d, unsigned members) {
 // One digit pass.  FULL tiles take a path without bounds checks; indices
 // inside a tile are 32-bit; the digit is (xform(key) >> shift) & mask.
 template <bool HAS_VALS, int KEY_MODE>
-__global__ void __launch_bounds__(RS_THREADS, 4)
+__global__ void __launch_bounds__(RS_THREADS, RS_MIN_CTAS)
 k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   // the tile staged in digit order: (key, value) words, or keys alone
-  __shared__ uint2 s_kv[HAS_VALS ? RS_TILE : 1];
-  __shared__ uint32_t s_k[HAS_VALS ? 1 : RS_TILE];
+  extern __shared__ __align__(16) uint2 rs_stage[];  // RS_TILE (key, value) words or keys
+  uint2 *s_kv = rs_stage;
+  uint32_t *s_k = reinterpret_cast<uint32_t *>(rs_stage);
   __shared__ uint32_t s_whist[RS_WARPS][RS_RADIX];  // warp digit counts -> tile offsets
-  __shared__ uint16_t s_wcnt[RS_WARPS][RS_RADIX];   // running counters of the ranking (< 512)
+  __shared__ uint16_t s_wcnt[RS_WARPS][RS_RADIX];   // running counters of the ranking (< RS_WARP_TILE)
   __shared__ int32_t s_gdelta[RS_RADIX];
   __shared__ uint32_t s_warp[RS_WARPS];
   __shared__ uint32_t s_tile;
@@ -336,7 +345,7 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   for (int w = 0; w < RS_WARPS; ++w) s_whist[w][d] += dstart;
 
   // Warp-level stable ranking (match.any groups the lanes of one digit).
-  uint32_t rank2[RS_ITEMS / 2];  // two 16-bit warp-local ranks per register (< 512)
+  uint32_t rank2[RS_ITEMS / 2];  // two 16-bit warp-local ranks per register (< RS_WARP_TILE)
 #pragma unroll
   for (int k = 0; k < RS_ITEMS / 2; ++k) rank2[k] = 0;
   const uint32_t lt = (1u << lane) - 1u;
@@ -560,7 +569,9 @@ int pd_sort_ex2(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode,
     const uint32_t bits = std::min<uint32_t>(RS_RADIX_BITS, p.end_bit - shift);
     const uint32_t mask = (1u << bits) - 1u;
     auto k = pick_pass(p.has_vals != 0, key_mode);
-    k<<<(unsigned)l.tiles, RS_THREADS, 0, s>>>(p, q, shift, mask);
+    const int smem = (p.has_vals ? 8 : 4) * RS_TILE;
+    PD_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k<<<(unsigned)l.tiles, RS_THREADS, smem, s>>>(p, q, shift, mask);
   }
   return pd_launch_status(ctx);
 }
