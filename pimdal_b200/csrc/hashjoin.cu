@@ -41,7 +41,13 @@ constexpr uint64_t HJ_EMPTY = ~0ull;
 constexpr int HJ_THREADS = 256;
 constexpr int HJ_ITEMS = 16;
 constexpr int HJ_TILE = HJ_THREADS * HJ_ITEMS;  // 4096 probe rows per tile
-constexpr int HJ_BATCH = 2;
+#ifndef PD_HJ_BATCH
+#define PD_HJ_BATCH 2  // probe rows of a thread whose bucket loads are in flight together
+#endif
+#ifndef PD_HJ_MIN_CTAS
+#define PD_HJ_MIN_CTAS 3  // probe CTAs per SM (register budget)
+#endif
+constexpr int HJ_BATCH = PD_HJ_BATCH;
 constexpr uint32_t HJ_MIN_BITS = 10;
 
 }  // namespace
@@ -366,7 +372,7 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(HJ_THREADS, 3) k_hj_probe(JoinParams p) {
+__global__ void __launch_bounds__(HJ_THREADS, PD_HJ_MIN_CTAS) k_hj_probe(JoinParams p) {
   __shared__ uint64_t s_tile;
   const int tid = threadIdx.x;
   uint64_t lo, hi;

@@ -29,10 +29,17 @@ namespace {
 
 constexpr int MJ_THREADS = 256;
 constexpr int MJ_WARPS = MJ_THREADS / 32;
-constexpr int MJ_ITEMS = 8;
-constexpr int MJ_TILE = MJ_THREADS * MJ_ITEMS;  // 2048 outer rows per tile
-constexpr int MJ_INNER_CAP = 3072;               // inner rows staged in shared memory
-constexpr int MJ_OUT_CAP = 2048;                 // output pairs staged in shared memory
+#ifndef PD_MJ_ITEMS
+#define PD_MJ_ITEMS 8  // outer rows per thread of a merge tile (a multiple of 4)
+#endif
+#ifndef PD_MJ_INNER_CAP
+#define PD_MJ_INNER_CAP 3072  // inner rows staged in shared memory
+#endif
+constexpr int MJ_ITEMS = PD_MJ_ITEMS;
+constexpr int MJ_TILE = MJ_THREADS * MJ_ITEMS;  // outer rows per tile
+constexpr int MJ_INNER_CAP = PD_MJ_INNER_CAP;
+constexpr int MJ_OUT_CAP = MJ_TILE;              // output pairs staged in shared memory
+static_assert(MJ_ITEMS % 4 == 0 && 8 * (MJ_INNER_CAP + MJ_OUT_CAP) <= 46 * 1024, "static smem");
 
 struct MergeParams {
   const uint32_t *ikey, *iptr;  // sorted inner (keys, payload / row id)
