@@ -209,6 +209,7 @@ extern "C" int pimdal_hash_join_batch_create(pimdal_ctx_t *ctx,
     h.cap = a.out_capacity;
     h.d_count = &d_results[i].t_count;
     h.bits = pd_hj_table_bits(a.size_build, lf);
+    if (h.bits > 32) return PIMDAL_ERR_ARG;  // at most 2^32 slots per table
     h.tile0 = tile0[i];
     tile0[i + 1] = tile0[i] + pd_ceil_div(h.np, T);
     words += 1ull << h.bits;

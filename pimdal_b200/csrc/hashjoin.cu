@@ -44,6 +44,9 @@ constexpr int HJ_TILE = HJ_THREADS * HJ_ITEMS;  // 4096 probe rows per tile
 #ifndef PD_HJ_BATCH
 #define PD_HJ_BATCH 2  // probe rows of a thread whose bucket loads are in flight together
 #endif
+#ifndef PD_HJ_KEYS_FIRST
+#define PD_HJ_KEYS_FIRST 1  // a thread loads all its probe keys and row ids before any bucket
+#endif
 #ifndef PD_HJ_MIN_CTAS
 #define PD_HJ_MIN_CTAS 3  // probe CTAs per SM (register budget)
 #endif
@@ -64,10 +67,14 @@ uint32_t pd_hj_table_bits(uint64_t nb, uint32_t load_pct) {
 namespace {
 
 // Home bucket of a key: buckets are aligned groups of 4 slots (one 32-byte
-// sector); a table of 2^bits slots has 2^(bits-2) buckets.
-__device__ __forceinline__ uint64_t bucket_of(uint32_t key, uint32_t part_bits, uint32_t bits) {
-  const uint64_t h = (uint64_t)key * PD_GOLDEN64;
-  return (h << part_bits) >> (64 - (bits - 2));
+// sector); a table of 2^bits slots has 2^(bits-2) buckets.  The bucket is
+// bits [64 - part_bits - (bits-2), 64 - part_bits) of key * PD_GOLDEN64,
+// just below the bits that chose the partition.  part_bits + bits - 2 <= 30
+// (the table layout caps all partitions together at 2^32 slots), so they all
+// lie in the product's high word, computed here in 32-bit arithmetic.
+__device__ __forceinline__ uint32_t bucket_of(uint32_t key, uint32_t part_bits, uint32_t bits) {
+  const uint32_t hi = __umulhi(key, (uint32_t)PD_GOLDEN64) + key * (uint32_t)(PD_GOLDEN64 >> 32);
+  return (hi << part_bits) >> (34 - bits);
 }
 
 struct JoinParams {
@@ -132,12 +139,12 @@ __device__ __forceinline__ void hj_insert(const JoinParams &p, uint32_t k, uint3
     atomicAdd(p.side_count, 1u);
     return;
   }
-  const uint64_t gmask = ((1ull << p.bits) - 1) >> 2;
-  uint64_t g = bucket_of(k, p.part_bits, p.bits);
+  const uint32_t gmask = (uint32_t)(((1ull << p.bits) - 1) >> 2);
+  uint32_t g = bucket_of(k, p.part_bits, p.bits);
   bool done = false;
   bool dup = false;
   for (uint64_t t = 0; t <= gmask && !done; ++t) {
-    unsigned long long *b = p.table + 4 * g;
+    unsigned long long *b = p.table + 4 * (uint64_t)g;
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       if (done) break;
@@ -185,20 +192,24 @@ __device__ __forceinline__ bool resolve_bucket(ulonglong2 lo, ulonglong2 hi, uin
 
 // Writes every match of key (bucket walk from its home bucket) from output
 // position w on; returns the number of matches.
-__device__ __noinline__ uint32_t emit_all(const JoinParams &p, uint32_t key, uint64_t mask,
-                                          uint64_t w, uint32_t row, bool *overflow, bool emit) {
-  const uint64_t gmask = mask >> 2;
-  uint64_t g = bucket_of(key, p.part_bits, p.bits);
+// (The table and output fields are passed by value: a reference to the
+// parameter struct would make every caller copy it to local memory.)
+__device__ __noinline__ uint32_t emit_all(const unsigned long long *table, uint32_t bits,
+                                          uint32_t part_bits, uint32_t *out_pay, uint32_t *out_row,
+                                          uint64_t cap, uint32_t key, uint64_t w, uint32_t row,
+                                          bool *overflow, bool emit) {
+  const uint32_t gmask = (uint32_t)(((1ull << bits) - 1) >> 2);
+  uint32_t g = bucket_of(key, part_bits, bits);
   uint32_t c = 0;
   for (uint64_t t = 0; t <= gmask; ++t) {
     bool has_empty = false;
     for (int j = 0; j < 4; ++j) {
-      const unsigned long long e = p.table[4 * g + j];
+      const unsigned long long e = table[4 * (uint64_t)g + j];
       if (e == HJ_EMPTY) {
         has_empty = true;
       } else if ((uint32_t)e == key) {
         if (emit) {
-          if (w < p.cap) { p.out_pay[w] = (uint32_t)(e >> 32); p.out_row[w] = row; } else *overflow = true;
+          if (w < cap) { out_pay[w] = (uint32_t)(e >> 32); out_row[w] = row; } else *overflow = true;
         }
         ++w;
         ++c;
@@ -232,33 +243,52 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
   // Phase 1: match counts (4 bits per row, 15 = "count again") and first payloads.
   uint64_t cnt4 = 0;
   uint32_t mine = 0;
+#if PD_HJ_KEYS_FIRST
+  // All keys and row ids of the thread are loaded together (one memory
+  // latency per tile); row ids go straight to shared memory, where the
+  // output phase reads them.
+  uint32_t keys[HJ_ITEMS];
+#pragma unroll
+  for (int k = 0; k < HJ_ITEMS; ++k) {
+    const uint64_t r = wbase + (uint64_t)k * 32 + lane;
+    keys[k] = r < hi ? __ldcs(p.pkey + r) : 0u;
+    s_row[k][tid] = (p.prow && r < hi) ? __ldcs(p.prow + r) : (uint32_t)r;
+  }
+#endif
 #pragma unroll
   for (int b = 0; b < HJ_ITEMS; b += HJ_BATCH) {
-    uint32_t key[HJ_BATCH], c[HJ_BATCH], fk[HJ_BATCH], rowv[HJ_BATCH];
-    uint64_t g[HJ_BATCH];
+    uint32_t key[HJ_BATCH], c[HJ_BATCH], fk[HJ_BATCH];
+#if !PD_HJ_KEYS_FIRST
+    uint32_t rowv[HJ_BATCH];
+#endif
+    uint32_t g[HJ_BATCH];
     bool active[HJ_BATCH];
 #pragma unroll
     for (int i = 0; i < HJ_BATCH; ++i) {
       const uint64_t r = wbase + (uint64_t)(b + i) * 32 + lane;
       active[i] = r < hi;
+#if PD_HJ_KEYS_FIRST
+      key[i] = keys[b + i];
+#else
       key[i] = active[i] ? __ldcs(p.pkey + r) : 0u;
       // row ids are loaded here, with the keys, so the output phase reads them
       // from shared memory instead of waiting on a load per row
       rowv[i] = (p.prow && active[i]) ? __ldcs(p.prow + r) : (uint32_t)r;
+#endif
       g[i] = bucket_of(key[i], p.part_bits, p.bits);
       c[i] = 0;
       fk[i] = 0;
     }
     // Lockstep bucket walks: all loads of a round are in flight together;
     // almost every row resolves in its home bucket.
-    const uint64_t gmask = mask >> 2;
+    const uint32_t gmask = (uint32_t)(mask >> 2);
     for (uint64_t round = 0; round <= gmask; ++round) {
       ulonglong2 glo[HJ_BATCH], ghi[HJ_BATCH];
       bool any = false;
 #pragma unroll
       for (int i = 0; i < HJ_BATCH; ++i) {
         if (active[i]) {
-          const ulonglong2 *q = reinterpret_cast<const ulonglong2 *>(p.table + 4 * g[i]);
+          const ulonglong2 *q = reinterpret_cast<const ulonglong2 *>(p.table + 4 * (uint64_t)g[i]);
           glo[i] = q[0];
           ghi[i] = q[1];
           any = true;
@@ -281,7 +311,9 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
       uint32_t ci = c[i];
       if (r < hi && key[i] == 0xFFFFFFFFu) ci += side;
       s_first[k][tid] = fk[i];
+#if !PD_HJ_KEYS_FIRST
       s_row[k][tid] = rowv[i];
+#endif
       mine += ci;
       cnt4 |= (uint64_t)(ci < 15 ? ci : 15u) << (4 * k);
     }
@@ -343,7 +375,8 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
       if (c4 == 1) c = 1;
       else if (c4 > 1) {
         bool dummy = false;
-        c = emit_all(p, key, mask, 0, 0, &dummy, false);  // count only
+        c = emit_all(p.table, p.bits, p.part_bits, p.out_pay, p.out_row, p.cap, key, 0, 0, &dummy,
+                     false);  // count only
         if (key == 0xFFFFFFFFu) c += side;
       }
       uint32_t ci = c;
@@ -357,7 +390,8 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
       if (c4 == 1) {
         if (pos < p.cap) { p.out_pay[pos] = s_first[k][tid]; p.out_row[pos] = row; } else overflow = true;
       } else if (c) {
-        uint64_t q = pos + emit_all(p, key, mask, pos, row, &overflow, true);
+        uint64_t q = pos + emit_all(p.table, p.bits, p.part_bits, p.out_pay, p.out_row, p.cap, key,
+                                    pos, row, &overflow, true);
         if (key == 0xFFFFFFFFu) {
           for (uint32_t m2 = 0; m2 < side; ++m2, ++q) {
             if (q < p.cap) { p.out_pay[q] = 0xFFFFFFFFu; p.out_row[q] = row; } else overflow = true;
@@ -534,6 +568,7 @@ bool hj_layout(const pimdal_hash_join_arguments_t *a, HjLayout *l) {
   const uint32_t load_pct = a->load_factor_pct ? a->load_factor_pct : 50;
   if (load_pct > 90) return false;
   const uint32_t bits = pd_hj_table_bits(a->size_build, load_pct);
+  if (bits > 32) return false;  // bucket_of's 32-bit arithmetic
   uint64_t budget = a->l2_budget_bytes ? a->l2_budget_bytes : (48ull << 20);
   uint32_t pb = a->partition_bits;
   if (pb == 0xFFFFFFFFu) pb = 0;  // explicit "no partitioning"

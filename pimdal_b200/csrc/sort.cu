@@ -16,11 +16,13 @@
 //     digit is the same for every key (count == n) is skipped; buffers are
 //     routed so the last active pass writes the caller's output.  Computed on
 //     the device, so the whole sort is stream-ordered and capturable.
-//  3. k_sort_pass, once per digit: a CTA takes the next 4096-key tile (atomic
-//     tile counter, so tiles are processed in input order), ranks keys per
-//     warp with match.any, publishes per-digit tile counts and resolves their
-//     global offsets with a per-digit decoupled look-back, stages the tile in
-//     shared memory in digit order and writes each digit run contiguously.
+//  3. k_sort_pass, once per digit: a CTA takes the next tile of RS_TILE keys
+//     (atomic tile counter, so tiles are processed in input order), counts
+//     its digits and publishes the counts early, ranks keys per warp
+//     (shared-memory lane masks group the lanes of one digit), resolves the
+//     digits' global offsets with a per-digit decoupled look-back, stages the
+//     tile in shared memory in digit order and writes each digit run
+//     contiguously.
 #include <algorithm>
 
 #include "common.cuh"
@@ -35,16 +37,28 @@ constexpr int RS_WARPS = RS_THREADS / 32;
 #ifndef PD_RS_MIN_CTAS
 #define PD_RS_MIN_CTAS 3  // CTAs per SM the pass is compiled for (register budget)
 #endif
+#ifndef PD_RS_MATCH
+// lanes sharing a digit in full tiles: 0 one ballot per digit bit, 1
+// shared-memory atomicOr masks
+#define PD_RS_MATCH 1
+#endif
+#ifndef PD_RS_WFULL
+#define PD_RS_WFULL 1  // 1: full tiles write their staged keys in a fully unrolled loop
+#endif
 constexpr int RS_ITEMS = PD_RS_ITEMS;
 constexpr int RS_WARP_TILE = 32 * RS_ITEMS;
 constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
 constexpr int RS_MIN_CTAS = PD_RS_MIN_CTAS;
-static_assert(RS_ITEMS % 2 == 0 && RS_WARP_TILE <= 65535, "16-bit packed ranks");
+static_assert(RS_ITEMS % 2 == 0 && RS_TILE <= 65536, "16-bit packed staged positions");
 constexpr int RS_RADIX_BITS = 8;
 constexpr int RS_RADIX = 1 << RS_RADIX_BITS;       // 256 (== RS_THREADS)
 constexpr int RS_MAX_PASSES = 4;
 constexpr uint32_t RS_FLAG_AGG = 1u << 30, RS_FLAG_INC = 2u << 30, RS_COUNT_MASK = (1u << 30) - 1;
 static_assert(RS_RADIX == RS_THREADS, "one thread per digit");
+// The atomicOr masks (two per warp and digit) borrow the staging buffer
+// during the ranking; it must hold them even for keys alone.
+constexpr int RS_MATCH_WORDS = 2 * RS_WARPS * RS_RADIX;
+static_assert(PD_RS_MATCH == 0 || RS_MATCH_WORDS <= RS_TILE, "match masks fit the key staging");
 
 enum : uint32_t { BUF_IN = 0, BUF_OUT = 1, BUF_ALT = 2 };
 
@@ -255,8 +269,8 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   extern __shared__ __align__(16) uint2 rs_stage[];  // RS_TILE (key, value) words or keys
   uint2 *s_kv = rs_stage;
   uint32_t *s_k = reinterpret_cast<uint32_t *>(rs_stage);
-  __shared__ uint32_t s_whist[RS_WARPS][RS_RADIX];  // warp digit counts -> tile offsets
-  __shared__ uint16_t s_wcnt[RS_WARPS][RS_RADIX];   // running counters of the ranking (< RS_WARP_TILE)
+  __shared__ uint32_t s_whist[RS_WARPS][RS_RADIX];  // warp digit counts -> warp offsets in the digit
+  __shared__ uint16_t s_wcnt[RS_WARPS][RS_RADIX];   // running staged positions of the ranking (< RS_TILE)
   __shared__ int32_t s_gdelta[RS_RADIX];
   __shared__ uint32_t s_warp[RS_WARPS];
   __shared__ uint32_t s_tile;
@@ -273,8 +287,12 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
 #pragma unroll
   for (int w = 0; w < RS_WARPS; ++w) {
     s_whist[w][tid] = 0;
-    s_wcnt[w][tid] = 0;
   }
+#if PD_RS_MATCH == 1
+#pragma unroll
+  for (int j = 0; j < RS_MATCH_WORDS / (4 * RS_THREADS); ++j)
+    reinterpret_cast<uint4 *>(rs_stage)[tid + j * RS_THREADS] = make_uint4(0, 0, 0, 0);
+#endif
   __syncthreads();
   const uint64_t tile = s_tile;
   const uint64_t base = tile * (uint64_t)RS_TILE;
@@ -340,17 +358,48 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   if (tile == 0) pd_store_relaxed_u32(st, RS_FLAG_INC | count);
   else pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_AGG | count);
   const uint32_t dstart = block_exclusive_scan(count, s_warp, nullptr);
-  // each warp's first position of digit d in the staged tile
+  // each warp's first position of digit d in the staged tile seeds its
+  // running counter, so the ranking below yields staged positions
 #pragma unroll
-  for (int w = 0; w < RS_WARPS; ++w) s_whist[w][d] += dstart;
+  for (int w = 0; w < RS_WARPS; ++w) s_wcnt[w][d] = (uint16_t)(s_whist[w][d] + dstart);
+  __syncthreads();
 
-  // Warp-level stable ranking (match.any groups the lanes of one digit).
-  uint32_t rank2[RS_ITEMS / 2];  // two 16-bit warp-local ranks per register (< RS_WARP_TILE)
+  // Warp-level stable ranking: the lanes of one digit are grouped, and the
+  // lowest-numbered item and lane come first.
+  uint32_t rank2[RS_ITEMS / 2];  // two 16-bit staged positions per register (< RS_TILE)
 #pragma unroll
   for (int k = 0; k < RS_ITEMS / 2; ++k) rank2[k] = 0;
   const uint32_t lt = (1u << lane) - 1u;
   uint16_t *whist = s_wcnt[warp];
   if (full) {
+#if PD_RS_MATCH == 1
+    // Each lane sets its bit in the mask of its digit; after the warp
+    // barrier the mask holds the lanes sharing the digit.  Two mask sets
+    // alternate by item: the leader clears item k's mask after the shuffle
+    // (every lane has read it by then), and item k+2 reuses that set only
+    // after item k+1's barrier.  The barrier also orders the leaders'
+    // counter updates from one item to the next.
+    uint32_t *mbase = reinterpret_cast<uint32_t *>(rs_stage) + warp * 2 * RS_RADIX;
+    const uint32_t lanebit = 1u << lane;
+#pragma unroll
+    for (int k = 0; k < RS_ITEMS; ++k) {
+      const uint32_t d = dig(key[k]);
+      uint32_t *mb = mbase + (k & 1) * RS_RADIX;
+      atomicOr(&mb[d], lanebit);
+      __syncwarp();
+      const unsigned peers = mb[d];
+      const int leader = 31 - __clz(peers);
+      uint32_t old = 0;
+      if (lane == leader) old = whist[d];
+      old = __shfl_sync(0xffffffffu, old, leader);
+      if (lane == leader) {
+        whist[d] = (uint16_t)(old + __popc(peers));
+        mb[d] = 0;
+      }
+      rank2[k >> 1] |= (old + __popc(peers & lt)) << (16 * (k & 1));
+    }
+    __syncwarp();
+#else
 #pragma unroll
     for (int k = 0; k < RS_ITEMS; ++k) {
       const uint32_t d = dig(key[k]);
@@ -365,6 +414,7 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
       rank2[k >> 1] |= (old + __popc(peers & lt)) << (16 * (k & 1));
       __syncwarp();
     }
+#endif
   } else {
 #pragma unroll
     for (int k = 0; k < RS_ITEMS; ++k) {
@@ -429,8 +479,7 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
 #pragma unroll
   for (int k = 0; k < RS_ITEMS; ++k) {
     if (full || wl + 32u * k < tile_n) {
-      const uint32_t dg = dig(key[k]);
-      const uint32_t pos = s_whist[warp][dg] + ((rank2[k >> 1] >> (16 * (k & 1))) & 0xFFFFu);
+      const uint32_t pos = (rank2[k >> 1] >> (16 * (k & 1))) & 0xFFFFu;
       if (HAS_VALS) s_kv[pos] = make_uint2(key[k], val[k]);
       else s_k[pos] = key[k];
     }
@@ -440,8 +489,7 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   // Write each digit run contiguously (global index < 2^30).
   uint32_t *dkey32 = reinterpret_cast<uint32_t *>(dkey);
   uint2 *dkey64 = reinterpret_cast<uint2 *>(dkey);
-#pragma unroll 4
-  for (uint32_t i = tid; i < tile_n; i += RS_THREADS) {
+  auto put = [&](uint32_t i) {
     const uint2 e = HAS_VALS ? s_kv[i] : make_uint2(s_k[i], 0u);
     const uint32_t g = (uint32_t)(s_gdelta[dig(e.x)] + (int32_t)i);
     if (dst_pairs) {
@@ -450,7 +498,16 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
       dkey32[g] = e.x;
       if (HAS_VALS) dval[g] = e.y;
     }
+  };
+#if PD_RS_WFULL
+  if (full) {
+#pragma unroll
+    for (int j = 0; j < RS_ITEMS; ++j) put(tid + j * RS_THREADS);
+    return;
   }
+#endif
+#pragma unroll 4
+  for (uint32_t i = tid; i < tile_n; i += RS_THREADS) put(i);
 }
 
 using PassKernel = void (*)(SortParams, uint32_t, uint32_t, uint32_t);
