@@ -57,6 +57,12 @@ def lib() -> C.CDLL:
         l.oracle_hash_join.argtypes = [_P, _P, _U64, _P, _P, _U64, C.c_uint32, _P, _P, _U64]
         l.oracle_part_hash0.restype = None
         l.oracle_part_hash0.argtypes = [_P, _P, _U64, C.c_uint32, C.c_uint32, _P, _P, _P]
+        l.oracle_hash.restype = C.c_uint32
+        l.oracle_hash.argtypes = [C.c_int, C.c_uint32]
+        l.oracle_bloom_build.restype = None
+        l.oracle_bloom_build.argtypes = [_P, _P, C.c_uint32, _P]
+        l.oracle_bloom_match.restype = _U64
+        l.oracle_bloom_match.argtypes = [_P, _P, _P, _U64, _P, C.c_uint32, _P, _P, _U64, _P]
         for f in (l.oracle_group_by, l.oracle_sort_group_by):
             f.restype = _U64
             f.argtypes = [_P, _P, _U64, _P, _P, _P, _P, _P]
@@ -135,6 +141,42 @@ def part_hash0(keys, ptr=None, shift: int = 32, part_n: int = 32):
     pp = None if ptr is None else _u32(ptr)
     lib().oracle_part_hash0(_p(k), _p(pp), n, shift, part_n, _p(ok), _p(op), _p(sizes))
     return ok[:n], op[:n], sizes
+
+
+FILTER_BITS = 16384
+FILTER_BYTES = FILTER_BITS // 8
+
+
+def hash_fn(which: int, keys) -> np.ndarray:
+    """hash0 (which = 0) or the filter hash hashK (which = K = 1..4)."""
+    f = lib().oracle_hash
+    return np.fromiter((f(which, int(x)) for x in _u32(keys)), np.uint32, count=np.size(keys))
+
+
+def bloom_build(keys, part_sizes) -> np.ndarray:
+    """One FILTER_BYTES filter per partition of the partitioned keys
+    (part_sizes: part_n + 1 offsets), as a uint8 array."""
+    k = _u32(keys)
+    ps = np.ascontiguousarray(part_sizes, dtype=np.uint64)
+    part_n = ps.size - 1
+    out = np.zeros(max(part_n, 1) * FILTER_BYTES, np.uint8)
+    lib().oracle_bloom_build(_p(k), _p(ps), part_n, _p(out))
+    return out[:part_n * FILTER_BYTES]
+
+
+def bloom_match(filters, keys, part_sizes, ptr=None):
+    """Kept (keys, row ids) in input order and match_sizes (part_n + 1)."""
+    f = np.ascontiguousarray(filters, dtype=np.uint8)
+    k = _u32(keys)
+    ps = np.ascontiguousarray(part_sizes, dtype=np.uint64)
+    part_n = ps.size - 1
+    pp = None if ptr is None else _u32(ptr)
+    ok = np.empty(max(k.size, 1), np.uint32)
+    op = np.empty(max(k.size, 1), np.uint32)
+    ms = np.empty(part_n + 1, np.uint64)
+    c = lib().oracle_bloom_match(_p(f), _p(k), _p(pp), k.size, _p(ps), part_n, _p(ok), _p(op),
+                                 k.size, _p(ms))
+    return ok[:c], op[:c], ms
 
 
 def _group(fn, keys, vals):
@@ -235,6 +277,39 @@ class Ref:
         outs = [np.empty(max(n, 1), np.int32)] + [np.empty(max(n, 1), np.int64) for _ in range(4)]
         g = int(f(_p(k), _p(v), n, *map(_p, outs)))
         return tuple(o[:g] for o in outs)
+
+    def hash_fn(self, which: int, keys) -> np.ndarray:
+        f = self._get("bloom").pimdal_ref_hash
+        f.restype = None
+        f.argtypes = [C.c_int, _P, _U64, _P]
+        k = _u32(keys)
+        out = np.empty(max(k.size, 1), np.uint32)
+        f(which, _p(k), k.size, _p(out))
+        return out[:k.size]
+
+    def bloom_build(self, keys, part_sizes) -> np.ndarray:
+        f = self._get("bloom").pimdal_ref_bloom_build
+        f.restype = None
+        f.argtypes = [_P, _P, C.c_uint32, _P]
+        k = _u32(keys)
+        ps = np.ascontiguousarray(part_sizes, dtype=np.uint64)
+        out = np.zeros(max(ps.size - 1, 1) * FILTER_BYTES, np.uint8)
+        f(_p(k), _p(ps), ps.size - 1, _p(out))
+        return out[:(ps.size - 1) * FILTER_BYTES]
+
+    def bloom_match(self, filters, keys, part_sizes, ptr=None):
+        f = self._get("bloom").pimdal_ref_bloom_match
+        f.restype = _U64
+        f.argtypes = [_P, _P, _P, _P, C.c_uint32, _P, _P, _P]
+        fl = np.ascontiguousarray(filters, dtype=np.uint8)
+        k = _u32(keys)
+        ps = np.ascontiguousarray(part_sizes, dtype=np.uint64)
+        pp = None if ptr is None else _u32(ptr)
+        ok = np.empty(max(k.size, 1), np.uint32)
+        op = np.empty(max(k.size, 1), np.uint32)
+        ms = np.empty(ps.size, np.uint64)
+        c = int(f(_p(fl), _p(k), _p(pp), _p(ps), ps.size - 1, _p(ok), _p(op), _p(ms)))
+        return ok[:c], op[:c], ms
 
     def smj(self, inner_keys, outer_keys, buffer_size: int, threads: int = 1):
         """Reference sort-merge join on key columns (the outer size must equal

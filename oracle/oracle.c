@@ -230,6 +230,75 @@ void oracle_part_hash0(const uint32_t *key, const uint32_t *ptr, uint64_t n, uin
   free(cur);
 }
 
+/* ---------------------------------------------------------- bloom filter */
+/* The four filter hashes, hash1..hash4 of pimdal/hash/hash_func.h:16-58
+ * (hash_func[] at :60), restated: an add of a constant, then shift-add /
+ * shift-xor mixing steps with the constants and shifts of each function. */
+static uint32_t bloom_hash(int f, uint32_t k) {
+  static const uint32_t add[4] = {593627u, 274277u, 855467u, 176521u};
+  static const uint8_t sh[4][4] = {{22, 26, 10, 28}, {13, 20, 3, 9}, {4, 21, 5, 16}, {10, 25, 5, 24}};
+  k += add[f];
+  k += ~(k << sh[f][0]);
+  k ^= (k >> sh[f][1]);
+  k += (k << sh[f][2]);
+  k ^= (k >> sh[f][3]);
+  return k;
+}
+
+uint32_t oracle_hash(int which, uint32_t key) { return which == 0 ? hash0(key) : bloom_hash(which - 1, key); }
+
+/* filter_kernel (pimdal/join/hash_join.c:116-149) with insert_bloom_filter
+ * (pimdal/hash/hash_steps.c:143-152): per partition, a zeroed filter of
+ * ORACLE_FILTER_BITS bits with bit hashK(key) % ORACLE_FILTER_BITS set for
+ * K = 1..4.  Bit b lives in byte b / 8 at bit b % 8. */
+void oracle_bloom_build(const uint32_t *key, const uint64_t *part_sizes, uint32_t part_n,
+                        uint8_t *filters) {
+  for (uint32_t p = 0; p < part_n; p++) {
+    uint8_t *f = filters + (uint64_t)p * ORACLE_FILTER_BYTES;
+    memset(f, 0, ORACLE_FILTER_BYTES);
+    for (uint64_t i = part_sizes[p]; i < part_sizes[p + 1]; i++)
+      for (int h = 0; h < 4; h++) {
+        uint32_t bit = bloom_hash(h, key[i]) % ORACLE_FILTER_BITS;
+        f[bit / 8] |= (uint8_t)(1u << (bit % 8));
+      }
+  }
+}
+
+/* match_kernel (pimdal/join/hash_join.c:236-341) with probe_bloom_filter
+ * (hash_steps.c:163-185): the rows of each partition whose key has all four
+ * bits set in the partition's filter, in input order; match_sizes[0] = 0 and
+ * match_sizes[p + 1] = kept rows of partition p.  Rows of [0, n) outside
+ * every partition are not kept (the reference reads past part_sizes there,
+ * hash_join.c:268-273).  Writes at most cap rows; returns the total. */
+uint64_t oracle_bloom_match(const uint8_t *filters, const uint32_t *key, const uint32_t *ptr,
+                            uint64_t n, const uint64_t *part_sizes, uint32_t part_n,
+                            uint32_t *out_key, uint32_t *out_ptr, uint64_t cap,
+                            uint64_t *match_sizes) {
+  uint64_t c = 0;
+  match_sizes[0] = 0;
+  for (uint32_t p = 0; p < part_n; p++) {
+    const uint8_t *f = filters + (uint64_t)p * ORACLE_FILTER_BYTES;
+    uint64_t hits = 0;
+    uint64_t end = part_sizes[p + 1] < n ? part_sizes[p + 1] : n;
+    for (uint64_t i = part_sizes[p]; i < end; i++) {
+      int hit = 1;
+      for (int h = 0; h < 4 && hit; h++) {
+        uint32_t bit = bloom_hash(h, key[i]) % ORACLE_FILTER_BITS;
+        hit = (f[bit / 8] >> (bit % 8)) & 1;
+      }
+      if (!hit) continue;
+      if (c < cap) {
+        out_key[c] = key[i];
+        if (out_ptr) out_ptr[c] = ptr ? ptr[i] : (uint32_t)i;
+      }
+      c++;
+      hits++;
+    }
+    match_sizes[p + 1] = hits;
+  }
+  return c;
+}
+
 /* -------------------------------------------------------------- group by */
 typedef struct {
   int32_t key;

@@ -63,4 +63,19 @@ uint64_t oracle_sort_group_by(const int32_t *key, const int64_t *val, uint64_t n
                               int64_t *out_sum, int64_t *out_count, int64_t *out_min,
                               int64_t *out_max);
 
+/* Bloom-filter semi-join prefilter (pimdal/join/hash_join.c:116-149 and
+ * :236-341, pimdal/hash/hash_steps.c:143-185): filters of ORACLE_FILTER_BITS
+ * bits (hash_steps.c:15-16), one per partition of partitioned keys, and the
+ * ordered compaction of the rows that hit their partition's filter.
+ * oracle_hash(0, k) is hash0, oracle_hash(K, k) is hashK (K = 1..4). */
+#define ORACLE_FILTER_BITS 16384u
+#define ORACLE_FILTER_BYTES (ORACLE_FILTER_BITS / 8u)
+uint32_t oracle_hash(int which, uint32_t key);
+void oracle_bloom_build(const uint32_t *key, const uint64_t *part_sizes, uint32_t part_n,
+                        uint8_t *filters);
+uint64_t oracle_bloom_match(const uint8_t *filters, const uint32_t *key, const uint32_t *ptr,
+                            uint64_t n, const uint64_t *part_sizes, uint32_t part_n,
+                            uint32_t *out_key, uint32_t *out_ptr, uint64_t cap,
+                            uint64_t *match_sizes);
+
 #endif

@@ -5,7 +5,10 @@ come from the reference's own CPU operators (reference/db_operators, compiled
 where they lie into oracle/_ref/ by `make -C oracle ref`).  The fixtures pin
 the oracle (tests/test_oracle.py) on machines without the reference checkout.
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [fixture ...]
+
+With names (select sort hash_join group_by smj bloom), only those fixtures
+are rewritten.
 """
 from __future__ import annotations
 
@@ -29,8 +32,42 @@ def uni(n, lo, hi, stream, dt=L.I32, seed=SEED):
     return gen.generate_cpu(gen.Spec(L.GEN_UNIFORM, dt, seed=seed, stream_id=stream, lo=lo, hi=hi), n)
 
 
-def main() -> None:
+def bloom(ref) -> None:
+    """Hash values of hash0..hash4 and per-partition Bloom filters / matches
+    from the reference's hash functions (pimdal/hash/hash_func.h)."""
+    b = {}
+    hk = uni(4096, 0, 2**32 - 1, 100, L.U32)
+    hk[:4] = [0, 1, 0xFFFFFFFF, 272333]
+    b["h_keys"] = hk
+    for w in range(5):
+        b[f"h{w}"] = ref.hash_fn(w, hk)
+    # build side: 8 partitions, two of them empty; probe side: half of each
+    # partition's rows drawn from that partition's build keys
+    bps = np.array([0, 0, 700, 700, 3000, 3001, 6000, 9000, 9000], np.uint64)
+    pps = np.array([0, 10, 2000, 2000, 7000, 7001, 12000, 20000, 20000], np.uint64)
+    bk = uni(int(bps[-1]), 0, 2**32 - 1, 101, L.U32)
+    pk = uni(int(pps[-1]), 0, 2**32 - 1, 102, L.U32)
+    pick = uni(int(pps[-1]), 0, 2**31 - 1, 103, L.U32)
+    for p in range(8):
+        lo, hi, blo, bhi = int(pps[p]), int(pps[p + 1]), int(bps[p]), int(bps[p + 1])
+        if bhi > blo:
+            rows = np.arange(lo, hi)[::2]
+            pk[rows] = bk[blo + pick[rows] % (bhi - blo)]
+    filt = ref.bloom_build(bk, bps)
+    mk, mp, ms = ref.bloom_match(filt, pk, pps)
+    b.update(bk=bk, bps=bps, pk=pk, pps=pps, filters=filt, match_key=mk, match_ptr=mp,
+             match_sizes=ms)
+    np.savez_compressed(OUT / "bloom.npz", **b)
+
+
+def main(only: list[str]) -> None:
+    want = lambda name: not only or name in only
     ref = oracle.Ref()
+    if want("bloom"):
+        bloom(ref)
+    if only and only == ["bloom"]:
+        print("golden fixtures written to", OUT)
+        return
     for name in ("select", "sort", "hash_join", "aggregate", "smj_64000"):
         ref.set_threads(name, 1)
 
@@ -101,4 +138,4 @@ def main() -> None:
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

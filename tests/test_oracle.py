@@ -101,3 +101,46 @@ def test_oracle_vs_reference_fresh_inputs():
                                    hi=10**7), n)
     for a, b in zip(oracle.group_by(ck, cv), ref.group_by(ck, cv)):
         assert np.array_equal(a, b)
+
+
+def test_bloom_matches_golden():
+    g = _load("bloom")
+    for w in range(5):
+        assert np.array_equal(oracle.hash_fn(w, g["h_keys"]), g[f"h{w}"]), w
+    filt = oracle.bloom_build(g["bk"], g["bps"])
+    assert np.array_equal(filt, g["filters"])
+    mk, mp, ms = oracle.bloom_match(filt, g["pk"], g["pps"])
+    assert np.array_equal(mk, g["match_key"]) and np.array_equal(mp, g["match_ptr"])
+    assert np.array_equal(ms, g["match_sizes"])
+    # every probe row whose key is in its partition's build keys is kept
+    bps, pps = g["bps"].astype(int), g["pps"].astype(int)
+    kept = set(mp.tolist())
+    for p in range(bps.size - 1):
+        bset = set(g["bk"][bps[p]:bps[p + 1]].tolist())
+        for r in range(pps[p], pps[p + 1]):
+            if int(g["pk"][r]) in bset:
+                assert r in kept
+
+
+def test_bloom_match_drops_rows_outside_every_partition():
+    k = np.arange(100, dtype=np.uint32)
+    ps = np.array([10, 40, 60], np.uint64)
+    filt = oracle.bloom_build(k, ps)
+    mk, mp, ms = oracle.bloom_match(filt, k, ps)
+    assert np.array_equal(mp, np.arange(10, 60, dtype=np.uint32))
+    assert ms.tolist() == [0, 30, 20]
+
+
+@pytest.mark.skipif(not oracle.Ref.available("bloom"), reason="oracle/_ref not built")
+def test_bloom_oracle_vs_reference_fresh_inputs():
+    ref = oracle.Ref()
+    k = gen.generate_cpu(gen.Spec(L.GEN_UNIFORM, L.U32, seed=21, lo=0, hi=2**32 - 1), 50000)
+    for w in range(5):
+        assert np.array_equal(oracle.hash_fn(w, k[:3000]), ref.hash_fn(w, k[:3000]))
+    ps = np.array([0, 1, 1, 2500, 20000, 50000], np.uint64)
+    filt = oracle.bloom_build(k, ps)
+    assert np.array_equal(filt, ref.bloom_build(k, ps))
+    q = gen.generate_cpu(gen.Spec(L.GEN_UNIFORM, L.U32, seed=22, lo=0, hi=2**32 - 1), 50000)
+    q[::4] = k[::4]
+    for a, b in zip(oracle.bloom_match(filt, q, ps), ref.bloom_match(filt, q, ps)):
+        assert np.array_equal(a, b)
