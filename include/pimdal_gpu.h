@@ -106,7 +106,9 @@ typedef enum {
   PIMDAL_KERNEL_GROUP = 8,       /* hash group-by                          */
   PIMDAL_KERNEL_SEGREDUCE = 9,   /* sort group-by segmented reduction      */
   PIMDAL_KERNEL_OTHER = 10,
-  PIMDAL_KERNEL_COUNT = 11
+  PIMDAL_KERNEL_FILTER = 11,     /* Bloom filter build                     */
+  PIMDAL_KERNEL_MATCH = 12,      /* Bloom filter probe + ordered compaction*/
+  PIMDAL_KERNEL_COUNT = 13
 } pimdal_kernel_id_t;
 int pimdal_ctx_set_profiling(pimdal_ctx_t *ctx, int enable);
 int pimdal_ctx_kernel_time(pimdal_ctx_t *ctx, int kernel_id, uint64_t *launches,
@@ -372,6 +374,56 @@ typedef struct {
 int pimdal_hash_join_workspace_size(const pimdal_hash_join_arguments_t *args, size_t *bytes);
 int pimdal_hash_join(pimdal_ctx_t *ctx, const pimdal_hash_join_arguments_t *args,
                      pimdal_merge_results_t *d_result, pimdal_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
+/* Bloom-filter semi-join prefilter.  pimdal_filter_kernel replaces           */
+/* filter_kernel (pimdal/join/hash_join.h:15-21,64-66; hash_join.c:116-149;   */
+/* insert_bloom_filter, pimdal/hash/hash_steps.c:143-152): for every          */
+/* partition p of already-partitioned keys (rows [part_sizes[p],              */
+/* part_sizes[p+1])), a filter of PIMDAL_FILTER_BITS bits is zeroed and bit   */
+/* hashK(key) % PIMDAL_FILTER_BITS is set for K = 1..4, hashK being the       */
+/* reference's hash1..hash4 (pimdal/hash/hash_func.h:16-60).  Filter p is     */
+/* bytes [p, p+1) * PIMDAL_FILTER_BYTES of filter_ptr; bit b is bit b % 8 of  */
+/* byte b / 8, as in the reference, so filters are interchangeable with it.   */
+/* pimdal_match_kernel replaces match_kernel (hash_join.h:33-42,74-76;        */
+/* hash_join.c:236-341; probe_bloom_filter, hash_steps.c:163-185): keeps the  */
+/* rows r < size whose key finds all four bits set in the filter of r's       */
+/* partition, in input order.  match_sizes[0] = 0 and match_sizes[p+1] = kept */
+/* rows of partition p (uint64, device); t_count = all kept rows.  Rows that  */
+/* lie in no partition are not kept.  part_sizes must be non-decreasing.      */
+/* ------------------------------------------------------------------------- */
+#define PIMDAL_FILTER_BITS 16384
+#define PIMDAL_FILTER_BYTES (PIMDAL_FILTER_BITS / 8)
+
+typedef struct {
+  const void *in;              /* filter_arguments_t.in_ptr: partitioned keys    */
+  void *filter_ptr;            /* filter_arguments_t.filter_ptr: part_n filters, */
+                               /* 16-byte aligned                                */
+  const uint64_t *part_sizes;  /* filter_arguments_t.part_sizes: part_n + 1      */
+                               /* row offsets (device)                           */
+  uint32_t part_n;             /* filter_arguments_t.part_n (>= 1)               */
+  int32_t layout;              /* PIMDAL_LAYOUT_COLUMNS (uint32 keys) or         */
+                               /* PIMDAL_LAYOUT_PAIRS (key_ptr32 pairs)          */
+} pimdal_filter_arguments_t;
+
+typedef struct {
+  const void *filter_ptr;      /* match_arguments_t.filter_ptr                   */
+  uint64_t size;               /* match_arguments_t.size: input rows (< 2^31)    */
+  const void *part_ptr;        /* match_arguments_t.part_ptr: partitioned keys   */
+  const uint32_t *part_row;    /* row ids (columns layout); NULL = row index     */
+  void *out_ptr;               /* match_arguments_t.out_ptr: kept keys (pairs)   */
+  uint32_t *out_row;           /* kept row ids (columns layout; may be NULL)     */
+  uint64_t out_capacity;       /* rows of room in the outputs                    */
+  uint64_t *match_sizes;       /* match_arguments_t.match_sizes: part_n + 1      */
+  const uint64_t *part_sizes;  /* match_arguments_t.part_sizes: part_n + 1       */
+  uint32_t part_n;             /* match_arguments_t.part_n (>= 1)                */
+  int32_t layout;              /* PIMDAL_LAYOUT_COLUMNS or PIMDAL_LAYOUT_PAIRS   */
+} pimdal_match_arguments_t;
+
+int pimdal_filter_kernel(pimdal_ctx_t *ctx, const pimdal_filter_arguments_t *args,
+                         pimdal_stream_t stream);
+int pimdal_match_kernel(pimdal_ctx_t *ctx, const pimdal_match_arguments_t *args,
+                        pimdal_merge_results_t *d_result, pimdal_stream_t stream);
 
 /* ------------------------------------------------------------------------- */
 /* Group-by.  Replaces group_kernel (pimdal/aggregate/aggregate.h:7-25):      */

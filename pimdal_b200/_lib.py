@@ -24,7 +24,10 @@ LAYOUT_COLUMNS, LAYOUT_PAIRS = 0, 1
 PRED_LT, PRED_LE, PRED_GT, PRED_GE, PRED_EQ, PRED_NE, PRED_BETWEEN, PRED_RANGE = range(8)
 GEN_UNIFORM, GEN_PERM, GEN_PERM_UNIFORM, GEN_PERM_ZIPF, GEN_PROBE = range(5)
 (KERNEL_SELECT, KERNEL_GEN, KERNEL_SORT_HIST, KERNEL_SORT_PASS, KERNEL_SMJ_MERGE, KERNEL_PARTITION,
- KERNEL_HJ_BUILD, KERNEL_HJ_PROBE, KERNEL_GROUP, KERNEL_SEGREDUCE, KERNEL_OTHER) = range(11)
+ KERNEL_HJ_BUILD, KERNEL_HJ_PROBE, KERNEL_GROUP, KERNEL_SEGREDUCE, KERNEL_OTHER, KERNEL_FILTER,
+ KERNEL_MATCH) = range(13)
+FILTER_BITS = 16384
+FILTER_BYTES = FILTER_BITS // 8
 
 
 class PimdalError(RuntimeError):
@@ -118,6 +121,22 @@ class HashJoinArguments(C.Structure):
     ]
 
 
+class FilterArguments(C.Structure):
+    _fields_ = [
+        ("in_", C.c_void_p), ("filter_ptr", C.c_void_p), ("part_sizes", C.c_void_p),
+        ("part_n", C.c_uint32), ("layout", C.c_int32),
+    ]
+
+
+class MatchArguments(C.Structure):
+    _fields_ = [
+        ("filter_ptr", C.c_void_p), ("size", C.c_uint64), ("part_ptr", C.c_void_p),
+        ("part_row", C.c_void_p), ("out_ptr", C.c_void_p), ("out_row", C.c_void_p),
+        ("out_capacity", C.c_uint64), ("match_sizes", C.c_void_p), ("part_sizes", C.c_void_p),
+        ("part_n", C.c_uint32), ("layout", C.c_int32),
+    ]
+
+
 GROUP_AUTO, GROUP_HASH, GROUP_SORT = 0, 1, 2
 
 
@@ -173,6 +192,8 @@ SIGNATURES = {
     "pimdal_hash_table_bytes": (_SZ, [_U64]),
     "pimdal_hash_kernel": (_I, [_VP, C.POINTER(HashArguments), _VP]),
     "pimdal_hj_probe": (_I, [_VP, C.POINTER(ProbeArguments), _VP, _VP]),
+    "pimdal_filter_kernel": (_I, [_VP, C.POINTER(FilterArguments), _VP]),
+    "pimdal_match_kernel": (_I, [_VP, C.POINTER(MatchArguments), _VP, _VP]),
     "pimdal_hash_join_workspace_size": (_I, [C.POINTER(HashJoinArguments), C.POINTER(_SZ)]),
     "pimdal_hash_join": (_I, [_VP, C.POINTER(HashJoinArguments), _VP, _VP]),
     "pimdal_group_workspace_size": (_I, [C.POINTER(AggrArguments), C.POINTER(_SZ)]),

@@ -31,7 +31,7 @@ enum : uint32_t {
 
 // Slots of pimdal_ctx::d_counters (two words each: claim counter, CTAs done).
 enum : uint32_t { PD_COUNTER_SELECT = 0, PD_COUNTER_PARTITION = 2, PD_COUNTER_GROUP = 4,
-                  PD_COUNTER_PROBE = 6, PD_COUNTER_MERGE = 8 };
+                  PD_COUNTER_PROBE = 6, PD_COUNTER_MERGE = 8, PD_COUNTER_MATCH = 10 };
 
 // Lookback status word: [epoch:16][flag:2][value:46].
 enum : uint32_t { PD_FLAG_INVALID = 0, PD_FLAG_AGGREGATE = 1, PD_FLAG_INCLUSIVE = 2 };
@@ -403,6 +403,26 @@ PD_HD uint32_t pd_hash0(uint32_t key) {
   key ^= (key >> 17);
   return key;
 }
+// The four Bloom-filter hashes of the reference's filter_kernel /
+// match_kernel (hash1..hash4, pimdal/hash/hash_func.h:16-60): a constant is
+// added, then four shift-add / shift-xor mixing steps.  The filter bits are
+// visible to callers (filters are caller memory), so the constants and shifts
+// are kept identical.  F is 0..3 for hash1..hash4.
+template <int F>
+PD_HD uint32_t pd_bloom_hash(uint32_t k) {
+  constexpr uint32_t add = F == 0 ? 593627u : F == 1 ? 274277u : F == 2 ? 855467u : 176521u;
+  constexpr int s0 = F == 0 ? 22 : F == 1 ? 13 : F == 2 ? 4 : 10;
+  constexpr int s1 = F == 0 ? 26 : F == 1 ? 20 : F == 2 ? 21 : 25;
+  constexpr int s2 = F == 0 ? 10 : F == 1 ? 3 : F == 2 ? 5 : 5;
+  constexpr int s3 = F == 0 ? 28 : F == 1 ? 9 : F == 2 ? 16 : 24;
+  k += add;
+  k += ~(k << s0);
+  k ^= (k >> s1);
+  k += (k << s2);
+  k ^= (k >> s3);
+  return k;
+}
+
 // Table-slot hash of this library (multiplicative / Fibonacci hashing):
 // the top `bits` bits of key * 2^64/phi.
 PD_HD uint64_t pd_hash_slot(uint32_t key, uint32_t bits) {

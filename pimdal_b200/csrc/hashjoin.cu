@@ -28,8 +28,9 @@
 //  * Probing: persistent CTAs claim 4096-row tiles of warp-striped rows; a
 //    thread walks 2 rows at a time in lockstep (their bucket loads in flight
 //    together); match counts are scanned and the tile's output
-//    offset resolved by a block-wide decoupled look-back that chains across
-//    the per-partition launches, so the output is in probe order within each
+//    offset resolved by a decoupled look-back (one warp polls while the rest
+//    of the CTA waits at a barrier) that chains across the per-partition
+//    launches, so the output is in probe order within each
 //    partition, partitions in order.
 #include <algorithm>
 
@@ -228,9 +229,6 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
                                               uint64_t gtile, uint32_t side, bool stop_first,
                                               bool count_last) {
   __shared__ uint32_t s_warp[HJ_THREADS / 32];
-  __shared__ uint32_t s_flags[2 * (HJ_THREADS / 32)];
-  __shared__ uint64_t s_sum[HJ_THREADS / 32 + 1];
-  __shared__ int s_state;
   __shared__ uint64_t s_prefix;
   __shared__ uint32_t s_first[HJ_ITEMS][HJ_THREADS];  // first payload of each row
   __shared__ uint32_t s_row[HJ_ITEMS][HJ_THREADS];    // probe row id of each row (p.prow)
@@ -341,14 +339,16 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
       s_prefix = 0;
     }
   } else {
-    if (tid == 0)
-      pd_store_relaxed_u64(p.status + gtile, pd_pack_status(p.epoch, PD_FLAG_AGGREGATE, total));
-    uint64_t pre = pd_block_lookback<HJ_THREADS>(p.status, (int64_t)gtile, p.epoch, p.d_error,
-                                                 s_flags, s_sum, &s_state);
-    if (tid == 0) {
-      pd_store_relaxed_u64(p.status + gtile,
-                           pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, pre + total));
-      s_prefix = pre;
+    // One warp waits for the predecessors; the others wait at the barrier
+    // below without taking issue slots from the SM's other CTAs.
+    if (warp == 0) {
+      if (lane == 0)
+        pd_store_relaxed_u64(p.status + gtile, pd_pack_status(p.epoch, PD_FLAG_AGGREGATE, total));
+      const uint64_t pre = pd_lookback_warp(p.status, (int64_t)gtile, p.epoch, p.d_error);
+      if (lane == 0) {
+        pd_store_relaxed_u64(p.status + gtile, pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, pre + total));
+        s_prefix = pre;
+      }
     }
   }
   __syncthreads();

@@ -15,8 +15,9 @@
 //  2. k_smj_merge: a CTA takes the next outer tile, stages the tile's inner
 //     range in shared memory (when it fits; otherwise it searches HBM), finds
 //     each outer row's match range by binary search, scans the match counts,
-//     resolves the tile's output offset with a block-wide decoupled
-//     look-back, and writes the pairs.
+//     resolves the tile's output offset with a decoupled look-back (one warp
+//     polls while the rest of the CTA waits at a barrier), and writes the
+//     pairs.
 // The full join (pimdal_sort_merge_join) sorts both sides with K-SORT first.
 #include <algorithm>
 
@@ -98,9 +99,6 @@ __global__ void __launch_bounds__(MJ_THREADS) k_smj_merge(MergeParams p) {
   __shared__ uint32_t s_oo[MJ_OUT_CAP];  // staged output of the tile
   __shared__ uint32_t s_oi[MJ_OUT_CAP];
   __shared__ uint32_t s_warp[MJ_WARPS];
-  __shared__ uint32_t s_flags[2 * MJ_WARPS];
-  __shared__ uint64_t s_sum[MJ_WARPS + 1];
-  __shared__ int s_state;
   __shared__ uint32_t s_tile;
   __shared__ uint64_t s_prefix;
 
@@ -202,13 +200,16 @@ __global__ void __launch_bounds__(MJ_THREADS) k_smj_merge(MergeParams p) {
       s_prefix = 0;
     }
   } else {
-    if (tid == 0)
-      pd_store_relaxed_u64(p.status + tile, pd_pack_status(p.epoch, PD_FLAG_AGGREGATE, total));
-    uint64_t pre = pd_block_lookback<MJ_THREADS>(p.status, (int64_t)tile, p.epoch, p.d_error,
-                                                 s_flags, s_sum, &s_state);
-    if (tid == 0) {
-      pd_store_relaxed_u64(p.status + tile, pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, pre + total));
-      s_prefix = pre;
+    // One warp waits for the predecessors; the others wait at the barrier
+    // below without taking issue slots from the SM's other CTAs.
+    if (warp == 0) {
+      if (lane == 0)
+        pd_store_relaxed_u64(p.status + tile, pd_pack_status(p.epoch, PD_FLAG_AGGREGATE, total));
+      const uint64_t pre = pd_lookback_warp(p.status, (int64_t)tile, p.epoch, p.d_error);
+      if (lane == 0) {
+        pd_store_relaxed_u64(p.status + tile, pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, pre + total));
+        s_prefix = pre;
+      }
     }
   }
   __syncthreads();

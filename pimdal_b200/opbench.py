@@ -5,6 +5,9 @@
     python -m pimdal_b200.opbench smj       --rows 67108864          (inner = rows / 4)
     python -m pimdal_b200.opbench hash_join --rows 268435456         (build = rows / 8)
     python -m pimdal_b200.opbench group     --rows 268435456 --card 4096 --method hash|sort
+    python -m pimdal_b200.opbench bloom     --rows 268435456 --parts 16384 --match-permille 50
+                                             (build = rows / 8; both sides partitioned first,
+                                              untimed; times filter + match)
 
 The per-operator counterpart of the reference's benchmark programs
 (reference/db_operators/*.cpp main: generate, run the kernel a fixed number of
@@ -53,6 +56,15 @@ def _inputs(ctx: ops.Context, a) -> tuple:
         return (g(gen.Spec(L.GEN_PERM, L.I32, seed=a.seed, perm_domain=2 * nb), nb),
                 g(gen.Spec(L.GEN_UNIFORM, L.I32, seed=a.seed, stream_id=1, lo=-2**31, hi=2**31 - 1), nb),
                 g(spec_p, n))
+    if a.op == "bloom":
+        nb = max(n // 8, 1)
+        bk = g(gen.Spec(L.GEN_PERM, L.I32, seed=a.seed, perm_domain=2 * nb), nb)
+        pk = g(gen.Spec(L.GEN_PROBE, L.I32, seed=a.seed, stream_id=2, lo=nb, perm_domain=2 * nb,
+                        match_permille=a.match_permille), n)
+        obk, _, bps = ops.part_kernel(ctx, bk, shift=32, part_n=a.parts, want_ptr=False)
+        opk, oprow, pps = ops.part_kernel(ctx, pk, shift=32, part_n=a.parts)
+        ctx.sync()
+        return obk, bps, opk, oprow, pps
     if a.op == "group":
         keys = g(gen.Spec(L.GEN_PERM_UNIFORM, L.I32, seed=a.seed, stream_id=10, lo=0,
                           hi=a.card - 1, perm_domain=0), n)
@@ -85,6 +97,18 @@ def _runner(ctx: ops.Context, a, inp):
         return lambda: ops.hash_join(ctx, inp[0], inp[1], inp[2], capacity=n, out_payload=op,
                                      out_row=orow, result=res, partition_bits=a.partition_bits,
                                      load_factor_pct=a.load_factor)
+    if a.op == "bloom":
+        obk, bps, opk, oprow, pps = inp
+        filt = torch.empty(a.parts * L.FILTER_BYTES, dtype=torch.uint8, device=dev)
+        ok = torch.empty(n, dtype=torch.int32, device=dev)
+        orow = torch.empty(n, dtype=torch.int32, device=dev)
+        res = torch.empty(1, dtype=torch.int64, device=dev)
+
+        def bloom():
+            ops.filter_kernel(ctx, obk, bps, filters=filt)
+            ops.match_kernel(ctx, filt, opk, pps, oprow, out=ok, out_row=orow, result=res)
+        bloom.result = res
+        return bloom
     method = {"hash": L.GROUP_HASH, "sort": L.GROUP_SORT, "auto": L.GROUP_AUTO}[a.method]
     cap = 2 * a.card
     outs = {w: torch.empty(cap, dtype=torch.int64, device=dev) for w in ("sum", "count", "min", "max")}
@@ -96,7 +120,7 @@ def _runner(ctx: ops.Context, a, inp):
 
 def main(argv=None) -> None:
     p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    p.add_argument("op", choices=["select", "sort", "smj", "hash_join", "group"])
+    p.add_argument("op", choices=["select", "sort", "smj", "hash_join", "group", "bloom"])
     p.add_argument("--rows", type=int, default=1 << 24)
     p.add_argument("--iters", type=int, default=10)
     p.add_argument("--warmup", type=int, default=2)
@@ -107,6 +131,8 @@ def main(argv=None) -> None:
     p.add_argument("--partition-bits", type=int, default=0,
                    help="hash join: 0 = auto, 4294967295 = never partition, else 1..8")
     p.add_argument("--load-factor", type=int, default=0, help="hash join table load factor, percent")
+    p.add_argument("--parts", type=int, default=16384, help="bloom: partitions (power of 2)")
+    p.add_argument("--match-permille", type=int, default=50, help="bloom: probe match rate")
     p.add_argument("--device", type=int, default=0)
     p.add_argument("--kernels", action="store_true",
                    help="also print the mean time of each library kernel class")
@@ -149,6 +175,7 @@ def main(argv=None) -> None:
                       "method": a.method if a.op == "group" else None,
                       "ms_median": med, "ms_min": min(times) if times else None,
                       "rows_per_s": a.rows / (med * 1e-3) if times else None,
+                      "kept": int(run.result.item()) if hasattr(run, "result") else None,
                       "kernels": kernels}))
 
 

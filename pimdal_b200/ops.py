@@ -272,6 +272,51 @@ def hj_probe(ctx: Context, table, table_size: int, keys, ptr=None, *, capacity: 
     return result, out_outer, out_inner
 
 
+# ---------------------------------------------------------------------------
+# Bloom-filter prefilter (filter_kernel / match_kernel, pimdal/join/hash_join.h:66,76)
+# ---------------------------------------------------------------------------
+def filter_kernel(ctx: Context, keys, part_sizes, *, filters=None, pairs: bool = False,
+                  stream=None):
+    """One PIMDAL_FILTER_BYTES Bloom filter per partition of partitioned keys
+    (part_sizes: int64 device tensor of part_n + 1 row offsets).  keys is a
+    uint32/int32 column, or an (n, 2) key_ptr32 pair tensor with pairs=True.
+    Returns the filters (uint8 device tensor)."""
+    part_n = part_sizes.numel() - 1
+    if filters is None:
+        filters = torch.empty(part_n * L.FILTER_BYTES, dtype=torch.uint8, device=keys.device)
+    a = L.FilterArguments(in_=_ptr(keys), filter_ptr=_ptr(filters), part_sizes=_ptr(part_sizes),
+                          part_n=part_n, layout=L.LAYOUT_PAIRS if pairs else L.LAYOUT_COLUMNS)
+    L.check(ctx.lib.pimdal_filter_kernel(ctx.handle, C.byref(a), _stream(stream)),
+            "pimdal_filter_kernel")
+    return filters
+
+
+def match_kernel(ctx: Context, filters, keys, part_sizes, ptr=None, *, pairs: bool = False,
+                 capacity: int | None = None, out=None, out_row=None, want_row: bool = True,
+                 result=None, stream=None):
+    """Keeps the rows whose key hits its partition's filter, in input order.
+    Returns (result, kept keys or pairs, kept row ids or None, match_sizes)."""
+    dev = keys.device
+    n = keys.shape[0]
+    part_n = part_sizes.numel() - 1
+    if capacity is None:
+        capacity = max(n, 1)
+    if out is None:
+        out = torch.empty((capacity, 2) if pairs else capacity, dtype=torch.int32, device=dev)
+    if not pairs and want_row and out_row is None:
+        out_row = torch.empty(capacity, dtype=torch.int32, device=dev)
+    if result is None:
+        result = torch.empty(1, dtype=torch.int64, device=dev)
+    sizes = torch.empty(part_n + 1, dtype=torch.int64, device=dev)
+    a = L.MatchArguments(filter_ptr=_ptr(filters), size=n, part_ptr=_ptr(keys), part_row=_ptr(ptr),
+                         out_ptr=_ptr(out), out_row=_ptr(out_row), out_capacity=capacity,
+                         match_sizes=_ptr(sizes), part_sizes=_ptr(part_sizes), part_n=part_n,
+                         layout=L.LAYOUT_PAIRS if pairs else L.LAYOUT_COLUMNS)
+    L.check(ctx.lib.pimdal_match_kernel(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
+            "pimdal_match_kernel")
+    return result, out, (None if pairs else out_row), sizes
+
+
 def hash_join(ctx: Context, build_key, build_payload, probe_key, probe_ptr=None, *,
               capacity: int | None = None, partition_bits: int = 0, load_factor_pct: int = 0,
               l2_budget_bytes: int = 0, out_payload=None, out_row=None, result=None, stream=None):
