@@ -783,9 +783,10 @@ class ServeWorkload(Workload):
     flags) and two dimensions (1.5e7 orders, 2e6 parts), request row ranges
     log-uniform in [1e5, 6e7], date selectivity 1-50%, 8 concurrency slots
     under a 150 GB HBM budget.  A step is one saturated stream of 200 requests
-    (all arrived at the start); the same stream run serially (one request at a
-    time) and a Poisson stream at 70% of the serial throughput are measured
-    beside it."""
+    (all arrived at the start), each run as one fused filter-join-group-by
+    pass; the same stream run serially through the staged plain operators (one
+    request at a time), the concurrent staged run, and a Poisson stream at 70%
+    of the serial throughput are measured beside it."""
     name = "serve"
     R = 200
     SLOTS = 8
@@ -801,8 +802,8 @@ class ServeWorkload(Workload):
                        "requests_per_step": self.R, "slots": self.SLOTS, "hbm_budget_gb": 150,
                        "l2": "inputs (resident tables, GBs) larger than L2"}
         self.units_per_step = self.R
-        self.dominant = L.KERNEL_SELECT
-        self.dominant_name = "k_select (date-range selection)"
+        self.dominant = L.KERNEL_FUSED
+        self.dominant_name = "k_sja_aggregate (fused filter-join-group-by pass)"
 
     def setup(self, ctx, dev):
         import torch
@@ -828,16 +829,16 @@ class ServeWorkload(Workload):
         self._runs.append(st)
 
     def dominant_timing(self):
-        """(launches, ms) of the selection kernel over one served run (profiled)."""
+        """(launches, ms) of the fused pass over one served run (profiled)."""
         for sl in self.server.slots:
-            sl.ctx.kernel_time(self.L.KERNEL_SELECT)
+            sl.ctx.kernel_time(self.dominant)
             sl.ctx.set_profiling(True)
         st = self.server.run(self.reqs)
         n = ms = 0
         for sl in self.server.slots:
             sl.ctx.sync(sl.stream)
             sl.ctx.set_profiling(False)
-            a, b = sl.ctx.kernel_time(self.L.KERNEL_SELECT)
+            a, b = sl.ctx.kernel_time(self.dominant)
             n += a
             ms += b
         self._sel_rows = sum(r.n for r in self.reqs)
@@ -859,11 +860,15 @@ class ServeWorkload(Workload):
         pois = serve.make_requests(self.R, self.tables.n, rate=rate, seed=0xB207)
         p_served = self.server.run(pois).summary()
         p_serial = self.server.run(pois, serial=True).summary()
-        same = serve.same_results(served, serial)
+        staged = self.server.run(self.reqs, fused=False)
+        same = serve.same_results(served, serial) and serve.same_results(staged, serial)
+        stg = staged.summary()
         return {"served_saturated": served.summary(), "serial_saturated": ser,
+                "served_staged_saturated": stg,
                 "poisson": {"rate_per_s": round(rate, 2), "served": p_served, "serial": p_serial},
                 "served_equals_serial": same,
-                "speedup_vs_serial": round(served.summary()["queries_per_s"] / ser["queries_per_s"], 3)}
+                "speedup_vs_serial": round(served.summary()["queries_per_s"] / ser["queries_per_s"], 3),
+                "speedup_staged_concurrency_only": round(stg["queries_per_s"] / ser["queries_per_s"], 3)}
 
     def step_e2e(self, stream):
         """A served run: request parameters in kernel arguments, each result

@@ -108,7 +108,8 @@ typedef enum {
   PIMDAL_KERNEL_OTHER = 10,
   PIMDAL_KERNEL_FILTER = 11,     /* Bloom filter build                     */
   PIMDAL_KERNEL_MATCH = 12,      /* Bloom filter probe + ordered compaction*/
-  PIMDAL_KERNEL_COUNT = 13
+  PIMDAL_KERNEL_FUSED = 13,      /* fused select -> join -> group-by pass  */
+  PIMDAL_KERNEL_COUNT = 14
 } pimdal_kernel_id_t;
 int pimdal_ctx_set_profiling(pimdal_ctx_t *ctx, int enable);
 int pimdal_ctx_kernel_time(pimdal_ctx_t *ctx, int kernel_id, uint64_t *launches,
@@ -492,6 +493,44 @@ typedef struct {
 
 int pimdal_revenue_keys(pimdal_ctx_t *ctx, const pimdal_revenue_arguments_t *args,
                         pimdal_stream_t stream);
+
+/* Fused filter -> join -> group-by of one query over a fact range: the chain  */
+/* the reference's TPC-H pipelines run as sel_kernel, merge_kernel,           */
+/* arithmetic_kernel and group_kernel with host steps between them (e.g.      */
+/* pimdal/main/tpc_h/query6/dpu/kernel_q6.c:112-156), in one pass.  Fact row  */
+/* r < size takes part when date_lo <= date[r] <= date_hi; it is joined       */
+/* through a table built by pimdal_hash_kernel (every build row whose key is  */
+/* jkey[r] contributes, its payload being the attribute); the group key is    */
+/* attr * attr_mult + (flag ? flag[r] : 0) and the value                      */
+/* price[r] * (100 - discount[r]).  Output: the groups with at least one row, */
+/* ascending by key, with SUM (int64, wrapping) and COUNT -- exactly what     */
+/* selection + gather + pimdal_hj_probe + pimdal_revenue_keys +               */
+/* pimdal_group_kernel return.  Group keys must be < key_space (at most       */
+/* PIMDAL_FUSED_MAX_KEYS); a larger one raises PIMDAL_ERR_ARG at              */
+/* pimdal_ctx_sync_status.  Scratch: key_space * 16 bytes of the context's    */
+/* workspace.                                                                 */
+#define PIMDAL_FUSED_MAX_KEYS 4096
+typedef struct {
+  uint64_t size;               /* fact rows in the range                        */
+  const int32_t *date;         /* filter column                                 */
+  int32_t date_lo, date_hi;    /* inclusive bounds                              */
+  const uint32_t *jkey;        /* join key per fact row                         */
+  const void *table_ptr;       /* table of pimdal_hash_kernel                   */
+  uint64_t table_size;         /* its slots                                     */
+  const uint8_t *flag;         /* second group column (NULL: none)              */
+  const int64_t *price;
+  const int32_t *discount;     /* percent, 0..100                               */
+  uint32_t attr_mult;          /* key = attr * attr_mult + flag[row]            */
+  uint32_t key_space;          /* keys are < key_space (1..PIMDAL_FUSED_MAX_KEYS) */
+  uint32_t *out_key;           /* groups, ascending                             */
+  int64_t *out_sum;
+  int64_t *out_count;
+  uint64_t out_capacity;
+} pimdal_select_join_aggregate_arguments_t;
+
+int pimdal_select_join_aggregate(pimdal_ctx_t *ctx,
+                                 const pimdal_select_join_aggregate_arguments_t *args,
+                                 pimdal_aggr_results_t *d_result, pimdal_stream_t stream);
 
 /* ------------------------------------------------------------------------- */
 /* Batched form: many independent group-by or hash-join instances, each phase */

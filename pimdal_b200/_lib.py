@@ -25,7 +25,7 @@ PRED_LT, PRED_LE, PRED_GT, PRED_GE, PRED_EQ, PRED_NE, PRED_BETWEEN, PRED_RANGE =
 GEN_UNIFORM, GEN_PERM, GEN_PERM_UNIFORM, GEN_PERM_ZIPF, GEN_PROBE = range(5)
 (KERNEL_SELECT, KERNEL_GEN, KERNEL_SORT_HIST, KERNEL_SORT_PASS, KERNEL_SMJ_MERGE, KERNEL_PARTITION,
  KERNEL_HJ_BUILD, KERNEL_HJ_PROBE, KERNEL_GROUP, KERNEL_SEGREDUCE, KERNEL_OTHER, KERNEL_FILTER,
- KERNEL_MATCH) = range(13)
+ KERNEL_MATCH, KERNEL_FUSED) = range(14)
 FILTER_BITS = 16384
 FILTER_BYTES = FILTER_BITS // 8
 
@@ -137,6 +137,19 @@ class MatchArguments(C.Structure):
     ]
 
 
+FUSED_MAX_KEYS = 4096
+
+
+class SelectJoinAggregateArguments(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint64), ("date", C.c_void_p), ("date_lo", C.c_int32), ("date_hi", C.c_int32),
+        ("jkey", C.c_void_p), ("table_ptr", C.c_void_p), ("table_size", C.c_uint64),
+        ("flag", C.c_void_p), ("price", C.c_void_p), ("discount", C.c_void_p),
+        ("attr_mult", C.c_uint32), ("key_space", C.c_uint32), ("out_key", C.c_void_p),
+        ("out_sum", C.c_void_p), ("out_count", C.c_void_p), ("out_capacity", C.c_uint64),
+    ]
+
+
 GROUP_AUTO, GROUP_HASH, GROUP_SORT = 0, 1, 2
 
 
@@ -193,6 +206,7 @@ SIGNATURES = {
     "pimdal_hash_kernel": (_I, [_VP, C.POINTER(HashArguments), _VP]),
     "pimdal_hj_probe": (_I, [_VP, C.POINTER(ProbeArguments), _VP, _VP]),
     "pimdal_filter_kernel": (_I, [_VP, C.POINTER(FilterArguments), _VP]),
+    "pimdal_select_join_aggregate": (_I, [_VP, C.POINTER(SelectJoinAggregateArguments), _VP, _VP]),
     "pimdal_match_kernel": (_I, [_VP, C.POINTER(MatchArguments), _VP, _VP]),
     "pimdal_hash_join_workspace_size": (_I, [C.POINTER(HashJoinArguments), C.POINTER(_SZ)]),
     "pimdal_hash_join": (_I, [_VP, C.POINTER(HashJoinArguments), _VP, _VP]),

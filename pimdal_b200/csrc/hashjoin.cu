@@ -761,7 +761,8 @@ extern "C" int pimdal_hash_kernel(pimdal_ctx_t *ctx, const pimdal_hash_arguments
                                   pimdal_stream_t stream) {
   if (!ctx || !a || !a->table_ptr || ((uintptr_t)a->table_ptr & 31u)) return PIMDAL_ERR_ARG;
   if (a->size && !a->in_key) return PIMDAL_ERR_ARG;
-  if (a->table_size < 16 || (a->table_size & (a->table_size - 1)) || a->size > a->table_size)
+  if (a->table_size < 16 || (a->table_size & (a->table_size - 1)) || a->size > a->table_size ||
+      a->table_size > (1ull << 32))  // bucket_of's 32-bit arithmetic
     return PIMDAL_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   cudaSetDevice(ctx->device);
@@ -793,7 +794,8 @@ extern "C" int pimdal_hj_probe(pimdal_ctx_t *ctx, const pimdal_probe_arguments_t
   if (!ctx || !a || !d_result || !a->table_ptr || ((uintptr_t)a->table_ptr & 31u)) return PIMDAL_ERR_ARG;
   if (a->size && !a->in_key) return PIMDAL_ERR_ARG;
   if (a->out_capacity && (!a->out_inner || !a->out_outer)) return PIMDAL_ERR_ARG;
-  if (a->table_size < 16 || (a->table_size & (a->table_size - 1)) || a->size >= (1ull << 32))
+  if (a->table_size < 16 || (a->table_size & (a->table_size - 1)) || a->size >= (1ull << 32) ||
+      a->table_size > (1ull << 32))
     return PIMDAL_ERR_ARG;
   cudaStream_t s = (cudaStream_t)stream;
   cudaSetDevice(ctx->device);
@@ -964,4 +966,208 @@ extern "C" int pimdal_part_kernel(pimdal_ctx_t *ctx, const pimdal_part_arguments
   sa.begin_bit = sh;
   sa.end_bit = a->shift;
   return pd_sort_ex(ctx, &sa, PD_KEY_HASH0, ws, s, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// pimdal_select_join_aggregate: one query's filter -> join -> group-by in one
+// pass over its fact range (the reference chains sel_kernel, merge_kernel,
+// arithmetic_kernel and group_kernel with host steps between them, e.g.
+// pimdal/main/tpc_h/query6/dpu/kernel_q6.c:112-156).  Each selected row
+// probes the resident table exactly as pimdal_hj_probe does and adds its
+// revenue to a shared-memory table indexed by the (small, dense) group key:
+// one table per warp for key spaces up to 256 keys, one per CTA above.  The
+// CTAs' tables are folded into a global table with one atomic per key, and a
+// single CTA emits the non-empty groups in key order.  Integer sums do not
+// depend on the order of the additions, so the result is bit-identical to
+// the staged pipeline's.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int SJA_THREADS = 256;
+constexpr int SJA_WARPS = SJA_THREADS / 32;
+constexpr uint32_t SJA_WARP_KEYS = 256;  // key spaces up to this get one table per warp
+static_assert(PIMDAL_FUSED_MAX_KEYS * 12 <= 48 * 1024, "a CTA-wide table fits 48 KB");
+static_assert(SJA_WARP_KEYS * SJA_WARPS <= PIMDAL_FUSED_MAX_KEYS, "per-warp tables fit too");
+
+struct SjaParams {
+  uint64_t n;
+  const int32_t *date;
+  int32_t lo, hi;
+  const uint32_t *jkey;
+  const unsigned long long *table;  // the slots, after the table's 32-byte header
+  uint32_t bits;
+  const uint32_t *side_count, *dup_flag;
+  const uint8_t *flag;
+  const int64_t *price;
+  const int32_t *discount;
+  uint32_t attr_mult, key_space;
+  unsigned long long *g_sum, *g_cnt;  // key_space words each (workspace)
+  uint32_t *d_error;
+};
+
+uint32_t sja_tables(uint32_t key_space) { return key_space <= SJA_WARP_KEYS ? SJA_WARPS : 1; }
+
+__global__ void __launch_bounds__(SJA_THREADS) k_sja_aggregate(SjaParams p) {
+  extern __shared__ __align__(16) unsigned long long sja_smem[];
+  const uint32_t ks = p.key_space;
+  const uint32_t tables = ks <= SJA_WARP_KEYS ? SJA_WARPS : 1;
+  unsigned long long *s_sum = sja_smem;                                           // [tables][ks]
+  unsigned int *s_cnt = reinterpret_cast<unsigned int *>(sja_smem + tables * ks);  // [tables][ks]
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (uint32_t i = tid; i < tables * ks; i += SJA_THREADS) {
+    s_sum[i] = 0;
+    s_cnt[i] = 0;
+  }
+  __syncthreads();
+  unsigned long long *my_sum = s_sum + (warp % tables) * ks;
+  unsigned int *my_cnt = s_cnt + (warp % tables) * ks;
+  const uint32_t gmask = (uint32_t)(((1ull << p.bits) - 1) >> 2);
+  const uint32_t side = *p.side_count;
+  const bool no_dup = *p.dup_flag == 0;
+  bool bad = false;
+  const uint64_t stride = (uint64_t)gridDim.x * SJA_THREADS;
+  for (uint64_t r = (uint64_t)blockIdx.x * SJA_THREADS + tid; r < p.n; r += stride) {
+    const int32_t d = __ldcs(p.date + r);
+    if (d < p.lo || d > p.hi) continue;
+    const uint32_t key = __ldg(p.jkey + r);
+    const uint32_t f = p.flag ? __ldg(p.flag + r) : 0u;
+    const int64_t v = __ldg(p.price + r) * (int64_t)(100 - __ldg(p.discount + r));
+    auto add = [&](uint32_t attr) {
+      const uint64_t g = (uint64_t)attr * p.attr_mult + f;
+      if (g >= ks) {
+        bad = true;
+        return;
+      }
+      atomicAdd(&my_sum[g], (unsigned long long)v);
+      atomicAdd(&my_cnt[g], 1u);
+    };
+    // the bucket walk of the probe: stop at a bucket with a free slot, or at
+    // the first match when the build had no duplicate key
+    const bool stop_first = no_dup && key != 0xFFFFFFFFu;
+    uint32_t b = bucket_of(key, 0, p.bits);
+    for (uint64_t step = 0; step <= gmask; ++step) {
+      const ulonglong2 *q = reinterpret_cast<const ulonglong2 *>(p.table + 4 * (uint64_t)b);
+      const ulonglong2 lo = q[0], hi = q[1];
+      const unsigned long long e[4] = {lo.x, lo.y, hi.x, hi.y};
+      bool empty = false, found = false;
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        if (e[j] == HJ_EMPTY) {
+          empty = true;
+        } else if ((uint32_t)e[j] == key) {
+          add((uint32_t)(e[j] >> 32));
+          found = true;
+        }
+      }
+      if (empty || (stop_first && found)) break;
+      b = (b + 1) & gmask;
+    }
+    if (key == 0xFFFFFFFFu)  // build rows equal to the empty word, counted on the side
+      for (uint32_t m = 0; m < side; ++m) add(0xFFFFFFFFu);
+  }
+  if (bad) atomicOr(p.d_error, PD_DEVERR_ARG);
+  __syncthreads();
+  for (uint32_t k = tid; k < ks; k += SJA_THREADS) {
+    unsigned long long sum = 0, cnt = 0;
+    for (uint32_t t = 0; t < tables; ++t) {
+      sum += s_sum[t * ks + k];
+      cnt += s_cnt[t * ks + k];
+    }
+    if (cnt) {
+      atomicAdd(&p.g_sum[k], sum);
+      atomicAdd(&p.g_cnt[k], cnt);
+    }
+  }
+}
+
+// One CTA: the non-empty groups in key order.
+__global__ void __launch_bounds__(1024) k_sja_emit(const unsigned long long *g_sum,
+                                                   const unsigned long long *g_cnt, uint32_t ks,
+                                                   uint32_t *out_key, int64_t *out_sum,
+                                                   int64_t *out_count, uint64_t cap,
+                                                   uint64_t *t_count, uint32_t *d_error) {
+  __shared__ uint32_t s_warp[32];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t base = 0;
+  bool overflow = false;
+  for (uint32_t k0 = 0; k0 < ks; k0 += 1024) {
+    const uint32_t k = k0 + tid;
+    const bool has = k < ks && g_cnt[k] != 0;
+    const unsigned m = __ballot_sync(0xffffffffu, has);
+    if (lane == 0) s_warp[warp] = __popc(m);
+    __syncthreads();
+    uint32_t pre = 0, total = 0;
+    for (int w = 0; w < 32; ++w) {
+      const uint32_t x = s_warp[w];
+      if (w < warp) pre += x;
+      total += x;
+    }
+    if (has) {
+      const uint64_t pos = base + pre + __popc(m & ((1u << lane) - 1u));
+      if (pos < cap) {
+        out_key[pos] = k;
+        out_sum[pos] = (int64_t)g_sum[k];
+        out_count[pos] = (int64_t)g_cnt[k];
+      } else {
+        overflow = true;
+      }
+    }
+    base += total;
+    __syncthreads();  // s_warp is rewritten by the next round
+  }
+  if (overflow) atomicOr(d_error, PD_DEVERR_CAPACITY);
+  if (tid == 0) *t_count = base;
+}
+
+}  // namespace
+
+extern "C" int pimdal_select_join_aggregate(pimdal_ctx_t *ctx,
+                                            const pimdal_select_join_aggregate_arguments_t *a,
+                                            pimdal_aggr_results_t *d_result, pimdal_stream_t stream) {
+  if (!ctx || !a || !d_result || !a->table_ptr || ((uintptr_t)a->table_ptr & 31u)) return PIMDAL_ERR_ARG;
+  if (a->table_size < 16 || (a->table_size & (a->table_size - 1)) || a->table_size > (1ull << 32))
+    return PIMDAL_ERR_ARG;
+  if (a->key_space == 0 || a->key_space > PIMDAL_FUSED_MAX_KEYS || a->size >= (1ull << 32))
+    return PIMDAL_ERR_ARG;
+  if (a->size && (!a->date || !a->jkey || !a->price || !a->discount)) return PIMDAL_ERR_ARG;
+  if (a->out_capacity && (!a->out_key || !a->out_sum || !a->out_count)) return PIMDAL_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaSetDevice(ctx->device);
+  const size_t ws_bytes = 16ull * a->key_space;
+  int st;
+  char *ws = (char *)pd_workspace(ctx, ws_bytes, s, &st);
+  if (!ws) return st;
+  PD_CHECK_CUDA(cudaMemsetAsync(ws, 0, ws_bytes, s));
+  SjaParams p{};
+  p.n = a->size;
+  p.date = a->date;
+  p.lo = a->date_lo;
+  p.hi = a->date_hi;
+  p.jkey = a->jkey;
+  p.table = (const unsigned long long *)a->table_ptr + 4;
+  p.side_count = (const uint32_t *)a->table_ptr;
+  p.dup_flag = (const uint32_t *)a->table_ptr + 2;
+  uint32_t bits = 0;
+  while ((1ull << bits) < a->table_size) ++bits;
+  p.bits = bits;
+  p.flag = a->flag;
+  p.price = a->price;
+  p.discount = a->discount;
+  p.attr_mult = a->attr_mult;
+  p.key_space = a->key_space;
+  p.g_sum = (unsigned long long *)ws;
+  p.g_cnt = (unsigned long long *)ws + a->key_space;
+  p.d_error = ctx->d_error;
+  if (a->size) {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_FUSED, s);
+    const size_t smem = 12ull * sja_tables(a->key_space) * a->key_space;
+    const unsigned g = (unsigned)std::min<uint64_t>(pd_ceil_div(a->size, SJA_THREADS), ctx->sm_count * 4ull);
+    k_sja_aggregate<<<g, SJA_THREADS, smem, s>>>(p);
+  }
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_sja_emit<<<1, 1024, 0, s>>>(p.g_sum, p.g_cnt, a->key_space, a->out_key, a->out_sum,
+                                  a->out_count, a->out_capacity, &d_result->t_count, ctx->d_error);
+  }
+  return pd_launch_status(ctx);
 }

@@ -272,6 +272,29 @@ def hj_probe(ctx: Context, table, table_size: int, keys, ptr=None, *, capacity: 
     return result, out_outer, out_inner
 
 
+def select_join_aggregate(ctx: Context, date, lo: int, hi: int, jkey, table, table_size: int,
+                          price, discount, *, flag=None, attr_mult: int = 1, key_space: int,
+                          outs=None, result=None, stream=None):
+    """One query's date filter -> join -> SUM(price*(100-discount)), COUNT
+    group-by in one pass.  Returns (result, outs) with outs key/sum/count
+    columns holding the groups in key order (result[0] of them)."""
+    dev = date.device
+    if outs is None:
+        outs = {"key": torch.empty(key_space, dtype=torch.int32, device=dev),
+                "sum": torch.empty(key_space, dtype=torch.int64, device=dev),
+                "count": torch.empty(key_space, dtype=torch.int64, device=dev)}
+    if result is None:
+        result = torch.empty(1, dtype=torch.int64, device=dev)
+    a = L.SelectJoinAggregateArguments(
+        size=date.numel(), date=_ptr(date), date_lo=lo, date_hi=hi, jkey=_ptr(jkey),
+        table_ptr=_ptr(table), table_size=table_size, flag=_ptr(flag), price=_ptr(price),
+        discount=_ptr(discount), attr_mult=attr_mult, key_space=key_space, out_key=_ptr(outs["key"]),
+        out_sum=_ptr(outs["sum"]), out_count=_ptr(outs["count"]), out_capacity=outs["key"].numel())
+    L.check(ctx.lib.pimdal_select_join_aggregate(ctx.handle, C.byref(a), _ptr(result),
+                                                 _stream(stream)), "pimdal_select_join_aggregate")
+    return result, outs
+
+
 # ---------------------------------------------------------------------------
 # Bloom-filter prefilter (filter_kernel / match_kernel, pimdal/join/hash_join.h:66,76)
 # ---------------------------------------------------------------------------

@@ -11,18 +11,22 @@ payload) and stay resident.  A request is
     FROM fact[r0 : r0 + n] JOIN dim USING (key)
     WHERE date BETWEEN d0 AND d1  GROUP BY attr [, flag]  ORDER BY attr [, flag]
 
-run as four stages on the GPU: selection of the date range (row ids),
-gather of the join keys, probe of the resident table, fused key/revenue
-gather, hash group-by (groups come out ordered by key).  The stages are a
-non-blocking state machine: a stage is launched on the request's slot
-(one CUDA stream and one library context each), the counts it produces are
-copied to pinned host memory, and the next stage starts when they arrive.
+run either fused -- one pass, pimdal_select_join_aggregate: date filter,
+probe of the resident table, revenue, group-by into a table indexed by the
+small group key -- or as the plain operators in stages: selection of the
+date range (row ids), gather of the join keys, probe of the resident table,
+fused key/revenue gather, hash group-by (groups come out ordered by key).
+Both give identical groups.  The stages are a non-blocking state machine: a
+stage is launched on the request's slot (one CUDA stream and one library
+context each), the counts it produces are copied to pinned host memory, and
+the next stage starts when they arrive.
 
 Scheduling (continuous batching): requests arrive (Poisson); an arrived
 request is admitted as soon as a slot is free and its working-set bytes fit
 the HBM byte budget left after the resident tables; admitted requests run
-concurrently, their stages interleaving on the device.  Serial plain
-execution is the same loop with one slot and one request at a time.  The
+concurrently, their stages interleaving on the device.  Served runs use the
+fused pass by default; serial plain execution is the same loop with one
+slot, one request at a time, through the staged plain operators.  The
 reference runs one query at a time on the DPUs (pimdal/main/tpc_h/*/host).
 """
 from __future__ import annotations
@@ -116,6 +120,10 @@ class Tables:
         ts = [v for v in vars(self).values() if isinstance(v, torch.Tensor)]
         return sum(t.numel() * t.element_size() for t in ts)
 
+    def n_attr(self, which: int) -> int:
+        """Distinct values of the dimension attribute (the build payload)."""
+        return N_PRIO if which == 0 else N_CAT
+
     def dim(self, which: int):
         """(join key column of the fact, table, table size, flag column, attribute count)."""
         if which == 0:
@@ -172,6 +180,7 @@ class Slot:
         self.req: Request | None = None
         self.stage = 0
         self.result: Result | None = None
+        self.fused = False  # run requests as one fused pass (else the staged operators)
 
     def close(self):
         self.ctx.close()
@@ -186,7 +195,19 @@ class Slot:
     def _launch(self, t: Tables) -> None:
         r, s, ctx = self.req, self.stream, self.ctx
         with torch.cuda.stream(s):
-            if self.stage == 0:
+            if self.fused:
+                col, table, tsize, flag, nflag = t.dim(r.dim)
+                mult = nflag if r.two_keys else 1
+                rng = slice(r.r0, r.r0 + r.n)
+                ops.select_join_aggregate(
+                    ctx, t.l_date[rng], r.d0, r.d1, col[rng], table, tsize, t.l_price[rng],
+                    t.l_discount[rng], flag=flag[rng] if r.two_keys else None, attr_mult=mult,
+                    key_space=t.n_attr(r.dim) * mult, outs=self.outs, result=self.res[2:3], stream=s)
+                self.h_cnt[2:3].copy_(self.res[2:3], non_blocking=True)
+                self.h_key.copy_(self.outs["key"], non_blocking=True)
+                self.h_sum.copy_(self.outs["sum"], non_blocking=True)
+                self.h_count.copy_(self.outs["count"], non_blocking=True)
+            elif self.stage == 0:
                 pred = ops.make_pred(L.PRED_BETWEEN, r.d0, r.d1)
                 ops.sel_kernel(ctx, t.l_date[r.r0:r.r0 + r.n], pred, ptr_base=r.r0,
                                out=self.sel_val, out_ptr=self.sel_row, result=self.res[0:1],
@@ -218,6 +239,8 @@ class Slot:
         """Advances the request when its stage finished; True when it is done."""
         if not self.event.query():
             return False
+        if self.fused:
+            return self._finish(now, int(self.h_cnt[2]))
         if self.stage == 0:
             self.result.selected = int(self.h_cnt[0])
             if self.result.selected == 0:
@@ -293,18 +316,25 @@ class Server:
             s.close()
 
     def warm(self) -> None:
-        """One small and one large request through every slot (workspaces)."""
+        """A large request of each dimension through every slot, staged and
+        fused (workspaces)."""
         rs = [Request(0, 0.0, 0, self.max_rows, 0, DAYS - 1, d, True) for d in (0, 1)]
         for s in self.slots:
-            for r in rs:
-                s.start(self.tables, r, 0.0)
-                while not s.poll(self.tables, 0.0):
-                    pass
+            for fused in (False, True):
+                s.fused = fused
+                for r in rs:
+                    s.start(self.tables, r, 0.0)
+                    while not s.poll(self.tables, 0.0):
+                        pass
 
-    def run(self, requests: list[Request], serial: bool = False) -> RunStats:
+    def run(self, requests: list[Request], serial: bool = False,
+            fused: bool | None = None) -> RunStats:
         """Plays the request stream (arrival times relative to the start).
-        serial: one slot, one request at a time (plain execution)."""
+        serial: one slot, one request at a time.  fused: one pass per request
+        (default: fused when served, the staged plain operators when serial)."""
         slots = self.slots[:1] if serial else self.slots
+        for s in slots:
+            s.fused = (not serial) if fused is None else fused
         adm = Admission(self.budget)
         pending = deque(sorted(requests, key=lambda r: r.arrival))
         queue: deque[Request] = deque()

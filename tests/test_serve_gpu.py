@@ -1,11 +1,16 @@
 """GPU parity of the served form: every request's groups (key, SUM of
 price * (100 - discount), COUNT) equal a numpy restatement of the pipeline,
-and are identical alone (serial plain execution), in the concurrent mix and
-under a byte budget that admits one request at a time."""
+and are identical through the fused pass and the staged plain operators,
+alone (serial plain execution), in the concurrent mix and under a byte
+budget that admits one request at a time.  The fused operator
+(pimdal_select_join_aggregate) is also checked on its own: duplicate build
+keys, a second group column, empty ranges, no selected row, a key outside the
+key space and a full output."""
 import numpy as np
 import pytest
 import torch
 
+from pimdal_b200 import _lib as L
 from pimdal_b200 import ops, serve
 
 pytestmark = pytest.mark.gpu
@@ -44,11 +49,12 @@ def expected(t, r):
 def test_served_equals_serial_and_numpy(server):
     t = server.tables
     reqs = serve.make_requests(40, t.n, rate=2000.0, seed=21, min_rows=1_000, max_rows=t.n)
-    served = server.run(reqs)
-    serial = server.run(reqs, serial=True)
+    served = server.run(reqs)                      # fused passes, concurrent
+    staged = server.run(reqs, fused=False)         # staged operators, concurrent
+    serial = server.run(reqs, serial=True)         # staged operators, one at a time
     assert len(served.results) == len(serial.results) == len(reqs)
     assert served.max_inflight > 1 and serial.max_inflight == 1
-    assert serve.same_results(served, serial)
+    assert serve.same_results(served, serial) and serve.same_results(staged, serial)
     for r in reqs:
         k, s, c = expected(t, r)
         got = served.results[r.rid]
@@ -69,3 +75,80 @@ def test_budget_admits_one_request_at_a_time(server):
     assert tight.max_reserved <= max(r.need_bytes for r in reqs)
     loose = server.run(reqs)
     assert serve.same_results(tight, loose)
+
+
+def fused_expected(date, lo, hi, jkey, bkey, battr, flag, mult, price, disc):
+    """numpy: every selected row joined with every build row of its key."""
+    sel = np.nonzero((date >= lo) & (date <= hi))[0]
+    order = np.argsort(bkey, kind="stable")
+    sk = bkey[order]
+    keys, vals = [], []
+    for r in sel:
+        a, b = np.searchsorted(sk, jkey[r], "left"), np.searchsorted(sk, jkey[r], "right")
+        for i in order[a:b]:
+            keys.append(int(battr[i]) * mult + (int(flag[r]) if flag is not None else 0))
+            vals.append(int(price[r]) * (100 - int(disc[r])))
+    keys = np.asarray(keys, np.int64)
+    vals = np.asarray(vals, np.int64)
+    uk, inv = np.unique(keys, return_inverse=True)
+    sums = np.zeros(uk.size, np.int64)
+    np.add.at(sums, inv, vals)
+    return uk, sums, np.bincount(inv, minlength=uk.size).astype(np.int64)
+
+
+def test_fused_operator_matches_numpy_with_duplicate_build_keys(ctx):
+    rng = np.random.default_rng(31)
+    n, nb, attrs, nflag = 50_000, 3000, 12, 3
+    bkey = rng.integers(0, 2000, nb).astype(np.uint32)   # many duplicate keys
+    battr = rng.integers(0, attrs, nb).astype(np.uint32)
+    jkey = rng.integers(0, 2600, n).astype(np.uint32)
+    date = rng.integers(0, 2557, n).astype(np.int32)
+    price = rng.integers(90_000, 10_500_000, n).astype(np.int64)
+    disc = rng.integers(0, 11, n).astype(np.int32)
+    flag = rng.integers(0, nflag, n).astype(np.uint8)
+    d = lambda a: torch.from_numpy(a).cuda()
+    table = ops.hash_kernel(ctx, d(bkey.view(np.int32)), d(battr.view(np.int32)), table_size=8192)
+    for lo, hi, fl in ((300, 1500, flag), (0, 2556, None), (3000, 4000, None)):
+        mult = nflag if fl is not None else 1
+        res, outs = ops.select_join_aggregate(
+            ctx, d(date), lo, hi, d(jkey.view(np.int32)), table, 8192, d(price), d(disc),
+            flag=None if fl is None else d(fl), attr_mult=mult, key_space=attrs * mult)
+        ctx.sync()
+        g = int(res.item())
+        k, s_, c = fused_expected(date, lo, hi, jkey, bkey, battr, fl, mult, price, disc)
+        assert g == k.size
+        assert np.array_equal(outs["key"][:g].cpu().numpy(), k)
+        assert np.array_equal(outs["sum"][:g].cpu().numpy(), s_)
+        assert np.array_equal(outs["count"][:g].cpu().numpy(), c)
+
+
+def test_fused_operator_edges(ctx):
+    d = lambda a: torch.from_numpy(a).cuda()
+    bkey = np.arange(100, dtype=np.int32)
+    table = ops.hash_kernel(ctx, d(bkey), d(bkey % 7), table_size=256)
+    z32, z64 = np.zeros(0, np.int32), np.zeros(0, np.int64)
+    res, _ = ops.select_join_aggregate(ctx, d(z32), 0, 10, d(z32), table, 256, d(z64), d(z32),
+                                       key_space=7)
+    ctx.sync()
+    assert int(res.item()) == 0
+    n = 1000
+    date = np.full(n, 5, np.int32)
+    jk = np.arange(n, dtype=np.int32) % 100
+    price, disc = np.ones(n, np.int64), np.zeros(n, np.int32)
+    res, _ = ops.select_join_aggregate(ctx, d(date), 6, 9, d(jk), table, 256, d(price), d(disc),
+                                       key_space=7)
+    ctx.sync()
+    assert int(res.item()) == 0  # no row selected
+    res, _ = ops.select_join_aggregate(ctx, d(date), 0, 9, d(jk), table, 256, d(price), d(disc),
+                                       key_space=6)  # attribute 6 lies outside the key space
+    with pytest.raises(L.PimdalError) as e:
+        ctx.sync()
+    assert e.value.status == 1
+    small = {"key": torch.empty(3, dtype=torch.int32, device="cuda"),
+             "sum": torch.empty(3, dtype=torch.int64, device="cuda"),
+             "count": torch.empty(3, dtype=torch.int64, device="cuda")}
+    res, _ = ops.select_join_aggregate(ctx, d(date), 0, 9, d(jk), table, 256, d(price), d(disc),
+                                       key_space=7, outs=small)
+    with pytest.raises(L.PimdalError) as e:
+        ctx.sync()
+    assert e.value.status == 7 and int(res.item()) == 7
