@@ -292,6 +292,22 @@ int pimdal_sort_merge_join(pimdal_ctx_t *ctx, const pimdal_smj_arguments_t *args
                            pimdal_merge_results_t *d_result, pimdal_stream_t stream);
 
 /* ------------------------------------------------------------------------- */
+/* Ingress of a host column into device memory.  Replaces the scatter of     */
+/* Arrow buffers to the DPUs (populate_mram / dist_table,                     */
+/* pimdal/support/transfer_helper.h, after the parquet read of                */
+/* pimdal/main/tpc_h/reader/read_table.cpp:18-34): copies bytes from host     */
+/* memory to dst on the stream.  A pageable source goes through two pinned    */
+/* staging buffers of PIMDAL_INGEST_CHUNK bytes owned by the context (made by */
+/* the first call), so the host copy of one chunk overlaps the transfer of   */
+/* the previous one; a pinned (page-locked or registered) source is copied    */
+/* directly.  On return the source may be reused: every host read is done;   */
+/* the device copy completes in stream order.                                */
+/* ------------------------------------------------------------------------- */
+#define PIMDAL_INGEST_CHUNK (16u << 20)
+int pimdal_ingest(pimdal_ctx_t *ctx, const void *host_src, size_t bytes, void *dst,
+                  pimdal_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
 /* Radix partition.  Replaces part_kernel (pimdal/join/hash_join.h:23-31,    */
 /* hash_join.c:154-235): element e goes to partition                         */
 /* (hash0(e.key) >> (shift - log2(part_n))) & (part_n - 1), hash0 being the  */

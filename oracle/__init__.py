@@ -311,6 +311,17 @@ class Ref:
         c = int(f(_p(fl), _p(k), _p(pp), _p(ps), ps.size - 1, _p(ok), _p(op), _p(ms)))
         return ok[:c], op[:c], ms
 
+    def date_to_int(self, dates) -> np.ndarray:
+        """The reference reader's packed dates of "YYYY-MM-DD" strings."""
+        f = self._get("reader").pimdal_ref_date_to_int
+        f.restype = None
+        f.argtypes = [C.c_char_p, _U64, _P]
+        buf = "".join(dates).encode()
+        assert len(buf) == 10 * len(dates)
+        out = np.empty(max(len(dates), 1), np.int32)
+        f(buf, len(dates), _p(out))
+        return out[:len(dates)]
+
     def smj(self, inner_keys, outer_keys, buffer_size: int, threads: int = 1):
         """Reference sort-merge join on key columns (the outer size must equal
         the library's BUFFER_SIZE).  With one thread the result is exact:

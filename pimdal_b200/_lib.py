@@ -206,6 +206,7 @@ SIGNATURES = {
     "pimdal_hash_kernel": (_I, [_VP, C.POINTER(HashArguments), _VP]),
     "pimdal_hj_probe": (_I, [_VP, C.POINTER(ProbeArguments), _VP, _VP]),
     "pimdal_filter_kernel": (_I, [_VP, C.POINTER(FilterArguments), _VP]),
+    "pimdal_ingest": (_I, [_VP, _VP, _SZ, _VP, _VP]),
     "pimdal_select_join_aggregate": (_I, [_VP, C.POINTER(SelectJoinAggregateArguments), _VP, _VP]),
     "pimdal_match_kernel": (_I, [_VP, C.POINTER(MatchArguments), _VP, _VP]),
     "pimdal_hash_join_workspace_size": (_I, [C.POINTER(HashJoinArguments), C.POINTER(_SZ)]),

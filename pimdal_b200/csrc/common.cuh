@@ -65,6 +65,9 @@ struct pimdal_ctx {
   double prof_ms[PIMDAL_KERNEL_COUNT] = {};
   // batch autotuner: best tuning per batch shape
   std::map<std::vector<uint64_t>, pimdal_batch_tuning_t> tune_cache;
+  // pimdal_ingest: two pinned staging buffers and the events of their copies
+  void *stage[2] = {nullptr, nullptr};
+  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
 };
 
 // Brackets one launch with timing events when profiling is on.

@@ -114,6 +114,13 @@ extern "C" int pimdal_ctx_destroy(pimdal_ctx_t *ctx) {
   cudaSetDevice(ctx->device);
   prof_drain(ctx);
   for (cudaEvent_t e : ctx->prof_free) cudaEventDestroy(e);
+  for (int i = 0; i < 2; ++i) {
+    if (ctx->stage_ev[i]) {
+      cudaEventSynchronize(ctx->stage_ev[i]);
+      cudaEventDestroy(ctx->stage_ev[i]);
+    }
+    if (ctx->stage[i]) cudaFreeHost(ctx->stage[i]);
+  }
   if (ctx->ws_owned) cudaFree(ctx->ws);
   cudaFree(ctx->d_error);
   cudaFree(ctx->d_status);

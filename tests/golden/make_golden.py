@@ -7,7 +7,7 @@ the oracle (tests/test_oracle.py) on machines without the reference checkout.
 
     make -C oracle ref && python tests/golden/make_golden.py [fixture ...]
 
-With names (select sort hash_join group_by smj bloom), only those fixtures
+With names (select sort hash_join group_by smj bloom dates), only those fixtures
 are rewritten.
 """
 from __future__ import annotations
@@ -60,12 +60,23 @@ def bloom(ref) -> None:
     np.savez_compressed(OUT / "bloom.npz", **b)
 
 
+def dates(ref) -> None:
+    """Packed dates from the reference reader's date_to_int
+    (pimdal/main/tpc_h/reader/read_table.cpp:8-16) over 1992-1998 and edges."""
+    days = uni(5000, 0, 2556, 110)
+    d = (np.datetime64("1992-01-01") + days.astype("timedelta64[D]")).astype(str).tolist()
+    d += ["1970-01-01", "1900-01-01", "1999-12-31", "2000-02-29", "2024-02-29", "2099-12-31"]
+    np.savez_compressed(OUT / "dates.npz", dates=np.array(d), packed=ref.date_to_int(d))
+
+
 def main(only: list[str]) -> None:
     want = lambda name: not only or name in only
     ref = oracle.Ref()
     if want("bloom"):
         bloom(ref)
-    if only and only == ["bloom"]:
+    if want("dates"):
+        dates(ref)
+    if only and set(only) <= {"bloom", "dates"}:
         print("golden fixtures written to", OUT)
         return
     for name in ("select", "sort", "hash_join", "aggregate", "smj_64000"):
