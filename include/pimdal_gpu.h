@@ -296,12 +296,13 @@ int pimdal_sort_merge_join(pimdal_ctx_t *ctx, const pimdal_smj_arguments_t *args
 /* Arrow buffers to the DPUs (populate_mram / dist_table,                     */
 /* pimdal/support/transfer_helper.h, after the parquet read of                */
 /* pimdal/main/tpc_h/reader/read_table.cpp:18-34): copies bytes from host     */
-/* memory to dst on the stream.  A pageable source goes through two pinned    */
+/* memory to dst on the stream.  A pageable source is copied chunk by chunk  */
+/* by several host threads (PIMDAL_INGEST_THREADS, default 8) into pinned     */
 /* staging buffers of PIMDAL_INGEST_CHUNK bytes owned by the context (made by */
-/* the first call), so the host copy of one chunk overlaps the transfer of   */
-/* the previous one; a pinned (page-locked or registered) source is copied    */
-/* directly.  On return the source may be reused: every host read is done;   */
-/* the device copy completes in stream order.                                */
+/* the first call that needs them), so host copies overlap each other and the */
+/* transfers; a pinned (page-locked or registered) source is copied directly. */
+/* On return the source may be reused: every host read is done; the device   */
+/* copy completes in stream order.                                           */
 /* ------------------------------------------------------------------------- */
 #define PIMDAL_INGEST_CHUNK (16u << 20)
 int pimdal_ingest(pimdal_ctx_t *ctx, const void *host_src, size_t bytes, void *dst,

@@ -44,6 +44,8 @@ struct pd_prof_rec {
   cudaEvent_t start, stop;
 };
 
+constexpr int PD_INGEST_MAX_THREADS = 16;  // host copy threads of pimdal_ingest
+
 struct pimdal_ctx {
   int device = 0;
   int sm_count = 148;
@@ -65,9 +67,10 @@ struct pimdal_ctx {
   double prof_ms[PIMDAL_KERNEL_COUNT] = {};
   // batch autotuner: best tuning per batch shape
   std::map<std::vector<uint64_t>, pimdal_batch_tuning_t> tune_cache;
-  // pimdal_ingest: two pinned staging buffers and the events of their copies
-  void *stage[2] = {nullptr, nullptr};
-  cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+  // pimdal_ingest: pinned staging buffers (one per host copy thread) and the
+  // events of their last transfers
+  void *stage[PD_INGEST_MAX_THREADS] = {};
+  cudaEvent_t stage_ev[PD_INGEST_MAX_THREADS] = {};
 };
 
 // Brackets one launch with timing events when profiling is on.

@@ -114,7 +114,7 @@ extern "C" int pimdal_ctx_destroy(pimdal_ctx_t *ctx) {
   cudaSetDevice(ctx->device);
   prof_drain(ctx);
   for (cudaEvent_t e : ctx->prof_free) cudaEventDestroy(e);
-  for (int i = 0; i < 2; ++i) {
+  for (int i = 0; i < PD_INGEST_MAX_THREADS; ++i) {
     if (ctx->stage_ev[i]) {
       cudaEventSynchronize(ctx->stage_ev[i]);
       cudaEventDestroy(ctx->stage_ev[i]);

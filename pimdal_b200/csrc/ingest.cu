@@ -6,12 +6,19 @@
 // over the DPUs' MRAM (populate_mram / dist_table,
 // pimdal/support/transfer_helper.h).  Here a column goes to one GPU's HBM.
 // A DMA from pageable memory cannot overlap the host: the driver stages it
-// through its own buffers and the call blocks.  So a pageable source is
-// copied chunk by chunk into two pinned buffers in turn; each chunk's
-// transfer is queued on the stream and overlaps the host copy of the next,
-// and a buffer is refilled only after the event of its last transfer.
+// through its own buffers, one host thread at a time.  So a pageable source
+// is split into chunks that PIMDAL_INGEST_THREADS host threads copy into
+// their own pinned buffers; each chunk's transfer is queued on the stream
+// and overlaps the host copies of the next chunks, and a buffer is refilled
+// only after the event of its previous transfer.  The chunks land in
+// disjoint parts of the destination, so their order on the stream does not
+// matter, and all of them are queued before the call returns.
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
 #include <cstring>
+#include <thread>
+#include <vector>
 
 #include "common.cuh"
 
@@ -26,6 +33,16 @@ bool host_pinned(const void *p) {
   return at.type == cudaMemoryTypeHost;
 }
 
+int ingest_threads() {
+  static int t = 0;
+  if (!t) {
+    const char *e = std::getenv("PIMDAL_INGEST_THREADS");
+    t = e ? std::atoi(e) : 8;
+    t = std::max(1, std::min(t, PD_INGEST_MAX_THREADS));
+  }
+  return t;
+}
+
 }  // namespace
 
 extern "C" int pimdal_ingest(pimdal_ctx_t *ctx, const void *host_src, size_t bytes, void *dst,
@@ -38,7 +55,9 @@ extern "C" int pimdal_ingest(pimdal_ctx_t *ctx, const void *host_src, size_t byt
     PD_CHECK_CUDA(cudaMemcpyAsync(dst, host_src, bytes, cudaMemcpyHostToDevice, s));
     return PIMDAL_OK;
   }
-  for (int i = 0; i < 2; ++i) {
+  const size_t chunks = (bytes + PIMDAL_INGEST_CHUNK - 1) / PIMDAL_INGEST_CHUNK;
+  const int nt = (int)std::min<size_t>(ingest_threads(), chunks);
+  for (int i = 0; i < nt; ++i) {
     if (!ctx->stage[i] && cudaHostAlloc(&ctx->stage[i], PIMDAL_INGEST_CHUNK, cudaHostAllocDefault) != cudaSuccess) {
       ctx->stage[i] = nullptr;
       return PIMDAL_ERR_OOM;
@@ -47,13 +66,31 @@ extern "C" int pimdal_ingest(pimdal_ctx_t *ctx, const void *host_src, size_t byt
   }
   const char *src = (const char *)host_src;
   char *d = (char *)dst;
-  int b = 0;
-  for (size_t off = 0; off < bytes; off += PIMDAL_INGEST_CHUNK, b ^= 1) {
-    const size_t n = std::min<size_t>(PIMDAL_INGEST_CHUNK, bytes - off);
-    PD_CHECK_CUDA(cudaEventSynchronize(ctx->stage_ev[b]));  // its previous transfer is done
-    std::memcpy(ctx->stage[b], src + off, n);
-    PD_CHECK_CUDA(cudaMemcpyAsync(d + off, ctx->stage[b], n, cudaMemcpyHostToDevice, s));
-    PD_CHECK_CUDA(cudaEventRecord(ctx->stage_ev[b], s));
+  std::atomic<int> status{PIMDAL_OK};
+  // Worker w copies chunks w, w + nt, ... through staging buffer w.
+  auto work = [&](int w) {
+    cudaSetDevice(ctx->device);
+    for (size_t c = w; c < chunks && status.load() == PIMDAL_OK; c += nt) {
+      const size_t off = c * PIMDAL_INGEST_CHUNK;
+      const size_t n = std::min<size_t>(PIMDAL_INGEST_CHUNK, bytes - off);
+      if (cudaEventSynchronize(ctx->stage_ev[w]) != cudaSuccess) {  // its previous transfer is done
+        status = PIMDAL_ERR_CUDA;
+        return;
+      }
+      std::memcpy(ctx->stage[w], src + off, n);
+      if (cudaMemcpyAsync(d + off, ctx->stage[w], n, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+          cudaEventRecord(ctx->stage_ev[w], s) != cudaSuccess) {
+        status = PIMDAL_ERR_CUDA;
+        return;
+      }
+    }
+  };
+  if (nt == 1) {
+    work(0);
+  } else {
+    std::vector<std::thread> pool;
+    for (int w = 0; w < nt; ++w) pool.emplace_back(work, w);
+    for (auto &t : pool) t.join();
   }
-  return PIMDAL_OK;
+  return status.load();
 }
