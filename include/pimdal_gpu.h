@@ -409,6 +409,8 @@ int pimdal_hash_join(pimdal_ctx_t *ctx, const pimdal_hash_join_arguments_t *args
 /* partition, in input order.  match_sizes[0] = 0 and match_sizes[p+1] = kept */
 /* rows of partition p (uint64, device); t_count = all kept rows.  Rows that  */
 /* lie in no partition are not kept.  part_sizes must be non-decreasing.      */
+/* pimdal_match_kernel takes 8 bytes per 2048 input rows of the context's     */
+/* workspace.                                                                */
 /* ------------------------------------------------------------------------- */
 #define PIMDAL_FILTER_BITS 16384
 #define PIMDAL_FILTER_BYTES (PIMDAL_FILTER_BITS / 8)

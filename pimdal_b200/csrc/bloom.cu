@@ -18,8 +18,9 @@
 //    each row's bits into the global filters directly.  The partitions of a
 //    tile's first and last row are found by two warps, 32 offsets per round.
 //  * k_match: persistent CTAs claim 2048-row tiles in order (8 warp-striped
-//    keys per thread, loads issued together, before the tile's partition
-//    search).  A tile spanning at most 8 partitions stages their filters and
+//    keys per thread, loads issued together).  A pre-pass finds every
+//    tile's first and last partition in parallel; a tile reads its pair when
+//    it is claimed.  A tile spanning at most 8 partitions stages their filters and
 //    first rows in shared memory and counts its kept rows per partition
 //    there; otherwise each row finds its partition by binary search and
 //    reads its filter through L1.  Kept rows are ranked with ballots and a
@@ -38,6 +39,9 @@ constexpr int BF_THREADS = 256;
 constexpr int BF_WARPS = BF_THREADS / 32;
 #ifndef PD_BF_ITEMS
 #define PD_BF_ITEMS 8  // rows per thread of a match / filter tile (measured best with 6 CTAs per SM)
+#endif
+#ifndef PD_BF_RANGES
+#define PD_BF_RANGES 1  // 1: tile partition ranges from a pre-pass (0: searched by each tile)
 #endif
 #ifndef PD_BF_MATCH_CTAS
 #define PD_BF_MATCH_CTAS 6  // match CTAs per SM the kernel is compiled for
@@ -192,7 +196,17 @@ struct MatchParams {
   uint32_t *claim;
   uint32_t *d_error;
   uint64_t *d_count;
+  const int2 *ranges;  // per tile: partitions of its first and last row
 };
+
+// Pre-pass of k_match: the partitions of every tile's first and last row,
+// one thread per tile, all tiles in parallel.
+__global__ void __launch_bounds__(256) k_match_ranges(MatchParams p, int2 *ranges) {
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= p.tiles) return;
+  const uint64_t a = t * BF_TILE, b = min(a + (uint64_t)BF_TILE, p.n) - 1;
+  ranges[t] = make_int2((int)part_of(p.ps, 0, p.part_n, a), (int)part_of(p.ps, 0, p.part_n, b));
+}
 
 __global__ void __launch_bounds__(BF_THREADS, BF_MATCH_CTAS) k_match(MatchParams p) {
   __shared__ __align__(16) uint32_t s_f[BF_SMEM_PARTS * BF_WORDS];  // the tile's filters
@@ -212,6 +226,13 @@ __global__ void __launch_bounds__(BF_THREADS, BF_MATCH_CTAS) k_match(MatchParams
         p.claim[1] = 0;
       }
       s_tile = t;
+#if PD_BF_RANGES
+      if (t < p.tiles) {
+        const int2 rg = p.ranges[t];
+        s_pa = rg.x;
+        s_pb = rg.y;
+      }
+#endif
     }
     __syncthreads();
     const uint32_t tile = s_tile;
@@ -230,9 +251,11 @@ __global__ void __launch_bounds__(BF_THREADS, BF_MATCH_CTAS) k_match(MatchParams
         key[k] = p.pairs ? reinterpret_cast<const uint2 *>(p.key)[r].x
                          : reinterpret_cast<const uint32_t *>(p.key)[r];
     }
+#if !PD_BF_RANGES
     const uint32_t last = (uint32_t)(min((uint64_t)tile * BF_TILE + BF_TILE, p.n) - 1);
     tile_parts(p.ps, p.part_n, tile * BF_TILE, last, &s_pa, &s_pb);
     __syncthreads();
+#endif
     const int64_t pa = s_pa, pb = s_pb, np = pb - pa + 1;
     const bool local = pa >= 0 && pb < (int64_t)p.part_n && np <= BF_SMEM_PARTS;
     if (local) {
@@ -393,6 +416,7 @@ extern "C" int pimdal_match_kernel(pimdal_ctx_t *ctx, const pimdal_match_argumen
   if (((uintptr_t)a->filter_ptr & 15u) || !layout_ok(a->layout) || a->size >= (1ull << 32))
     return PIMDAL_ERR_ARG;
   if ((a->size && !a->part_ptr) || (a->out_capacity && !a->out_ptr)) return PIMDAL_ERR_ARG;
+  if (a->part_n >= (1u << 31)) return PIMDAL_ERR_ARG;  // partition indices are int32 here
   cudaStream_t s = (cudaStream_t)stream;
   cudaSetDevice(ctx->device);
   PD_CHECK_CUDA(cudaMemsetAsync(a->match_sizes, 0, sizeof(uint64_t) * ((size_t)a->part_n + 1), s));
@@ -420,6 +444,15 @@ extern "C" int pimdal_match_kernel(pimdal_ctx_t *ctx, const pimdal_match_argumen
   p.claim = ctx->d_counters + PD_COUNTER_MATCH;
   p.d_error = ctx->d_error;
   p.d_count = &d_result->t_count;
+#if PD_BF_RANGES
+  int2 *ranges = (int2 *)pd_workspace(ctx, sizeof(int2) * tiles, s, &st);
+  if (!ranges) return st;
+  p.ranges = ranges;
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_MATCH, s);
+    k_match_ranges<<<(unsigned)pd_ceil_div(tiles, 256), 256, 0, s>>>(p, ranges);
+  }
+#endif
   p.epoch = pd_next_epoch(ctx, s, &st);
   if (st) return st;
   {
