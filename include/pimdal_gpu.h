@@ -442,6 +442,7 @@ typedef struct {
 
 int pimdal_filter_kernel(pimdal_ctx_t *ctx, const pimdal_filter_arguments_t *args,
                          pimdal_stream_t stream);
+int pimdal_match_workspace_size(const pimdal_match_arguments_t *args, size_t *bytes);
 int pimdal_match_kernel(pimdal_ctx_t *ctx, const pimdal_match_arguments_t *args,
                         pimdal_merge_results_t *d_result, pimdal_stream_t stream);
 
@@ -547,6 +548,8 @@ typedef struct {
   uint64_t out_capacity;
 } pimdal_select_join_aggregate_arguments_t;
 
+int pimdal_select_join_aggregate_workspace_size(
+    const pimdal_select_join_aggregate_arguments_t *args, size_t *bytes);
 int pimdal_select_join_aggregate(pimdal_ctx_t *ctx,
                                  const pimdal_select_join_aggregate_arguments_t *args,
                                  pimdal_aggr_results_t *d_result, pimdal_stream_t stream);

@@ -208,6 +208,9 @@ SIGNATURES = {
     "pimdal_filter_kernel": (_I, [_VP, C.POINTER(FilterArguments), _VP]),
     "pimdal_ingest": (_I, [_VP, _VP, _SZ, _VP, _VP]),
     "pimdal_select_join_aggregate": (_I, [_VP, C.POINTER(SelectJoinAggregateArguments), _VP, _VP]),
+    "pimdal_select_join_aggregate_workspace_size": (_I, [C.POINTER(SelectJoinAggregateArguments),
+                                                        C.POINTER(_SZ)]),
+    "pimdal_match_workspace_size": (_I, [C.POINTER(MatchArguments), C.POINTER(_SZ)]),
     "pimdal_match_kernel": (_I, [_VP, C.POINTER(MatchArguments), _VP, _VP]),
     "pimdal_hash_join_workspace_size": (_I, [C.POINTER(HashJoinArguments), C.POINTER(_SZ)]),
     "pimdal_hash_join": (_I, [_VP, C.POINTER(HashJoinArguments), _VP, _VP]),

@@ -409,6 +409,12 @@ extern "C" int pimdal_filter_kernel(pimdal_ctx_t *ctx, const pimdal_filter_argum
   return pd_launch_status(ctx);
 }
 
+extern "C" int pimdal_match_workspace_size(const pimdal_match_arguments_t *a, size_t *bytes) {
+  if (!a || !bytes) return PIMDAL_ERR_ARG;
+  *bytes = PD_BF_RANGES ? sizeof(int2) * pd_ceil_div(a->size, BF_TILE) : 0;
+  return PIMDAL_OK;
+}
+
 extern "C" int pimdal_match_kernel(pimdal_ctx_t *ctx, const pimdal_match_arguments_t *a,
                                    pimdal_merge_results_t *d_result, pimdal_stream_t stream) {
   if (!ctx || !a || !d_result || !a->filter_ptr || !a->match_sizes || !a->part_sizes || a->part_n == 0)

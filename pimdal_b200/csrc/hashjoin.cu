@@ -1121,6 +1121,13 @@ __global__ void __launch_bounds__(1024) k_sja_emit(const unsigned long long *g_s
 
 }  // namespace
 
+extern "C" int pimdal_select_join_aggregate_workspace_size(
+    const pimdal_select_join_aggregate_arguments_t *a, size_t *bytes) {
+  if (!a || !bytes || a->key_space == 0 || a->key_space > PIMDAL_FUSED_MAX_KEYS) return PIMDAL_ERR_ARG;
+  *bytes = 16ull * a->key_space;
+  return PIMDAL_OK;
+}
+
 extern "C" int pimdal_select_join_aggregate(pimdal_ctx_t *ctx,
                                             const pimdal_select_join_aggregate_arguments_t *a,
                                             pimdal_aggr_results_t *d_result, pimdal_stream_t stream) {

@@ -60,3 +60,22 @@ def test_batch_argument_errors_need_no_gpu():
     assert lib.pimdal_batch_device_bytes(None, ctypes.byref(sz)) == 1
     best = L.BatchTuning()
     assert lib.pimdal_batch_autotune(None, 0, None, 0, None, ctypes.byref(best), None, None) == 1
+
+
+def test_prefilter_fused_and_ingest_argument_errors_need_no_gpu():
+    lib = L.lib()
+    fa, ma = L.FilterArguments(), L.MatchArguments()
+    sa = L.SelectJoinAggregateArguments()
+    assert lib.pimdal_filter_kernel(None, ctypes.byref(fa), None) == 1
+    assert lib.pimdal_match_kernel(None, ctypes.byref(ma), None, None) == 1
+    assert lib.pimdal_select_join_aggregate(None, ctypes.byref(sa), None, None) == 1
+    assert lib.pimdal_ingest(None, None, 16, None, None) == 1
+    sz = ctypes.c_size_t(7)
+    ma.size = 2048 * 10 + 1
+    assert lib.pimdal_match_workspace_size(ctypes.byref(ma), ctypes.byref(sz)) == 0
+    assert sz.value == 8 * 11  # one (first, last) partition pair per 2048-row tile
+    sa.key_space = 50
+    assert lib.pimdal_select_join_aggregate_workspace_size(ctypes.byref(sa), ctypes.byref(sz)) == 0
+    assert sz.value == 16 * 50
+    sa.key_space = L.FUSED_MAX_KEYS + 1
+    assert lib.pimdal_select_join_aggregate_workspace_size(ctypes.byref(sa), ctypes.byref(sz)) == 1
