@@ -948,12 +948,20 @@ def dist_setup():
     return world, rank, local
 
 
+def _rank_tensor(x: float):
+    """x in a tensor on the device the process group reduces on (the GPU
+    under NCCL, the host under gloo)."""
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    return torch.tensor([x], dtype=torch.float64, device=dev)
+
+
 def reduce_max(x: float, world: int) -> float:
     if world == 1:
         return x
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = _rank_tensor(x)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -961,9 +969,8 @@ def reduce_max(x: float, world: int) -> float:
 def reduce_sum(x: float, world: int) -> float:
     if world == 1:
         return x
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = _rank_tensor(x)
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
