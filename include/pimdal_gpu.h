@@ -301,7 +301,9 @@ int pimdal_sort_merge_join(pimdal_ctx_t *ctx, const pimdal_smj_arguments_t *args
 /* staging buffers of PIMDAL_INGEST_CHUNK bytes owned by the context (made by */
 /* the first call that needs them), so host copies overlap each other and the */
 /* transfers; a pinned (page-locked or registered) source is copied directly. */
-/* On return the source may be reused: every host read is done; the device   */
+/* A pageable source may be reused on return (every host read is done); a    */
+/* pinned source is read by the transfer itself, so it must stay unchanged   */
+/* until the stream reaches the copy, as with cudaMemcpyAsync.  The device   */
 /* copy completes in stream order.                                           */
 /* ------------------------------------------------------------------------- */
 #define PIMDAL_INGEST_CHUNK (16u << 20)

@@ -12,7 +12,9 @@
 // and overlaps the host copies of the next chunks, and a buffer is refilled
 // only after the event of its previous transfer.  The chunks land in
 // disjoint parts of the destination, so their order on the stream does not
-// matter, and all of them are queued before the call returns.
+// matter, and all of them are queued before the call returns.  A pinned
+// source needs no staging: its transfer reads it directly, later, in stream
+// order.
 #include <algorithm>
 #include <atomic>
 #include <cstdlib>

@@ -66,7 +66,9 @@ def date_to_int(col) -> np.ndarray:
 
 def ingest(ctx: ops.Context, host: np.ndarray, out: torch.Tensor, stream=None) -> torch.Tensor:
     """Copies a contiguous host array into a device tensor of the same size
-    in bytes (pimdal_ingest); the host array may be reused on return."""
+    in bytes (pimdal_ingest).  A pageable array may be reused on return; a
+    pinned one is read by the transfer and must stay unchanged until the
+    stream has reached the copy."""
     host = np.ascontiguousarray(host)
     nbytes = host.nbytes
     assert out.is_cuda and out.numel() * out.element_size() == nbytes
