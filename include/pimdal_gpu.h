@@ -200,16 +200,20 @@ int pimdal_sel_kernel(pimdal_ctx_t *ctx, const pimdal_sel_arguments_t *args,
                       pimdal_sel_results_t *d_result, pimdal_stream_t stream);
 
 /* Selection that allocates nothing -- no counterpart in the reference.  For
- * callers that cannot call cudaMalloc (a host whose memory manager owns every
- * device allocation, code running during stream capture, latency-critical
- * paths): no context is needed, the caller passes only its own input, output
- * and result buffers.  Same arguments and results as pimdal_sel_kernel, on
- * the current device.  Scratch is a fixed 32 KiB device array inside the
- * library, so at most 2^29 rows per call with 16-byte-aligned input (2^24
- * otherwise); larger calls return PIMDAL_ERR_WORKSPACE.  The first call on a
- * device sets that array up (do it before any stream capture).  Calls share
- * the array: calls that overlap on the GPU race and must not be issued.  A
- * device-side failure sets d_result->t_count to UINT64_MAX. */
+ * callers that cannot call cudaMalloc: a host whose memory manager owns every
+ * device allocation (a database buffer pool, a framework's caching
+ * allocator), or a latency-critical path where an allocation could block on
+ * a device-wide synchronisation.  No context is needed: the caller passes
+ * only its own input, output and result buffers.  Same arguments and results
+ * as pimdal_sel_kernel, on the current device.  Scratch is a fixed 32 KiB
+ * device array inside the library (held by every GPU that loads the library
+ * until the process exits), so at most 2^29 rows per call with 16-byte-
+ * aligned input and row ids (2^24 otherwise); larger calls return
+ * PIMDAL_ERR_WORKSPACE before anything is launched.  The first call on a
+ * device looks up and clears that array; make that first call before any
+ * stream capture.  Every call shares the array: calls that overlap on the
+ * GPU race and must not be issued.  A device-side failure sets
+ * d_result->t_count to UINT64_MAX. */
 int pimdal_sel_kernel_noalloc(const pimdal_sel_arguments_t *args, pimdal_sel_results_t *d_result,
                               pimdal_stream_t stream);
 
@@ -507,8 +511,8 @@ typedef struct {
   const int64_t *price;        /* fact columns, indexed by fact row             */
   const int32_t *discount;     /* percent, 0..100                               */
   const uint8_t *flag;         /* second group column (NULL: none)              */
-  uint32_t attr_mult;          /* key = attr * attr_mult + flag[row]            */
-  uint32_t pad;
+  uint32_t attr_mult;          /* key = attr * attr_mult + flag[row] (uint32,   */
+  uint32_t pad;                /* wrapping)                                     */
   uint32_t *out_key;           /* group key per joined row                      */
   int64_t *out_val;            /* price * (100 - discount) per joined row       */
 } pimdal_revenue_arguments_t;
@@ -523,7 +527,8 @@ int pimdal_revenue_keys(pimdal_ctx_t *ctx, const pimdal_revenue_arguments_t *arg
 /* r < size takes part when date_lo <= date[r] <= date_hi; it is joined       */
 /* through a table built by pimdal_hash_kernel (every build row whose key is  */
 /* jkey[r] contributes, its payload being the attribute); the group key is    */
-/* attr * attr_mult + (flag ? flag[r] : 0) and the value                      */
+/* attr * attr_mult + (flag ? flag[r] : 0) in 32-bit arithmetic that wraps,   */
+/* exactly as pimdal_revenue_keys computes it, and the value                  */
 /* price[r] * (100 - discount[r]).  Output: the groups with at least one row, */
 /* ascending by key, with SUM (int64, wrapping) and COUNT -- exactly what     */
 /* selection + gather + pimdal_hj_probe + pimdal_revenue_keys +               */

@@ -1033,7 +1033,8 @@ __global__ void __launch_bounds__(SJA_THREADS) k_sja_aggregate(SjaParams p) {
     const uint32_t f = p.flag ? __ldg(p.flag + r) : 0u;
     const int64_t v = __ldg(p.price + r) * (int64_t)(100 - __ldg(p.discount + r));
     auto add = [&](uint32_t attr) {
-      const uint64_t g = (uint64_t)attr * p.attr_mult + f;
+      // the staged glue's key (k_revenue_keys): 32-bit, wrapping
+      const uint32_t g = attr * p.attr_mult + f;
       if (g >= ks) {
         bad = true;
         return;

@@ -234,6 +234,10 @@ __device__ __forceinline__ uint32_t block_reduce_sum_1024(uint32_t v, uint32_t *
   return t;
 }
 
+__device__ __forceinline__ bool sl_timed_out(const uint32_t *d_error) {
+  return (*(const volatile uint32_t *)d_error & PD_DEVERR_TIMEOUT) != 0;
+}
+
 template <int LAYOUT, bool SIGNED, bool HAS_PTR>
 __global__ void __launch_bounds__(SL_THREADS, 1) k_select_chunked(SlParams q) {
   extern __shared__ __align__(128) unsigned char s_ring[];
@@ -279,7 +283,8 @@ __global__ void __launch_bounds__(SL_THREADS, 1) k_select_chunked(SlParams q) {
     const uint32_t nst = (uint32_t)pd_ceil_div(bulk_bytes, SL_STAGE_BYTES);
 
     // ---- A: count through the bulk-copy ring ------------------------------
-    if (tid == 0) {
+    // After a wait anywhere in the launch gave up, no further copy is issued.
+    if (tid == 0 && !sl_timed_out(p.d_error)) {
       for (uint32_t j = 0; j < nst && j < (uint32_t)SL_STAGES; ++j) {
         uint32_t slot = issued % SL_STAGES;
         uint32_t b = (uint32_t)min((uint64_t)SL_STAGE_BYTES, bulk_bytes - (uint64_t)j * SL_STAGE_BYTES);
@@ -309,7 +314,7 @@ __global__ void __launch_bounds__(SL_THREADS, 1) k_select_chunked(SlParams q) {
         }
       }
       __syncthreads();
-      if (tid == 0 && j + SL_STAGES < nst) {
+      if (tid == 0 && j + SL_STAGES < nst && !sl_timed_out(p.d_error)) {
         const uint32_t jn = j + SL_STAGES;
         const uint32_t bn = (uint32_t)min((uint64_t)SL_STAGE_BYTES, bulk_bytes - (uint64_t)jn * SL_STAGE_BYTES);
         pd_fence_proxy_async_smem();
@@ -444,6 +449,22 @@ __global__ void __launch_bounds__(SL_THREADS, 1) k_select_chunked(SlParams q) {
       }
       out_base += tile_total;
       __syncthreads();
+    }
+  }
+  // Before the CTA exits, every bulk copy it issued must have landed: when a
+  // wait above gave up, a copy may still be writing into this CTA's shared
+  // memory.  Thread 0 (the only issuer) waits, bounded, for the last phase
+  // issued on each ring slot; on the normal path these phases are complete
+  // and each wait returns at once.
+  if (tid == 0) {
+    for (uint32_t slot = 0; slot < (uint32_t)SL_STAGES && slot < issued; ++slot) {
+      const uint32_t uses = (issued - slot + SL_STAGES - 1) / SL_STAGES;  // issues on this slot
+      const uint32_t parity = (uses - 1) & 1u;
+      uint32_t spins = 0;
+      const uint64_t t0 = pd_globaltimer_ns();
+      while (!pd_mbar_try_wait(&s_bar[slot], parity)) {
+        if (pd_wait_expired(p.d_error, t0, ++spins)) break;
+      }
     }
   }
 }
@@ -822,9 +843,10 @@ extern "C" int pimdal_sel_kernel(pimdal_ctx_t *ctx, const pimdal_sel_arguments_t
 //
 // Some hosts of this operator may not call cudaMalloc at all: code running
 // under a memory manager that owns every device allocation (a database
-// buffer pool or a framework's caching allocator), code called while a CUDA
-// graph is being captured, or a real-time path where an allocation could
-// block.  pimdal_sel_kernel needs a pimdal_ctx, and creating one allocates.
+// buffer pool or a framework's caching allocator, which would see a foreign
+// allocation as lost memory), or a real-time path where an allocation could
+// block on a device-wide synchronisation.  pimdal_sel_kernel needs a
+// pimdal_ctx, and creating one allocates.
 // This entry point needs nothing but the caller's input, output and result
 // buffers: its scratch (look-back status words, the chunk claim counters and
 // an error word) is the file-scope device array below, which every GPU that
@@ -904,7 +926,9 @@ extern "C" int pimdal_sel_kernel_noalloc(const pimdal_sel_arguments_t *a,
   std::lock_guard<std::mutex> lock(g_sel_na_mutex);
   SelNaDevice &d = g_sel_na[dev];
   if (!d.ready) {
-    // One-time set-up on this device (must not run inside stream capture).
+    // One-time set-up on this device: the array's device address, and the
+    // array cleared on the caller's stream (make this first call before any
+    // stream capture).
     void *addr = nullptr;
     if (cudaGetSymbolAddress(&addr, g_sel_noalloc_scratch) != cudaSuccess || !addr) {
       cudaGetLastError();

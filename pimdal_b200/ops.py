@@ -63,6 +63,10 @@ class Context:
             L.check(self.lib.pimdal_ctx_set_workspace(self.handle, self._ws.data_ptr(), size),
                     "pimdal_ctx_set_workspace")
 
+    def workspace_bytes(self) -> int:
+        """Bytes of the workspace this context holds."""
+        return 0 if self._ws is None else self._ws.numel()
+
     def sync(self, stream=None) -> None:
         """Waits for the stream and raises if a kernel reported a device error."""
         L.check(self.lib.pimdal_ctx_sync_status(self.handle, _stream(stream)),

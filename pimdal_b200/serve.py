@@ -23,11 +23,17 @@ the next stage starts when they arrive.
 
 Scheduling (continuous batching): requests arrive (Poisson); an arrived
 request is admitted as soon as a slot is free and its working-set bytes fit
-the HBM byte budget left after the resident tables; admitted requests run
-concurrently, their stages interleaving on the device.  Served runs use the
-fused pass by default; serial plain execution is the same loop with one
-slot, one request at a time, through the staged plain operators.  The
-reference runs one query at a time on the DPUs (pimdal/main/tpc_h/*/host).
+the HBM byte budget left after the resident tables and the slots' fixed
+memory; admitted requests run concurrently, their stages interleaving on the
+device.  The charge is what the request really holds on the device while it
+runs: a staged request allocates its per-row buffers (selected row ids and
+values, join keys, matches, group keys and values: 32 bytes per range row)
+in one allocation when it starts and frees it when it ends; a fused request
+allocates nothing per row and is charged its group table (16 bytes per key
+of its key space) and its outputs.  Served runs use the fused pass by
+default; serial plain execution is the same loop with one slot, one request
+at a time, through the staged plain operators.  The reference runs one query
+at a time on the DPUs (pimdal/main/tpc_h/*/host).
 """
 from __future__ import annotations
 
@@ -47,8 +53,7 @@ N_PRIO = 5
 N_RFLAG = 3
 N_CAT = 25
 N_LSTATUS = 2
-ROW_BYTES = 40          # working-set bytes per range row (selection, join, group-by buffers)
-FIXED_BYTES = 1 << 20   # per request on top
+STAGED_ROW_BYTES = 32   # staged buffers per range row: 6 x int32 + 1 x int64
 
 
 @dataclass
@@ -62,9 +67,16 @@ class Request:
     dim: int        # 0: orders (group by priority), 1: part (group by category)
     two_keys: bool  # also group by the fact's flag column
 
-    @property
-    def need_bytes(self) -> int:
-        return ROW_BYTES * self.n + FIXED_BYTES
+    def key_space(self) -> int:
+        """Group keys of the request: dimension attribute (x flag values)."""
+        attrs = N_PRIO if self.dim == 0 else N_CAT
+        return attrs * ((N_RFLAG if self.dim == 0 else N_LSTATUS) if self.two_keys else 1)
+
+    def need_bytes(self, fused: bool) -> int:
+        """Device bytes the request holds while it runs."""
+        if fused:  # the fused pass's group table (16 B per key) and nothing per row
+            return 16 * self.key_space()
+        return STAGED_ROW_BYTES * self.n
 
 
 @dataclass
@@ -154,20 +166,18 @@ def make_requests(count: int, fact_rows: int, rate: float | None, seed: int = 0x
 
 
 class Slot:
-    """One concurrency slot: a CUDA stream, a library context and buffers for
-    the largest request."""
+    """One concurrency slot: a CUDA stream, a library context, the outputs of
+    one request, and (while a staged request runs) its per-row buffers."""
 
     MAX_GROUPS = N_CAT * N_LSTATUS + N_PRIO * N_RFLAG
 
     def __init__(self, device: int, max_rows: int):
         dev = f"cuda:{device}"
+        self.dev = dev
         self.ctx = ops.Context(device)
         self.stream = torch.cuda.Stream(device=dev)
-        m = max(max_rows, 1)
+        self.buf = None
         e32 = lambda k: torch.empty(k, dtype=torch.int32, device=dev)
-        self.sel_val, self.sel_row = e32(m), e32(m)
-        self.jkey, self.mrow, self.mattr, self.gkey = e32(m), e32(m), e32(m), e32(m)
-        self.gval = torch.empty(m, dtype=torch.int64, device=dev)
         g = self.MAX_GROUPS
         self.outs = {"key": e32(g), "sum": torch.empty(g, dtype=torch.int64, device=dev),
                      "count": torch.empty(g, dtype=torch.int64, device=dev)}
@@ -190,6 +200,15 @@ class Slot:
         self.req, self.stage = req, 0
         self.result = Result(np.zeros(0, np.int32), np.zeros(0, np.int64), np.zeros(0, np.int64),
                              start=now)
+        if not self.fused:
+            # one allocation of exactly the charged bytes, on the slot's stream
+            m = max(req.n, 1)
+            with torch.cuda.stream(self.stream):
+                self.buf = torch.empty(8 * m, dtype=torch.int32, device=self.dev)
+            b = self.buf
+            self.sel_val, self.sel_row, self.jkey = b[0:m], b[m:2 * m], b[2 * m:3 * m]
+            self.mrow, self.mattr, self.gkey = b[3 * m:4 * m], b[4 * m:5 * m], b[5 * m:6 * m]
+            self.gval = b[6 * m:8 * m].view(torch.int64)
         self._launch(tables)
 
     def _launch(self, t: Tables) -> None:
@@ -257,6 +276,9 @@ class Slot:
 
     def _finish(self, now: float, groups: int) -> bool:
         self.ctx.sync(self.stream)  # raises on any device-side error of this request
+        # the stream has passed every use of the staged buffers: release them
+        self.buf = self.sel_val = self.sel_row = self.jkey = None
+        self.mrow = self.mattr = self.gkey = self.gval = None
         r = self.result
         r.keys = self.h_key[:groups].numpy().copy()
         r.sums = self.h_sum[:groups].numpy().copy()
@@ -309,7 +331,13 @@ class Server:
         self.tables = tables
         self.max_rows = min(tables.n, 60_000_000)
         self.slots = [Slot(device, self.max_rows) for _ in range(slots)]
+        self.hbm_budget = hbm_budget_bytes
         self.budget = max(0, hbm_budget_bytes - tables.resident_bytes)
+
+    def fixed_bytes(self) -> int:
+        """Device bytes the slots hold between requests: their contexts'
+        workspaces (grown by the first requests) and output buffers."""
+        return sum(sl.ctx.workspace_bytes() + 1024 for sl in self.slots)
 
     def close(self):
         for s in self.slots:
@@ -317,7 +345,8 @@ class Server:
 
     def warm(self) -> None:
         """A large request of each dimension through every slot, staged and
-        fused (workspaces)."""
+        fused: the contexts' workspaces reach their size; the budget left for
+        requests is what the tables and the slots do not hold."""
         rs = [Request(0, 0.0, 0, self.max_rows, 0, DAYS - 1, d, True) for d in (0, 1)]
         for s in self.slots:
             for fused in (False, True):
@@ -326,6 +355,7 @@ class Server:
                     s.start(self.tables, r, 0.0)
                     while not s.poll(self.tables, 0.0):
                         pass
+        self.budget = max(0, self.hbm_budget - self.tables.resident_bytes - self.fixed_bytes())
 
     def run(self, requests: list[Request], serial: bool = False,
             fused: bool | None = None) -> RunStats:
@@ -340,6 +370,7 @@ class Server:
         queue: deque[Request] = deque()
         free = list(slots)
         busy: list[Slot] = []
+        charged: dict[int, int] = {}
         st = RunStats()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -348,10 +379,13 @@ class Server:
             now = time.perf_counter() - t0
             while pending and pending[0].arrival <= now:
                 queue.append(pending.popleft())
-            while queue and free and adm.fits(queue[0].need_bytes) and not (serial and busy):
+            while (queue and free and adm.fits(queue[0].need_bytes(free[-1].fused))
+                   and not (serial and busy)):
                 r = queue.popleft()
                 s = free.pop()
-                adm.take(r.need_bytes)
+                r_need = r.need_bytes(s.fused)
+                charged[r.rid] = r_need
+                adm.take(r_need)
                 s.start(self.tables, r, now)
                 busy.append(s)
                 st.max_inflight = max(st.max_inflight, len(busy))
@@ -363,7 +397,7 @@ class Server:
                     st.results[r.rid] = s.result
                     st.latencies.append(now - r.arrival)
                     st.rows += r.n
-                    adm.give(r.need_bytes)
+                    adm.give(charged.pop(r.rid))
                     busy.remove(s)
                     free.append(s)
             if not busy and not queue and pending:

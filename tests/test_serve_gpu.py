@@ -62,18 +62,28 @@ def test_served_equals_serial_and_numpy(server):
         assert np.array_equal(got.counts, c), r.rid
 
 
-def test_budget_admits_one_request_at_a_time(server):
+@pytest.mark.parametrize("fused", [True, False])
+def test_budget_admits_one_request_at_a_time(server, fused):
+    """A budget with room for the smallest request alone admits one request
+    at a time; the charge is the request's real device bytes (the fused
+    pass's group table, or the staged pass's per-row buffers)."""
     t = server.tables
     reqs = serve.make_requests(12, t.n, rate=None, seed=22, min_rows=50_000, max_rows=t.n)
+    need = [r.need_bytes(fused) for r in reqs]
+    if fused:
+        assert max(need) <= 16 * serve.N_CAT * serve.N_LSTATUS
+    else:
+        assert need == [serve.STAGED_ROW_BYTES * r.n for r in reqs]
     free = server.budget
-    server.budget = min(r.need_bytes for r in reqs)  # room for exactly one request
+    server.budget = min(need)  # room for exactly one request
     try:
-        tight = server.run(reqs)
+        tight = server.run(reqs, fused=fused)
     finally:
         server.budget = free
     assert tight.max_inflight == 1
-    assert tight.max_reserved <= max(r.need_bytes for r in reqs)
-    loose = server.run(reqs)
+    assert tight.max_reserved <= max(need)
+    loose = server.run(reqs, fused=fused)
+    assert loose.max_inflight > 1
     assert serve.same_results(tight, loose)
 
 
@@ -152,3 +162,58 @@ def test_fused_operator_edges(ctx):
     with pytest.raises(L.PimdalError) as e:
         ctx.sync()
     assert e.value.status == 7 and int(res.item()) == 7
+
+
+def test_fused_and_staged_agree_on_the_all_ones_build_row(ctx):
+    """A build row whose key and payload are both 0xFFFFFFFF is the one row
+    the table counts on the side (its slot word would equal the empty word).
+    The fused pass and the staged operators (probe, then pimdal_revenue_keys,
+    then the group-by) compute the same 32-bit wrapping group key for it:
+    with attr_mult 1 and flag 1 the attribute 0xFFFFFFFF wraps to key 0."""
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    bkey = np.array([0xFFFFFFFF, 0xFFFFFFFF, 7, 9], np.uint32)
+    battr = np.array([0xFFFFFFFF, 2, 1, 0xFFFFFFFF], np.uint32)
+    table = ops.hash_kernel(ctx, d(bkey.view(np.int32)), d(battr.view(np.int32)), table_size=64)
+    n = 64
+    jkey = np.array([0xFFFFFFFF, 7, 9, 3] * (n // 4), np.uint32)
+    date = np.arange(n, dtype=np.int32)
+    price = (np.arange(n, dtype=np.int64) + 1) * 1000
+    disc = (np.arange(n) % 11).astype(np.int32)
+    flag = np.ones(n, np.uint8)
+    lo, hi = 3, 50
+    res, outs = ops.select_join_aggregate(
+        ctx, d(date), lo, hi, d(jkey.view(np.int32)), table, 64, d(price), d(disc),
+        flag=d(flag), attr_mult=1, key_space=8)
+    ctx.sync()
+    g = int(res.item())
+    fused = tuple(outs[c][:g].cpu().numpy() for c in ("key", "sum", "count"))
+    # staged: selected rows -> join-key gather -> probe -> revenue keys -> group-by
+    sel = np.flatnonzero((date >= lo) & (date <= hi)).astype(np.int32)
+    jk_sel = d(jkey[sel].view(np.int32))
+    pres, prow, pay = ops.hj_probe(ctx, table, 64, jk_sel)  # probe row = index into sel
+    ctx.sync()
+    m = int(pres.item())
+    kt = torch.empty(m, dtype=torch.int32, device="cuda")
+    vt = torch.empty(m, dtype=torch.int64, device="cuda")
+    ops.revenue_keys(ctx, m, prow, pay, d(sel), d(price), d(disc), d(flag), 1, kt, vt)
+    gres, gouts = ops.group_kernel(ctx, kt, vt, key_dtype=L.U32, method=L.GROUP_HASH,
+                                   expected_groups=16)
+    ctx.sync()
+    gg = int(gres.item())
+    staged = (gouts["key"][:gg].cpu().numpy(), gouts["sum"][:gg].cpu().numpy(),
+              gouts["count"][:gg].cpu().numpy())
+    # numpy restatement: every (selected row, matching build row) pair
+    keys, vals = [], []
+    for r in sel:
+        for b in range(bkey.size):
+            if bkey[b] == jkey[r]:
+                keys.append((int(battr[b]) * 1 + 1) & 0xFFFFFFFF)
+                vals.append(int(price[r]) * (100 - int(disc[r])))
+    uk, inv = np.unique(np.asarray(keys, np.int64), return_inverse=True)
+    sums = np.zeros(uk.size, np.int64)
+    np.add.at(sums, inv, np.asarray(vals, np.int64))
+    cnts = np.bincount(inv, minlength=uk.size)
+    assert g == gg == uk.size
+    assert np.array_equal(fused[0].view(np.uint32), uk) and np.array_equal(staged[0].view(np.uint32), uk)
+    assert np.array_equal(fused[1], sums) and np.array_equal(staged[1], sums)
+    assert np.array_equal(fused[2], cnts) and np.array_equal(staged[2], cnts)
