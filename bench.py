@@ -40,6 +40,34 @@ sys.path.insert(0, str(ROOT))
 L2_FLUSH_BYTES = 256 << 20
 FALLBACK_HBM_GBS = 6650.0
 
+# DRAM traffic of a dominant kernel per unit it processes, from one committed
+# ncu capture (dram__bytes_read.sum + dram__bytes_write.sum of the captured
+# launch divided by its units).  A full-size launch's traffic is this figure
+# times its units: each kernel streams its input once per unit, so traffic
+# grows in proportion to the units processed.
+NCU_TRAFFIC = {
+    "k_sort_pass": ((268.9e6 + 217.8e6) / 2**25, "pair",
+                    "profiles/k_sort_pass_2p25_pairs.md"),
+    "k_select_coop": ((537.0e6 + 39.6e6) / 2**26, "row",
+                      "profiles/k_select_coop_2p26.md (2^26 rows; at 2^24 the second read hits L2)"),
+    "k_hj_probe": ((170.2e6 + 24.4e6) / 2**24, "partitioned probe row",
+                   "profiles/k_hj_probe_2p25_probe.md"),
+    "k_gb_aggregate_shared": ((403.1e6 + 5.9e6) / 2**25, "row",
+                              "profiles/k_gb_aggregate_2p25_rows.md (4096 groups)"),
+    "k_gb_aggregate_direct": ((3528.9e6 + 874.8e6) / 2**25, "row",
+                              "profiles/k_gb_aggregate_2p25_rows.md (2^22 groups)"),
+    "k_smj_merge": ((336.1e6 + 215.0e6) / 2**25, "outer row",
+                    "profiles/k_smj_merge_2p25_outer.md"),
+}
+
+
+def ncu_traffic(kernel: str, units: float) -> dict | None:
+    """Traffic of one launch over `units` units, scaled from the capture."""
+    if kernel not in NCU_TRAFFIC:
+        return None
+    per, unit, src = NCU_TRAFFIC[kernel]
+    return {"bytes": round(per * units), "per_unit": round(per, 3), "unit": unit, "source": src}
+
 
 # ---------------------------------------------------------------------------
 # helpers
@@ -267,6 +295,16 @@ class SortSmjWorkload(Workload):
         # active pass (uniform and Zipf keys: 4 passes; R and S keys < 2^24: 3)
         self.pass_bytes = 16 * (4 * self.N + 4 * self.N + 3 * self.NR + 3 * self.NS)
         self.active_passes = 4 + 4 + 3 + 3
+        t = ncu_traffic("k_sort_pass", self.pass_bytes / 16 / self.active_passes)
+        self.traffic_per_launch = t["bytes"]
+        self.traffic_source = t
+
+    def release(self):
+        """Drops the device and pinned buffers (the per-operator suite runs next)."""
+        for name in ("ku", "kz", "rows", "rk", "rp", "sk", "sp", "ou", "oup", "oz", "ozp", "ji",
+                     "jo", "h_in", "d_in2", "h_out", "_streams"):
+            if hasattr(self, name):
+                delattr(self, name)
 
     def _run(self, ku, rows, kz, rk, rp, sk, sp):
         ops = self.ops
@@ -328,36 +366,44 @@ class SortSmjWorkload(Workload):
     def algorithmic_bytes_per_launch(self):
         return self.pass_bytes / self.active_passes
 
+    SMJ_BUFFER = 67112000  # the reference SMJ's BUFFER_SIZE: smallest multiple of 8000 >= 2^26
+
     def cpu_sample(self, ref, threads, budget_s):
-        """1/8 sample: reference sort of 2^23 uniform and 2^23 Zipf pairs and the
-        reference sort-merge join of 2^21 inner / 8,384,000 outer keys."""
+        """The full workload on the host cores, one whole step per repetition
+        (at least one; more while the budget lasts): the reference's
+        sort_kernel (sort.cpp:30-40) on the 2^26 uniform and the 2^26 Zipf
+        (key, row id) pairs -- packed into the harness's 64-bit pair words
+        before the timed region, so the timed call is the reference kernel
+        alone -- and the reference's sort_merge_join_kernel
+        (sort_merge_join.cpp:48-103) on the 2^24 R keys and 2^26 S keys (key
+        columns, as the reference joins; its merge cursor races with more
+        than one thread, which is the code as shipped).  The same seeded
+        inputs as the GPU arm."""
         from pimdal_b200 import gen
         if not hasattr(self, "_cpu"):
-            n = self.N // 8
-            nr = self.NR // 8
-            no = 8384000
             self.spec_z.cdf = gen.zipf_cdf(1 << 24, 1.0)
-            ku = gen.generate_cpu(self.spec_u, n)
-            kz = gen.generate_cpu(self.spec_z, n)
-            rk = (gen.generate_cpu(gen.Spec(self.L.GEN_PERM, self.L.U32, seed=7, perm_domain=nr), nr)
-                  + np.uint32(1))
-            sk = (gen.generate_cpu(gen.Spec(self.L.GEN_PERM_UNIFORM, self.L.U32, seed=7, stream_id=1,
-                                            lo=0, hi=nr - 1, perm_domain=nr), no) + np.uint32(1))
-            self._cpu = (ku, kz, rk, sk, 2 * n + nr + no)
-            for lib in ("sort", "smj_8384000"):
+            pu = ref.pack_pairs(gen.generate_cpu(self.spec_u, self.N))
+            pz = ref.pack_pairs(gen.generate_cpu(self.spec_z, self.N))
+            rk = gen.generate_cpu(self.spec_rk, self.NR).view(np.uint32)
+            sk = gen.generate_cpu(self.spec_sk, self.NS).view(np.uint32)
+            out = np.empty(self.N, np.uint64)
+            self._cpu = (pu, pz, rk, sk, out, 2 * self.N + self.NR + self.NS)
+            for lib in ("sort", f"smj_{self.SMJ_BUFFER}"):
                 ref.set_threads(lib, threads)
-        ku, kz, rk, sk, rows = self._cpu
+        pu, pz, rk, sk, out, rows = self._cpu
         reps = 0
-        t0 = time.perf_counter()
-        while reps < 1 or time.perf_counter() - t0 < budget_s:
-            ref.sort_pairs(ku)
-            ref.sort_pairs(kz)
-            ref.smj(rk, sk, 8384000, threads=threads)
+        dt = 0.0
+        while reps < 1 or dt < budget_s:
+            t0 = time.perf_counter()
+            ref.sort_packed(pu, out)
+            ref.sort_packed(pz, out)
+            ref.smj(rk, sk, self.SMJ_BUFFER, threads=threads)
+            dt += time.perf_counter() - t0
             reps += 1
-        dt = time.perf_counter() - t0
-        return rows * reps, dt, ("reference sort_kernel (sort.cpp:30-40) on 2^23 uniform and 2^23 "
-                                 "Zipf pairs + sort_merge_join_kernel (sort_merge_join.cpp:48-103, "
-                                 f"racy with >1 thread) on 2^21 x 8384000 keys, x{reps}")
+        return rows * reps, dt, (
+            "full config: reference sort_kernel (sort.cpp:30-40) on 2^26 uniform and 2^26 Zipf "
+            "(key, row id) pairs packed before the timed region + sort_merge_join_kernel "
+            f"(sort_merge_join.cpp:48-103) on 2^24 x 2^26 keys, x{reps}")
 
 
 class HashJoinWorkload(Workload):
@@ -691,11 +737,28 @@ class BatchWorkload(Workload):
             ok = m == int(rj[i]) and torch.equal(pay[:m], ppay[:m]) and torch.equal(row[:m], prow[:m])
             same += ok
         ms = min(times)
+        # the plain calls' device-busy time: every library kernel's duration
+        # (its CUDA events on the launching stream), summed -- what the 4096
+        # calls cost without the host's launch gaps between them
+        for k in range(self.L.KERNEL_COUNT):
+            self.ctx.kernel_time(k)
+        self.ctx.set_profiling(True)
+        self._plain(res_g, res_j)
+        self.ctx.sync()
+        self.ctx.set_profiling(False)
+        busy = sum(self.ctx.kernel_time(k)[1] for k in range(self.L.KERNEL_COUNT))
         self.plain = {"ms_per_step": round(ms, 3),
                       "value": round(self.rows_per_step / (ms / 1e3), 1), "unit": "rows/s",
+                      "device_busy_ms": round(busy, 3),
+                      "host_overhead_ms": round(max(0.0, ms - busy), 3),
                       "launches": "4096 plain operator calls (pimdal_group_kernel, "
-                                  "pimdal_hash_join unpartitioned), eager",
+                                  "pimdal_hash_join unpartitioned), eager from Python",
                       "bit_exact_instances": f"{same}/{self.NG + self.NJ}"}
+
+    def close(self):
+        del self.graph
+        self.gb.close()
+        self.jb.close()
 
     def step(self):
         self.graph.replay()
@@ -793,9 +856,11 @@ class ServeWorkload(Workload):
     metric_name = "queries/s"
     unit = "queries/s"
 
-    def __init__(self):
+    def __init__(self, requests: int | None = None):
         from pimdal_b200 import _lib as L
         self.L = L
+        if requests:
+            self.R = requests
         self.config = {"workload": "served filter->join->group-by pipelines (SUM(price*(100-discount)), "
                                    "COUNT by 1-2 keys) over a 6e7-row fact table + 1.5e7 / 2e6-row "
                                    "dimensions, ranges log-U[1e5,6e7], selectivity U[1%,50%]",
@@ -863,12 +928,17 @@ class ServeWorkload(Workload):
         staged = self.server.run(self.reqs, fused=False)
         same = serve.same_results(served, serial) and serve.same_results(staged, serial)
         stg = staged.summary()
-        return {"served_saturated": served.summary(), "serial_saturated": ser,
+        return {"requests_per_arm": self.R,
+                "served_saturated": served.summary(), "serial_saturated": ser,
                 "served_staged_saturated": stg,
-                "poisson": {"rate_per_s": round(rate, 2), "served": p_served, "serial": p_serial},
+                "poisson": {"rate_per_s": round(rate, 2), "served": p_served, "serial": p_serial,
+                            "p99_served_over_serial": round(p_served["p99_ms"] / p_serial["p99_ms"], 3)},
                 "served_equals_serial": same,
                 "speedup_vs_serial": round(served.summary()["queries_per_s"] / ser["queries_per_s"], 3),
                 "speedup_staged_concurrency_only": round(stg["queries_per_s"] / ser["queries_per_s"], 3)}
+
+    def close(self):
+        self.server.close()
 
     def step_e2e(self, stream):
         """A served run: request parameters in kernel arguments, each result
@@ -923,6 +993,201 @@ class ServeWorkload(Workload):
             f"reference select (select.cpp:77-100), partition + join (hash_join.cpp:57-157) and "
             f"hash_table_aggregate (aggregate.cpp:40-83) composed per request, numpy gathers "
             f"between them, {done} requests of the served mix")
+
+
+# ---------------------------------------------------------------------------
+# per-operator records of the default run: every config beside the headline
+# ---------------------------------------------------------------------------
+def _timed(fn, iters, flush, stream) -> list[float]:
+    """Device milliseconds of each of `iters` calls of fn, the L2 flushed
+    (256 MiB written) before each call, outside its events.  All calls are
+    enqueued behind a GPU sleep, so host-side launch gaps are not timed."""
+    import torch
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(iters)]
+    torch.cuda._sleep(int(1e8))
+    for i, (e0, e1) in enumerate(evs):
+        flush.fill_(i)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in evs]
+
+
+def _kernel_split(ctx, fn, iters=3) -> dict:
+    """Mean device milliseconds per call of each library kernel class (the
+    library's own CUDA events on the launching stream)."""
+    from pimdal_b200 import _lib as L
+    names = {getattr(L, k): k[len("KERNEL_"):].lower() for k in dir(L) if k.startswith("KERNEL_")}
+    for k in names:
+        ctx.kernel_time(k)
+    ctx.set_profiling(True)
+    for _ in range(iters):
+        fn()
+    ctx.sync()
+    ctx.set_profiling(False)
+    out = {}
+    for k, nm in sorted(names.items()):
+        n, ms = ctx.kernel_time(k)
+        if n:
+            out[nm] = {"launches": round(n / iters, 2), "ms": round(ms / iters, 4)}
+    return out
+
+
+def _op_record(rows, times, alg_bytes, peak, split=None, dominant=None, dom_bytes=None,
+               traffic=None) -> dict:
+    """rows/s, GB/s and roofline fraction of the whole operator (median of the
+    timed calls), and of its dominant kernel where one is named."""
+    med = statistics.median(times)
+    gbs = alg_bytes / (med * 1e-3) / 1e9
+    rec = {"rows": int(rows), "ms": round(med, 4), "ms_min": round(min(times), 4),
+           "calls": len(times), "rows_per_s": round(rows / (med * 1e-3), 1),
+           "algorithmic_bytes": int(alg_bytes), "gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
+    if split is not None:
+        rec["kernels_ms"] = split
+    if dominant and split and dominant in split:
+        kms = split[dominant]["ms"]
+        k = {"kernel_class": dominant, "ms": kms, "share": round(kms / med, 3)}
+        if dom_bytes:
+            kg = dom_bytes / (kms * 1e-3) / 1e9
+            k.update({"algorithmic_bytes": int(dom_bytes), "gbs": round(kg, 1),
+                      "frac": round(kg / peak, 4)})
+        if traffic:
+            k["traffic"] = traffic
+            if dom_bytes:
+                k["traffic_over_algorithmic"] = round(traffic["bytes"] / dom_bytes, 3)
+        rec["dominant"] = k
+    return rec
+
+
+def per_operator(ctx, dev, peak, iters=7) -> dict:
+    """The operators of configs 1, 3, 4 and 5 (and config 2's parts), each on
+    its config's full-size seeded inputs, measured in this run."""
+    import torch
+    from pimdal_b200 import _lib as L
+    from pimdal_b200 import gen, ops
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device=dev)
+    out = {}
+    g = lambda spec, n: ops.gen_column(ctx, spec, n)
+    e32 = lambda n: torch.empty(n, dtype=torch.int32, device=dev)
+    res = torch.empty(1, dtype=torch.int64, device=dev)
+
+    # ---- config 1: selection 2^24 int32 U[0, 2^31), v < 214748364 ----------
+    n = 1 << 24
+    keys = g(gen.Spec(L.GEN_UNIFORM, L.I32, seed=0xB200, lo=0, hi=2**31 - 1), n)
+    pred = ops.make_pred(L.PRED_LT, 214748364)
+    o1, o2 = e32(n), e32(n)
+    run = lambda: ops.sel_kernel(ctx, keys, pred, out=o1, out_ptr=o2, result=res)
+    run()
+    ctx.sync()
+    k = int(res.item())
+    t = _timed(run, 20, flush, stream)
+    alg = 4 * n + 8 * k
+    out["select_cfg1"] = dict(_op_record(n, t, alg, peak, _kernel_split(ctx, run), "select", alg,
+                                         ncu_traffic("k_select_coop", n)), selected=k)
+    del keys, o1, o2
+
+    # ---- config 2, by operator ----------------------------------------------
+    n = 1 << 26
+    for name, spec in (("sort_uniform_cfg2", gen.Spec(L.GEN_UNIFORM, L.U32, seed=0xB201, lo=0,
+                                                      hi=2**32 - 1)),
+                       ("sort_zipf_cfg2", gen.Spec(L.GEN_PERM_ZIPF, L.U32, seed=0xB201, stream_id=1,
+                                                   perm_domain=0, cdf=gen.zipf_cdf(1 << 24, 1.0)))):
+        keys = g(spec, n)
+        rows = torch.arange(n, dtype=torch.int32, device=dev)
+        ok, op = e32(n), e32(n)
+        run = lambda: ops.sort_kernel(ctx, keys, rows, out=ok, out_ptr=op)
+        run()
+        t = _timed(run, iters, flush, stream)
+        split = _kernel_split(ctx, run)
+        passes = split.get("sort_pass", {}).get("launches", 4)
+        out[name] = _op_record(n, t, 16 * n, peak, split, "sort_pass", 16 * n * passes,
+                               ncu_traffic("k_sort_pass", n * passes))
+        del keys, rows, ok, op
+
+    # ---- config 3: hash join, build 2^25 / probe 2^28, uniform and Zipf(0.75)
+    nb, npr = 1 << 25, 1 << 28
+    s3 = 0xB200 + 2
+    bk = g(gen.Spec(L.GEN_PERM, L.I32, seed=s3, perm_domain=2 * nb), nb)
+    bp = g(gen.Spec(L.GEN_UNIFORM, L.I32, seed=s3, stream_id=1, lo=-2**31, hi=2**31 - 1), nb)
+    opay, orow = e32(npr), e32(npr)
+    for name, sid, cdf in (("hash_join_uniform_cfg3", 2, None),
+                           ("hash_join_zipf_cfg3", 3, gen.zipf_cdf(nb, 0.75))):
+        pk = g(gen.Spec(L.GEN_PROBE, L.I32, seed=s3, stream_id=sid, lo=nb, perm_domain=2 * nb,
+                        match_permille=500, cdf=cdf), npr)
+        run = lambda: ops.hash_join(ctx, bk, bp, pk, capacity=npr, out_payload=opay,
+                                    out_row=orow, result=res)
+        run()
+        ctx.sync()
+        m = int(res.item())
+        t = _timed(run, iters, flush, stream)
+        split = _kernel_split(ctx, run)
+        alg = 8 * nb + 4 * npr + 8 * m
+        out[name] = dict(_op_record(nb + npr, t, alg, peak, split, "hj_probe",
+                                    8 * npr + 8 * m, ncu_traffic("k_hj_probe", npr)),
+                         matches=m, build_rows=nb, probe_rows=npr)
+        del pk
+    del bk, bp, opay, orow
+    torch.cuda.empty_cache()
+
+    # ---- config 3: group-by 2^28 rows, cardinality 16 / 2^12 / 2^22 ----------
+    n = 1 << 28
+    s3 = 0xB200 + 3
+    vals = g(gen.Spec(L.GEN_UNIFORM, L.I64, seed=s3, stream_id=1, lo=100, hi=10**7), n)
+    cap = 2 << 22
+    outs = {w: torch.empty(cap, dtype=torch.int64, device=dev) for w in ("sum", "count", "min", "max")}
+    outs["key"] = e32(cap)
+    for i, c in enumerate((16, 1 << 12, 1 << 22)):
+        keys = g(gen.Spec(L.GEN_PERM_UNIFORM, L.I32, seed=s3, stream_id=10 + i, lo=0, hi=c - 1,
+                          perm_domain=0), n)
+        for mname, method in (("hash", L.GROUP_HASH), ("sort", L.GROUP_SORT)):
+            run = lambda: ops.group_kernel(ctx, keys, vals, method=method, expected_groups=c,
+                                           capacity=cap, outs=outs, result=res)
+            run()
+            ctx.sync()
+            groups = int(res.item())
+            t = _timed(run, iters, flush, stream)
+            split = _kernel_split(ctx, run)
+            alg = 12 * n + 36 * groups
+            dom = "group" if method == L.GROUP_HASH else "sort_pass"
+            tr = None
+            if method == L.GROUP_HASH:
+                tr = ncu_traffic("k_gb_aggregate_direct" if c > (1 << 16) else "k_gb_aggregate_shared", n)
+            out[f"group_{mname}_{c}_cfg3"] = dict(
+                _op_record(n, t, alg, peak, split, dom, 12 * n if method == L.GROUP_HASH else None, tr),
+                groups=groups)
+        del keys
+    del vals, outs
+    torch.cuda.empty_cache()
+
+    # ---- config 4: batched form vs plain launches ---------------------------
+    bw = BatchWorkload()
+    bw.setup(ctx, dev)
+    t = _timed(bw.step, 5, flush, stream)
+    med = statistics.median(t)
+    plain = bw.plain
+    out["batched_cfg4"] = {
+        "instances": bw.NG + bw.NJ, "rows": bw.rows_per_step,
+        "batched_ms": round(med, 3), "batched_rows_per_s": round(bw.rows_per_step / (med * 1e-3), 1),
+        "plain": plain,
+        "speedup_vs_plain_wall": round(plain["ms_per_step"] / med, 3),
+        "speedup_vs_plain_device_busy": round(plain["device_busy_ms"] / med, 3),
+        "autotuned": bw.extra()["autotuned"]}
+    bw.close()
+    del bw
+    torch.cuda.empty_cache()
+
+    # ---- config 5: served form ------------------------------------------------
+    sw = ServeWorkload(requests=10_000)
+    sw.setup(ctx, dev)
+    sw.step()
+    out["served_cfg5"] = sw.extra()
+    sw.close()
+    del sw
+    torch.cuda.empty_cache()
+    return out
 
 
 WORKLOADS = {"select": SelectWorkload, "sort_smj": SortSmjWorkload,
@@ -1064,12 +1329,21 @@ def run_ours(args) -> None:
                 "peak": peak, "unit": "GB/s", "frac": round(ach / peak, 4),
                 "peak_source": peak_kind,
                 "traffic": wl.traffic_per_launch,
+                "traffic_source": getattr(wl, "traffic_source", None),
                 "algorithmic_bytes_per_launch": wl.algorithmic_bytes_per_launch(),
                 "mean_launch_ms": round(k_ms / k_launches, 5), "launches": k_launches}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(wl)
+
+    per_op = None
+    if world == 1 and args.workload == DEFAULT_WORKLOAD and not args.no_per_operator:
+        if hasattr(wl, "release"):
+            wl.release()
+        del flush
+        torch.cuda.empty_cache()
+        per_op = per_operator(ctx, dev, peak)
 
     if rank == 0:
         line = {
@@ -1085,6 +1359,8 @@ def run_ours(args) -> None:
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
             "gpu_launches": launches, "impl": "ours",
         }
+        if per_op is not None:
+            line["per_operator"] = per_op
         if hasattr(wl, "extra"):
             line.update(wl.extra())
         print(json.dumps(line), flush=True)
@@ -1101,14 +1377,34 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
+def host_cpu() -> dict:
+    """The host's CPU as the reference's runs record it: nproc, the lscpu
+    model name and socket count, and the threads the baseline uses."""
+    info = {"nproc": os.cpu_count(), "threads_used": host_threads()}
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=20).stdout
+        for line in out.splitlines():
+            key, _, val = line.partition(":")
+            key, val = key.strip(), val.strip()
+            if key == "Model name":
+                info["model"] = val
+            elif key == "Socket(s)":
+                info["sockets"] = int(val) if val.isdigit() else val
+            elif key == "Thread(s) per core":
+                info["threads_per_core"] = int(val) if val.isdigit() else val
+    except Exception:
+        pass
+    return info
+
+
 def cpu_baseline(wl) -> dict | None:
     import oracle
     if not oracle.Ref.available("select"):
         return {"value": None, "unavailable": "oracle/_ref not built"}
     threads = host_threads()
-    rows, secs, desc = wl.cpu_sample(oracle.Ref(), threads, 15.0)
+    rows, secs, desc = wl.cpu_sample(oracle.Ref(), threads, 12.0)
     return {"value": round(rows / secs, 1), "unit": getattr(wl, "unit", "rows/s"), "cores": threads,
-            "kind": "reference", "sample": desc}
+            "kind": "reference", "sample": desc, "cpu": host_cpu()}
 
 
 def run_reference(args) -> None:
@@ -1124,7 +1420,9 @@ def run_reference(args) -> None:
         return
     threads = host_threads()
     ref = oracle.Ref()
-    budget = max(0.5, min(5.0, 150.0 / (args.steps + args.warmup)))
+    # one step = one repetition of the workload's sample (the default
+    # workload's sample is the whole config); no extra budget per step
+    budget = 0.0 if args.workload == DEFAULT_WORKLOAD else max(0.5, min(5.0, 150.0 / (args.steps + args.warmup)))
     for _ in range(args.warmup):
         wl.cpu_sample(ref, threads, 0.0)
     rows = secs = 0.0
@@ -1142,9 +1440,10 @@ def run_reference(args) -> None:
         "ms_per_step": round(per_step / value * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "int32/uint32 keys, int64 sums", "data": "synthetic (seeded counter-based generator)",
-        "config": dict(wl.config, parallelism="host CPU"), "impl": "reference",
+        "config": dict(wl.config, parallelism=f"replicas x{world}"), "impl": "reference",
+        "execution": f"host CPU, {threads} threads (the reference's own CPU operators)",
         "cpu_baseline": {"value": round(value, 1), "unit": unit, "cores": threads,
-                         "kind": "reference", "sample": desc},
+                         "kind": "reference", "sample": desc, "cpu": host_cpu()},
         "e2e": {"value": round(value, 1), "unit": unit, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }), flush=True)
@@ -1158,6 +1457,8 @@ def main() -> None:
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-per-operator", action="store_true",
+                    help="skip the per-operator records of the default run (configs 1, 3, 4, 5)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

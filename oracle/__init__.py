@@ -179,22 +179,85 @@ def bloom_match(filters, keys, part_sizes, ptr=None):
     return ok[:c], op[:c], ms
 
 
-def _group(fn, keys, vals):
+def _group(fn, keys, vals, max_groups=None):
     k = np.ascontiguousarray(keys, dtype=np.int32)
     v = None if vals is None else np.ascontiguousarray(vals, dtype=np.int64)
     n = k.size
-    outs = [np.empty(max(n, 1), np.int32)] + [np.empty(max(n, 1), np.int64) for _ in range(4)]
+    cap = max(1, n if max_groups is None else min(n, max_groups))
+    outs = [np.empty(cap, np.int32)] + [np.empty(cap, np.int64) for _ in range(4)]
+    if max_groups is not None and n > cap:
+        # the C function writes every group: bound the count first
+        if np.unique(k).size > cap:
+            raise ValueError("more groups than max_groups")
     g = fn(_p(k), _p(v), n, *map(_p, outs))
     return tuple(o[:g] for o in outs)
 
 
-def group_by(keys, vals=None):
-    """(key, SUM, COUNT, MIN, MAX) per group, ascending by key."""
-    return _group(lib().oracle_group_by, keys, vals)
+def group_by(keys, vals=None, max_groups=None):
+    """(key, SUM, COUNT, MIN, MAX) per group, ascending by key.  max_groups
+    (optional) bounds the output arrays' size."""
+    return _group(lib().oracle_group_by, keys, vals, max_groups)
 
 
 def sort_group_by(keys, vals=None):
     return _group(lib().oracle_sort_group_by, keys, vals)
+
+
+def _key_parts(keys_u32: np.ndarray, parts_log2: int) -> np.ndarray:
+    """Partition index of every key: the top bits of key * 2^64/phi."""
+    h = keys_u32.astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15)
+    return (h >> np.uint64(64 - parts_log2)).astype(np.uint16)
+
+
+def _split_by_key(parts_log2: int, keys_u32: np.ndarray, *cols):
+    """Rows regrouped by key partition (stable): (bounds, keys, cols...)."""
+    part = _key_parts(keys_u32, parts_log2)
+    order = np.argsort(part, kind="stable")
+    bounds = np.concatenate([[0], np.cumsum(np.bincount(part, minlength=1 << parts_log2))])
+    return (bounds, keys_u32[order]) + tuple(None if c is None else c[order] for c in cols)
+
+
+def group_by_parallel(keys, vals=None, threads: int = 16, parts_log2: int = 6):
+    """group_by over disjoint key partitions in host threads (the C oracle
+    releases the GIL): every group lies in one partition, so the union of the
+    partitions' groups, ordered by key, is exactly group_by(keys, vals)."""
+    from concurrent.futures import ThreadPoolExecutor
+    k = np.ascontiguousarray(keys, dtype=np.int32)
+    v = None if vals is None else np.ascontiguousarray(vals, dtype=np.int64)
+    bounds, ks, vs = _split_by_key(parts_log2, k.view(np.uint32), v)
+    ks = ks.view(np.int32)
+
+    def one(p):
+        a, b = int(bounds[p]), int(bounds[p + 1])
+        return group_by(ks[a:b], None if vs is None else vs[a:b])
+
+    with ThreadPoolExecutor(threads) as ex:
+        res = list(ex.map(one, range(1 << parts_log2)))
+    cols = [np.concatenate([r[i] for r in res]) for i in range(5)]
+    order = np.argsort(cols[0], kind="stable")
+    return tuple(c[order] for c in cols)
+
+
+def hash_join_parallel(bkey, bpay, pkey, threads: int = 16, parts_log2: int = 6):
+    """hash_join over disjoint key partitions in host threads: a probe row
+    can only match build rows of its own key partition, so the union of the
+    partitions' matches is the multiset hash_join(bkey, bpay, pkey) returns
+    (probe row ids are global)."""
+    from concurrent.futures import ThreadPoolExecutor
+    bk, bp, pk = map(_u32, (bkey, bpay, pkey))
+    bb, bks, bps = _split_by_key(parts_log2, bk, bp)
+    pb, pks, prow = _split_by_key(parts_log2, pk, np.arange(pk.size, dtype=np.uint32))
+
+    def one(p):
+        a, b = int(bb[p]), int(bb[p + 1])
+        c, d = int(pb[p]), int(pb[p + 1])
+        if a == b or c == d:
+            return np.zeros(0, np.uint32), np.zeros(0, np.uint32)
+        return hash_join(bks[a:b], bps[a:b], pks[c:d], prow[c:d])
+
+    with ThreadPoolExecutor(threads) as ex:
+        res = list(ex.map(one, range(1 << parts_log2)))
+    return (np.concatenate([r[0] for r in res]), np.concatenate([r[1] for r in res]))
 
 
 # ------------------------------------------------------------ reference libs
@@ -247,6 +310,24 @@ class Ref:
         op = np.empty(max(k.size, 1), np.uint32)
         f(_p(k), _p(pp), k.size, int(is_signed), _p(ok), _p(op))
         return ok[:k.size], op[:k.size]
+
+    def sort_packed(self, packed: np.ndarray, out: np.ndarray | None = None) -> np.ndarray:
+        """The reference's sort_kernel on pre-packed (key, index) pairs: uint64
+        words with the key in the low 32 bits (pack with pack_pairs)."""
+        f = self._get("sort").pimdal_ref_sort_packed
+        f.restype = None
+        f.argtypes = [_P, _P, _U64]
+        src = np.ascontiguousarray(packed, dtype=np.uint64)
+        if out is None:
+            out = np.empty(max(src.size, 1), np.uint64)
+        f(_p(src), _p(out), src.size)
+        return out[:src.size]
+
+    @staticmethod
+    def pack_pairs(keys) -> np.ndarray:
+        """(key, row index) pairs as the sort harness's 64-bit words."""
+        k = _u32(keys).astype(np.uint64)
+        return k | (np.arange(k.size, dtype=np.uint64) << np.uint64(32))
 
     def sort_keys(self, keys):
         f = self._get("sort").pimdal_ref_sort_keys
@@ -335,7 +416,11 @@ class Ref:
         f.restype = None
         f.argtypes = [_P, _U64, _P, _U64, _P, _P]
         ik, ok = _u32(inner_keys), _u32(outer_keys)
-        ires = np.zeros(ok.size + 1, np.uint32)
-        ores = np.zeros(ok.size + 1, np.uint32)
+        assert ok.size <= buffer_size
+        # the merge walks all BUFFER_SIZE/8000 blocks of 8000 rows (:83-101):
+        # an outer size below BUFFER_SIZE needs that much slack in the buffers
+        room = buffer_size + 1
+        ires = np.zeros(room, np.uint32)
+        ores = np.zeros(room, np.uint32)
         f(_p(ik), ik.size, _p(ok), ok.size, _p(ires), _p(ores))
         return ires[:ok.size], ores[:ok.size]

@@ -330,20 +330,45 @@ static inline void grp_add(grp_t *g, int64_t v) {
   if (v > g->max) g->max = v;
 }
 
-uint64_t oracle_group_by(const int32_t *key, const int64_t *val, uint64_t n, int32_t *out_key,
-                         int64_t *out_sum, int64_t *out_count, int64_t *out_min, int64_t *out_max) {
-  /* hash_table_aggregate (aggregate.cpp:40-83): find-or-insert per row. */
-  uint64_t cap = 16;
-  while (cap < 2 * n + 1) cap *= 2;
+static int64_t *grp_table_new(uint64_t cap) {
   int64_t *slot = (int64_t *)malloc(cap * sizeof(int64_t));
   for (uint64_t s = 0; s < cap; s++) slot[s] = -1;
-  grp_t *g = (grp_t *)malloc((n ? n : 1) * sizeof(grp_t));
+  return slot;
+}
+
+static inline uint64_t grp_home(int32_t key, uint64_t cap) {
+  return ((uint64_t)(uint32_t)key * 0x9E3779B97F4A7C15ull) >> 20 & (cap - 1);
+}
+
+uint64_t oracle_group_by(const int32_t *key, const int64_t *val, uint64_t n, int32_t *out_key,
+                         int64_t *out_sum, int64_t *out_count, int64_t *out_min, int64_t *out_max) {
+  /* hash_table_aggregate (aggregate.cpp:40-83): find-or-insert per row into a
+   * table that doubles when half full, as absl::flat_hash_map grows. */
+  uint64_t cap = 16, gcap = 8;
+  int64_t *slot = grp_table_new(cap);
+  grp_t *g = (grp_t *)malloc(gcap * sizeof(grp_t));
   uint64_t ng = 0;
   for (uint64_t i = 0; i < n; i++) {
     int64_t v = val ? val[i] : 1;
-    uint64_t h = ((uint64_t)(uint32_t)key[i] * 0x9E3779B97F4A7C15ull) >> 20 & (cap - 1);
+    uint64_t h = grp_home(key[i], cap);
     while (slot[h] >= 0 && g[slot[h]].key != key[i]) h = (h + 1) & (cap - 1);
     if (slot[h] < 0) {
+      if (2 * (ng + 1) > cap) { /* grow, rehash every group, then find the slot again */
+        free(slot);
+        cap *= 2;
+        slot = grp_table_new(cap);
+        for (uint64_t q = 0; q < ng; q++) {
+          uint64_t t = grp_home(g[q].key, cap);
+          while (slot[t] >= 0) t = (t + 1) & (cap - 1);
+          slot[t] = (int64_t)q;
+        }
+        h = grp_home(key[i], cap);
+        while (slot[h] >= 0) h = (h + 1) & (cap - 1);
+      }
+      if (ng == gcap) {
+        gcap *= 2;
+        g = (grp_t *)realloc(g, gcap * sizeof(grp_t));
+      }
       slot[h] = (int64_t)ng;
       g[ng].key = key[i];
       g[ng].sum = 0;

@@ -30,6 +30,14 @@ void pimdal_ref_sort_keys(const uint32_t *in, uint32_t *out, uint64_t n) {
   sort_kernel(const_cast<uint32_t *>(in), out, n);
 }
 
+// The reference kernel on pairs that the caller packed beforehand: each
+// 64-bit word is a PdPairU (key in the low half, index in the high half, as
+// the struct lies in memory), so the timed call is sort_kernel alone.
+void pimdal_ref_sort_packed(const uint64_t *in, uint64_t *out, uint64_t n) {
+  sort_kernel(reinterpret_cast<PdPairU *>(const_cast<uint64_t *>(in)),
+              reinterpret_cast<PdPairU *>(out), n);
+}
+
 // Stable sort of (key, ptr) by key; ptr == NULL means row id = index.
 void pimdal_ref_sort_pairs(const uint32_t *key, const uint32_t *ptr, uint64_t n, int is_signed,
                            uint32_t *out_key, uint32_t *out_ptr) {

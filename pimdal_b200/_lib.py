@@ -26,6 +26,7 @@ GEN_UNIFORM, GEN_PERM, GEN_PERM_UNIFORM, GEN_PERM_ZIPF, GEN_PROBE = range(5)
 (KERNEL_SELECT, KERNEL_GEN, KERNEL_SORT_HIST, KERNEL_SORT_PASS, KERNEL_SMJ_MERGE, KERNEL_PARTITION,
  KERNEL_HJ_BUILD, KERNEL_HJ_PROBE, KERNEL_GROUP, KERNEL_SEGREDUCE, KERNEL_OTHER, KERNEL_FILTER,
  KERNEL_MATCH, KERNEL_FUSED) = range(14)
+KERNEL_COUNT = 14
 FILTER_BITS = 16384
 FILTER_BYTES = FILTER_BITS // 8
 

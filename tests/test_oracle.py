@@ -144,3 +144,33 @@ def test_bloom_oracle_vs_reference_fresh_inputs():
     q[::4] = k[::4]
     for a, b in zip(oracle.bloom_match(filt, q, ps), ref.bloom_match(filt, q, ps)):
         assert np.array_equal(a, b)
+
+
+def test_parallel_group_by_equals_serial():
+    """The key-partitioned, threaded group-by (used at full sizes) returns
+    exactly the serial oracle's groups."""
+    rng = np.random.default_rng(41)
+    k = rng.integers(-5000, 5000, 300_000).astype(np.int32)
+    k[::11] = -1
+    v = rng.integers(-10**12, 10**12, k.size).astype(np.int64)
+    exp = oracle.group_by(k, v)
+    got = oracle.group_by_parallel(k, v, threads=4, parts_log2=3)
+    for a, b in zip(got, exp):
+        assert np.array_equal(a, b)
+    got = oracle.group_by_parallel(k, None, threads=2, parts_log2=1)
+    for a, b in zip(got, oracle.group_by(k, None)):
+        assert np.array_equal(a, b)
+
+
+def test_parallel_hash_join_equals_serial():
+    """The key-partitioned, threaded hash join returns the serial oracle's
+    multiset of (build payload, probe row id), duplicate build keys included."""
+    rng = np.random.default_rng(42)
+    bk = rng.integers(0, 20_000, 30_000).astype(np.uint32)
+    bp = rng.integers(0, 2**32, bk.size, dtype=np.uint64).astype(np.uint32)
+    pk = rng.integers(0, 40_000, 200_000).astype(np.uint32)
+    ep, er = oracle.hash_join(bk, bp, pk)
+    gp, gr = oracle.hash_join_parallel(bk, bp, pk, threads=4, parts_log2=4)
+    a, b = np.lexsort((gp, gr)), np.lexsort((ep, er))
+    assert gp.size == ep.size
+    assert np.array_equal(gp[a], ep[b]) and np.array_equal(gr[a], er[b])
