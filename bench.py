@@ -1185,7 +1185,33 @@ def per_operator(ctx, dev, peak, iters=7) -> dict:
     sw.step()
     out["served_cfg5"] = sw.extra()
     sw.close()
-    del sw
+
+    # ---- the reference's TPC-H Q6 and Q1 pipelines, on the same table --------
+    from pimdal_b200 import tpch
+    li = tpch.Lineitem(ctx, sw.tables)
+    n = li.n
+    s6 = tpch.q6(ctx, li, staged=True)
+    preds, exprs = tpch.q6_args(li)
+    run = lambda: ops.select_aggregate(ctx, n, preds=preds, exprs=exprs, result=res)
+    run()
+    t = _timed(run, 20, flush, stream)
+    alg = tpch.algorithmic_bytes_q6(n, s6.stage_rows)
+    out["tpch_q6_fused"] = dict(_op_record(n, t, alg, peak, _kernel_split(ctx, run), "scan_agg", alg),
+                                stage_rows=list(s6.stage_rows), revenue=s6.revenue)
+    t = _timed(lambda: tpch.q6(ctx, li, staged=True), 5, flush, stream)
+    out["tpch_q6_staged"] = _op_record(n, t, alg, peak)
+    pred, group, exprs = tpch.q1_args(li)
+    sel = int(((li.shipdate < tpch.packed(tpch.Q1_DATE))).sum().item())
+    run = lambda: ops.select_aggregate(ctx, n, preds=[pred], group=group, key_space=6,
+                                       exprs=exprs, result=res)
+    run()
+    t = _timed(run, 20, flush, stream)
+    alg = tpch.algorithmic_bytes_q1(n, sel)
+    out["tpch_q1_fused"] = dict(_op_record(n, t, alg, peak, _kernel_split(ctx, run), "scan_agg", alg),
+                                selected=sel)
+    t = _timed(lambda: tpch.q1(ctx, li, staged=True), 5, flush, stream)
+    out["tpch_q1_staged"] = _op_record(n, t, alg, peak)
+    del li, sw
     torch.cuda.empty_cache()
     return out
 

@@ -61,7 +61,7 @@ typedef struct {
 } pimdal_key_ptr32_t;
 
 /* Column element types accepted at the boundary. */
-typedef enum { PIMDAL_U32 = 0, PIMDAL_I32 = 1, PIMDAL_I64 = 2 } pimdal_dtype_t;
+typedef enum { PIMDAL_U32 = 0, PIMDAL_I32 = 1, PIMDAL_I64 = 2, PIMDAL_U8 = 3 } pimdal_dtype_t;
 
 /* Input/output layout: structure-of-arrays columns (key column + row-id
  * column) or the reference's array of key_ptr32 pairs. */
@@ -109,7 +109,8 @@ typedef enum {
   PIMDAL_KERNEL_FILTER = 11,     /* Bloom filter build                     */
   PIMDAL_KERNEL_MATCH = 12,      /* Bloom filter probe + ordered compaction*/
   PIMDAL_KERNEL_FUSED = 13,      /* fused select -> join -> group-by pass  */
-  PIMDAL_KERNEL_COUNT = 14
+  PIMDAL_KERNEL_SCAN_AGG = 14,   /* fused select -> arithmetic -> group-by */
+  PIMDAL_KERNEL_COUNT = 15
 } pimdal_kernel_id_t;
 int pimdal_ctx_set_profiling(pimdal_ctx_t *ctx, int enable);
 int pimdal_ctx_kernel_time(pimdal_ctx_t *ctx, int kernel_id, uint64_t *launches,
@@ -560,6 +561,81 @@ int pimdal_select_join_aggregate_workspace_size(
 int pimdal_select_join_aggregate(pimdal_ctx_t *ctx,
                                  const pimdal_select_join_aggregate_arguments_t *args,
                                  pimdal_aggr_results_t *d_result, pimdal_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
+/* Fused select -> arithmetic -> group-by scan.  Replaces the chains that the */
+/* reference's query pipelines run as separate DPU kernels with host steps    */
+/* between them: one sel_kernel per predicate with load_next gathers in       */
+/* between, arithmetic_kernel (pimdal/general/arithmetic.c:35-67) and         */
+/* reduce_kernel (pimdal/general/reduce.c:42-77) -- e.g. the Q6 chain of      */
+/* pimdal/main/tpc_h/query6/dpu/kernel_q6.c:112-156 -- and the per-row sums   */
+/* and group-by of pimdal/main/tpc_h/query1/dpu/kernel_q1_1.c:84-170 with     */
+/* kernel_q1_2.c.                                                              */
+/*                                                                            */
+/* Row i < size is the table row r = rows ? rows[i] : i.  It takes part when  */
+/* every predicate holds on its column at r.  Its group key is                */
+/* sum_g group[g].col[r] * group[g].mult (uint32, wrapping; 0 without group   */
+/* columns) and must be < key_space, else PIMDAL_ERR_ARG is raised at         */
+/* pimdal_ctx_sync_status.  Expression e is the int64 product (wrapping) of   */
+/* its terms, term t being (negate ? -col[r] : col[r]) + add, or the constant */
+/* add when col is NULL.  Output: the groups with at least one row, ascending */
+/* by key: out_key, out_count and one SUM (int64, wrapping) per expression in */
+/* out_sum[e] (NULL: not written).  Columns are PIMDAL_I32, PIMDAL_U32,        */
+/* PIMDAL_I64 or PIMDAL_U8 (zero-extended) values.  Scratch:                  */
+/* key_space * (n_exprs + 1) * 8 bytes of the context's workspace.            */
+/* ------------------------------------------------------------------------- */
+#define PIMDAL_SA_MAX_PREDS 4
+#define PIMDAL_SA_MAX_GROUP_COLS 2
+#define PIMDAL_SA_MAX_EXPRS 6
+#define PIMDAL_SA_MAX_TERMS 3
+#define PIMDAL_SA_MAX_KEYS 1024
+
+typedef struct {
+  const void *col;
+  int32_t dtype;           /* pimdal_dtype_t                                   */
+  int32_t pad;
+  pimdal_pred_t pred;      /* the predicate on col (sel_arguments_t.pred)      */
+} pimdal_column_pred_t;
+
+typedef struct {
+  const void *col;
+  int32_t dtype;
+  uint32_t mult;           /* key += col[r] * mult                             */
+} pimdal_group_col_t;
+
+typedef struct {
+  const void *col;         /* NULL: the term is the constant add               */
+  int32_t dtype;
+  int32_t negate;          /* term = -col[r] + add                             */
+  int64_t add;
+} pimdal_term_t;
+
+typedef struct {
+  pimdal_term_t term[PIMDAL_SA_MAX_TERMS];
+  uint32_t n_terms;        /* 1..PIMDAL_SA_MAX_TERMS                           */
+  uint32_t pad;
+} pimdal_expr_t;
+
+typedef struct {
+  uint64_t size;                                  /* rows scanned (< 2^32)    */
+  const uint32_t *rows;                           /* NULL: row i is i         */
+  pimdal_column_pred_t pred[PIMDAL_SA_MAX_PREDS];
+  uint32_t n_preds;
+  uint32_t n_group;
+  pimdal_group_col_t group[PIMDAL_SA_MAX_GROUP_COLS];
+  uint32_t key_space;                             /* 1..PIMDAL_SA_MAX_KEYS    */
+  uint32_t n_exprs;                               /* 0..PIMDAL_SA_MAX_EXPRS   */
+  pimdal_expr_t expr[PIMDAL_SA_MAX_EXPRS];
+  uint32_t *out_key;
+  int64_t *out_count;
+  int64_t *out_sum[PIMDAL_SA_MAX_EXPRS];
+  uint64_t out_capacity;                          /* groups room              */
+} pimdal_select_aggregate_arguments_t;
+
+int pimdal_select_aggregate_workspace_size(const pimdal_select_aggregate_arguments_t *args,
+                                           size_t *bytes);
+int pimdal_select_aggregate(pimdal_ctx_t *ctx, const pimdal_select_aggregate_arguments_t *args,
+                            pimdal_aggr_results_t *d_result, pimdal_stream_t stream);
 
 /* ------------------------------------------------------------------------- */
 /* Batched form: many independent group-by or hash-join instances, each phase */

@@ -19,14 +19,14 @@ STATUS_NAMES = {
     4: "PIMDAL_ERR_TABLE_FULL", 5: "PIMDAL_ERR_DEVICE_TIMEOUT", 6: "PIMDAL_ERR_CUDA",
     7: "PIMDAL_ERR_CAPACITY", 8: "PIMDAL_ERR_BUDGET", 9: "PIMDAL_ERR_NOT_SUPPORTED",
 }
-U32, I32, I64 = 0, 1, 2
+U32, I32, I64, U8 = 0, 1, 2, 3
 LAYOUT_COLUMNS, LAYOUT_PAIRS = 0, 1
 PRED_LT, PRED_LE, PRED_GT, PRED_GE, PRED_EQ, PRED_NE, PRED_BETWEEN, PRED_RANGE = range(8)
 GEN_UNIFORM, GEN_PERM, GEN_PERM_UNIFORM, GEN_PERM_ZIPF, GEN_PROBE = range(5)
 (KERNEL_SELECT, KERNEL_GEN, KERNEL_SORT_HIST, KERNEL_SORT_PASS, KERNEL_SMJ_MERGE, KERNEL_PARTITION,
  KERNEL_HJ_BUILD, KERNEL_HJ_PROBE, KERNEL_GROUP, KERNEL_SEGREDUCE, KERNEL_OTHER, KERNEL_FILTER,
- KERNEL_MATCH, KERNEL_FUSED) = range(14)
-KERNEL_COUNT = 14
+ KERNEL_MATCH, KERNEL_FUSED, KERNEL_SCAN_AGG) = range(15)
+KERNEL_COUNT = 15
 FILTER_BITS = 16384
 FILTER_BYTES = FILTER_BITS // 8
 
@@ -151,6 +151,37 @@ class SelectJoinAggregateArguments(C.Structure):
     ]
 
 
+SA_MAX_PREDS, SA_MAX_GROUP_COLS, SA_MAX_EXPRS, SA_MAX_TERMS, SA_MAX_KEYS = 4, 2, 6, 3, 1024
+
+
+class ColumnPred(C.Structure):
+    _fields_ = [("col", C.c_void_p), ("dtype", C.c_int32), ("pad", C.c_int32), ("pred", Pred)]
+
+
+class GroupCol(C.Structure):
+    _fields_ = [("col", C.c_void_p), ("dtype", C.c_int32), ("mult", C.c_uint32)]
+
+
+class Term(C.Structure):
+    _fields_ = [("col", C.c_void_p), ("dtype", C.c_int32), ("negate", C.c_int32),
+                ("add", C.c_int64)]
+
+
+class Expr(C.Structure):
+    _fields_ = [("term", Term * SA_MAX_TERMS), ("n_terms", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class SelectAggregateArguments(C.Structure):
+    _fields_ = [
+        ("size", C.c_uint64), ("rows", C.c_void_p),
+        ("pred", ColumnPred * SA_MAX_PREDS), ("n_preds", C.c_uint32), ("n_group", C.c_uint32),
+        ("group", GroupCol * SA_MAX_GROUP_COLS), ("key_space", C.c_uint32),
+        ("n_exprs", C.c_uint32), ("expr", Expr * SA_MAX_EXPRS),
+        ("out_key", C.c_void_p), ("out_count", C.c_void_p),
+        ("out_sum", C.c_void_p * SA_MAX_EXPRS), ("out_capacity", C.c_uint64),
+    ]
+
+
 GROUP_AUTO, GROUP_HASH, GROUP_SORT = 0, 1, 2
 
 
@@ -211,6 +242,9 @@ SIGNATURES = {
     "pimdal_select_join_aggregate": (_I, [_VP, C.POINTER(SelectJoinAggregateArguments), _VP, _VP]),
     "pimdal_select_join_aggregate_workspace_size": (_I, [C.POINTER(SelectJoinAggregateArguments),
                                                         C.POINTER(_SZ)]),
+    "pimdal_select_aggregate": (_I, [_VP, C.POINTER(SelectAggregateArguments), _VP, _VP]),
+    "pimdal_select_aggregate_workspace_size": (_I, [C.POINTER(SelectAggregateArguments),
+                                                   C.POINTER(_SZ)]),
     "pimdal_match_workspace_size": (_I, [C.POINTER(MatchArguments), C.POINTER(_SZ)]),
     "pimdal_match_kernel": (_I, [_VP, C.POINTER(MatchArguments), _VP, _VP]),
     "pimdal_hash_join_workspace_size": (_I, [C.POINTER(HashJoinArguments), C.POINTER(_SZ)]),

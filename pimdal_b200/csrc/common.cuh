@@ -442,6 +442,9 @@ PD_HD uint32_t pd_mulhash32(uint32_t key) { return (uint32_t)(((uint64_t)key * P
 // Internal entry points shared between translation units.
 // ---------------------------------------------------------------------------
 enum : int { PD_KEY_PLAIN = 0, PD_KEY_HASH0 = 1, PD_KEY_MULHASH = 2 };
+// A predicate as an inclusive interval [lo, hi] of int64 (and an inversion
+// flag for NE); false for an unknown operator.
+bool pd_pred_interval(const pimdal_pred_t &pr, int64_t *lo, int64_t *hi, uint32_t *invert);
 int pd_sort_with_workspace(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, void *ws,
                            cudaStream_t s);
 int pd_sort_ex(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,

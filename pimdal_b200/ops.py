@@ -410,6 +410,68 @@ def gather_u32(ctx: Context, col, idx, n: int | None = None, out=None, stream=No
     return out
 
 
+_DTYPE_OF = {torch.int32: L.I32, torch.int64: L.I64, torch.uint8: L.U8}
+
+
+def _col_dtype(t, dtype=None) -> int:
+    return _DTYPE_OF[t.dtype] if dtype is None else dtype
+
+
+def select_aggregate(ctx: Context, size: int, *, preds=(), group=(), key_space: int = 1,
+                     exprs=(), rows=None, outs=None, result=None, stream=None):
+    """Fused select -> arithmetic -> group-by scan (pimdal_select_aggregate).
+
+    preds: (column, pred) or (column, pred, dtype); group: (column, mult) or
+    (column, mult, dtype); exprs: lists of terms, a term being a column, an
+    int constant, or (column | None, negate, add[, dtype]) for
+    (negate ? -col : col) + add.  Column dtypes follow the tensors (int32 ->
+    PIMDAL_I32, int64 -> I64, uint8 -> U8) unless given.  Returns
+    (result, outs) with outs "key", "count" and "sum0".. "sum{n-1}" holding
+    the groups in key order (result[0] of them)."""
+    dev = f"cuda:{ctx.device}"
+    a = L.SelectAggregateArguments()
+    a.size = size
+    a.rows = _ptr(rows)
+    a.n_preds = len(preds)
+    for q, pr in enumerate(preds):
+        col, pred = pr[0], pr[1]
+        a.pred[q] = L.ColumnPred(col=_ptr(col), dtype=_col_dtype(col, pr[2] if len(pr) > 2 else None),
+                                 pad=0, pred=pred)
+    a.n_group = len(group)
+    for g, gr in enumerate(group):
+        col, mult = gr[0], gr[1]
+        a.group[g] = L.GroupCol(col=_ptr(col), dtype=_col_dtype(col, gr[2] if len(gr) > 2 else None),
+                                mult=mult)
+    a.key_space = key_space
+    a.n_exprs = len(exprs)
+    for e, terms in enumerate(exprs):
+        a.expr[e].n_terms = len(terms)
+        for t, term in enumerate(terms):
+            if isinstance(term, int):
+                term = (None, 0, term)
+            elif isinstance(term, torch.Tensor):
+                term = (term, 0, 0)
+            col, neg, add = term[0], term[1], term[2]
+            dt = 0 if col is None else _col_dtype(col, term[3] if len(term) > 3 else None)
+            a.expr[e].term[t] = L.Term(col=_ptr(col), dtype=dt, negate=neg, add=add)
+    if outs is None:
+        outs = {"key": torch.empty(key_space, dtype=torch.int32, device=dev),
+                "count": torch.empty(key_space, dtype=torch.int64, device=dev)}
+        for e in range(len(exprs)):
+            outs[f"sum{e}"] = torch.empty(key_space, dtype=torch.int64, device=dev)
+    if result is None:
+        result = torch.empty(1, dtype=torch.int64, device=dev)
+    a.out_key = _ptr(outs["key"])
+    a.out_count = _ptr(outs["count"])
+    for e in range(len(exprs)):
+        a.out_sum[e] = _ptr(outs.get(f"sum{e}"))
+    a.out_capacity = outs["key"].numel()
+    _workspace(ctx, ctx.lib.pimdal_select_aggregate_workspace_size, a)
+    L.check(ctx.lib.pimdal_select_aggregate(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
+            "pimdal_select_aggregate")
+    return result, outs
+
+
 def revenue_keys(ctx: Context, n: int, match_row, match_attr, sel_rows, price, discount, flag,
                  attr_mult: int, out_key, out_val, stream=None) -> None:
     """key = attr * attr_mult + flag[row], value = price[row] * (100 - discount[row])

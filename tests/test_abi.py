@@ -79,3 +79,27 @@ def test_prefilter_fused_and_ingest_argument_errors_need_no_gpu():
     assert sz.value == 16 * 50
     sa.key_space = L.FUSED_MAX_KEYS + 1
     assert lib.pimdal_select_join_aggregate_workspace_size(ctypes.byref(sa), ctypes.byref(sz)) == 1
+
+
+def test_select_aggregate_layout_and_argument_errors_need_no_gpu():
+    lib = L.lib()
+    a = L.SelectAggregateArguments()
+    # the ctypes mirror has the C struct's size (offsets follow from the fields)
+    assert ctypes.sizeof(a) == (8 + 8 + L.SA_MAX_PREDS * 40 + 8 + L.SA_MAX_GROUP_COLS * 16 + 8
+                                + L.SA_MAX_EXPRS * (L.SA_MAX_TERMS * 24 + 8) + 8 + 8
+                                + L.SA_MAX_EXPRS * 8 + 8)
+    assert lib.pimdal_select_aggregate(None, ctypes.byref(a), None, None) == 1
+    sz = ctypes.c_size_t(7)
+    a.key_space, a.n_exprs = 6, 5
+    assert lib.pimdal_select_aggregate_workspace_size(ctypes.byref(a), ctypes.byref(sz)) == 0
+    assert sz.value == 8 * 6 * 6
+    a.key_space = L.SA_MAX_KEYS + 1
+    assert lib.pimdal_select_aggregate_workspace_size(ctypes.byref(a), ctypes.byref(sz)) == 1
+
+
+def test_tpch_packed_dates_follow_the_reference_reader():
+    from pimdal_b200 import tpch
+    # read_table.cpp:8-16: day + (month << 5) + ((year - 1900) << 9)
+    assert tpch.packed("1994-01-01") == 1 + (1 << 5) + (94 << 9)
+    assert tpch.packed("1998-09-02") == 2 + (9 << 5) + (98 << 9)
+    assert tpch.packed(tpch.Q6_DATE_LO) < tpch.packed(tpch.Q6_DATE_HI)
