@@ -510,6 +510,235 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   for (uint32_t i = tid; i < tile_n; i += RS_THREADS) put(i);
 }
 
+// ------------------------------------------------- small-radix partition pass
+// A single stable pass on a digit of at most 6 bits (the hash join's radix
+// partition): no per-item warp matching.  Each thread owns PP_ITEMS
+// consecutive elements of the tile and counts them per digit in its own
+// 16-bit shared-memory counters (no atomics; stable because a thread's items
+// are consecutive and counted in order).  A raking scan over the packed
+// counters, in (digit, thread) order, turns the counts into tile ranks and
+// digit starts; the digits' global offsets come from the same decoupled
+// look-back as the digit pass; the tile is staged in digit order and every
+// digit run is written contiguously.
+//
+// Counter layout: word (lane, thread), lane = digit % LANES, holds the
+// counters of digits lane and lane + LANES in its low and high halves, so a
+// digit's rank order is (half, lane, thread) = (digit, thread).  Each
+// thread's raking segment of LANES words is padded by one word, so the
+// segment walks hit distinct banks.
+constexpr int PP_ITEMS = RS_ITEMS;            // same tile as the digit pass
+static_assert(PP_ITEMS % 4 == 0, "16-byte loads of a thread's items");
+
+template <int BITS>
+struct PartShape {
+  static constexpr int B = 1 << BITS;          // digits
+  static constexpr int LANES = B / 2;          // packed counter words per thread
+  static constexpr int SEG = LANES;            // raking segment (words per thread)
+  static constexpr int WORDS = LANES * RS_THREADS + RS_THREADS;  // + one pad word per segment
+  static __device__ __forceinline__ int pad(int e) { return e + e / SEG; }
+};
+
+template <int BITS, bool HAS_VALS, int KEY_MODE>
+__global__ void __launch_bounds__(RS_THREADS, 3)
+k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
+  using S = PartShape<BITS>;
+  extern __shared__ __align__(16) uint2 pp_stage[];  // RS_TILE (key, value) words or keys
+  __shared__ uint32_t s_cnt[S::WORDS];
+  __shared__ uint32_t s_warp[RS_WARPS];
+  __shared__ uint32_t s_dstart[S::B + 1];
+  __shared__ int32_t s_gdelta[S::B];
+  __shared__ uint32_t s_tile;
+  uint2 *s_kv = pp_stage;
+  uint32_t *s_k = reinterpret_cast<uint32_t *>(pp_stage);
+
+  const SortPlan *plan = p.plan;
+  if (!plan->active[pass]) return;
+  const uint32_t src = plan->src[pass], dst = plan->dst[pass];
+  const bool first = plan->first[pass] != 0;
+  const uint32_t flip = p.flip;
+  const uint32_t mask = S::B - 1;
+  auto dig = [&](uint32_t k) { return (sort_xform<KEY_MODE>(k, flip) >> shift) & mask; };
+
+  const int tid = threadIdx.x;
+  if (tid == 0) s_tile = atomicAdd(&p.counters[pass], 1u);
+  for (int i = tid; i < S::WORDS; i += RS_THREADS) s_cnt[i] = 0;
+  __syncthreads();
+  const uint64_t tile = s_tile;
+  const uint64_t base = tile * (uint64_t)RS_TILE;
+  const uint64_t n = sort_n(p);
+  if (base >= n) return;
+  const uint32_t tile_n = (uint32_t)min((uint64_t)RS_TILE, n - base);
+  const uint32_t t0 = (uint32_t)tid * PP_ITEMS;  // tile-local index of this thread's first item
+
+  // columns only (the caller routes pair layouts to the digit pass)
+  const uint32_t *skey = (src == BUF_IN ? reinterpret_cast<const uint32_t *>(p.in)
+                          : src == BUF_OUT ? reinterpret_cast<const uint32_t *>(p.out) : p.alt_key) + base;
+  const uint32_t *sval = src == BUF_IN ? p.in_ptr : (src == BUF_OUT ? p.out_ptr : p.alt_ptr);
+  if (sval) sval += base;
+  uint32_t *dkey = dst == BUF_OUT ? reinterpret_cast<uint32_t *>(p.out) : p.alt_key;
+  uint32_t *dval = dst == BUF_OUT ? p.out_ptr : p.alt_ptr;
+  const bool gen_vals = first && src == BUF_IN && p.in_ptr == nullptr;
+  const uint32_t vbase = (uint32_t)(p.ptr_base + base);
+  const bool vec = ((reinterpret_cast<uintptr_t>(skey) | reinterpret_cast<uintptr_t>(sval)) & 15u) == 0;
+
+  // 1. load this thread's consecutive items
+  uint32_t key[PP_ITEMS];
+  uint32_t val[HAS_VALS ? PP_ITEMS : 1];
+  if (vec && t0 + PP_ITEMS <= tile_n) {
+#pragma unroll
+    for (int j = 0; j < PP_ITEMS / 4; ++j) {
+      const uint4 a = __ldcs(reinterpret_cast<const uint4 *>(skey + t0) + j);
+      key[4 * j] = a.x; key[4 * j + 1] = a.y; key[4 * j + 2] = a.z; key[4 * j + 3] = a.w;
+      if (HAS_VALS && !gen_vals) {
+        const uint4 b = __ldcs(reinterpret_cast<const uint4 *>(sval + t0) + j);
+        val[4 * j] = b.x; val[4 * j + 1] = b.y; val[4 * j + 2] = b.z; val[4 * j + 3] = b.w;
+      }
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < PP_ITEMS; ++i) {
+      const bool in = t0 + i < tile_n;
+      key[i] = in ? __ldcs(skey + t0 + i) : 0u;
+      if (HAS_VALS && !gen_vals) val[i] = in ? __ldcs(sval + t0 + i) : 0u;
+    }
+  }
+  if (HAS_VALS && gen_vals) {
+#pragma unroll
+    for (int i = 0; i < PP_ITEMS; ++i) val[i] = vbase + t0 + i;
+  }
+
+  // 2. thread-private counting: local rank of each item within its digit
+  uint32_t lrank[PP_ITEMS / 2];  // two 16-bit local ranks per register
+#pragma unroll
+  for (int i = 0; i < PP_ITEMS / 2; ++i) lrank[i] = 0;
+#pragma unroll
+  for (int i = 0; i < PP_ITEMS; ++i) {
+    if (t0 + i < tile_n) {
+      const uint32_t d = dig(key[i]);
+      const int w = S::pad((int)(d % S::LANES) * RS_THREADS + tid);
+      const uint32_t sh = (d / S::LANES) * 16;
+      const uint32_t old = s_cnt[w];
+      s_cnt[w] = old + (1u << sh);
+      lrank[i >> 1] |= ((old >> sh) & 0xFFFFu) << (16 * (i & 1));
+    }
+  }
+  __syncthreads();
+
+  // 3. raking scan of the packed counters in (lane, thread) word order; the
+  //    halves add without carries (a tile has fewer than 2^16 items)
+  uint32_t seg = 0;
+  uint32_t *mine = s_cnt + tid * (S::SEG + 1);
+#pragma unroll
+  for (int j = 0; j < S::SEG; ++j) seg += mine[j];
+  uint32_t total = 0;
+  const uint32_t excl = block_exclusive_scan(seg, s_warp, &total);
+  // the high halves' digits come after all low halves' digits
+  uint32_t run = excl + ((total & 0xFFFFu) << 16);
+#pragma unroll
+  for (int j = 0; j < S::SEG; ++j) {
+    const uint32_t c = mine[j];
+    mine[j] = run;
+    run += c;
+  }
+  __syncthreads();
+  // digit starts in the tile: the exclusive prefix of word (lane, thread 0)
+  if (tid < S::B) {
+    const uint32_t w = s_cnt[S::pad((tid % S::LANES) * RS_THREADS)];
+    s_dstart[tid] = (w >> ((tid / S::LANES) * 16)) & 0xFFFFu;
+  }
+  if (tid == 0) s_dstart[S::B] = tile_n;
+  __syncthreads();
+
+  // 4. publish the tile's digit counts; look back for the digits' global offsets
+  if (tid < S::B) {
+    const int d = tid;
+    const uint32_t count = s_dstart[d + 1] - s_dstart[d];
+    uint32_t *st = p.status + ((uint64_t)pass * p.tiles) * RS_RADIX + d;
+    uint32_t ex = 0;
+    if (tile == 0) {
+      pd_store_relaxed_u32(st, RS_FLAG_INC | count);
+    } else {
+      pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_AGG | count);
+      int64_t t = (int64_t)tile - 1;
+      uint32_t spins = 0;
+      const uint64_t tt0 = pd_globaltimer_ns();
+      while (t >= 0) {
+        uint32_t w[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          w[i] = (t - i >= 0) ? pd_load_relaxed_u32(st + (uint64_t)(t - i) * RS_RADIX) : RS_FLAG_INC;
+        int used = 0;
+        bool done = false, stalled = false;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          if (done || stalled) continue;
+          const uint32_t flag = w[i] & ~RS_COUNT_MASK;
+          if (flag == 0) {
+            stalled = true;
+            continue;
+          }
+          ex += w[i] & RS_COUNT_MASK;
+          ++used;
+          if (flag == RS_FLAG_INC) done = true;
+        }
+        if (done) break;
+        t -= used;
+        if (stalled) {
+          if (pd_wait_expired(p.d_error, tt0, ++spins)) break;
+          __nanosleep(spins < 8 ? 64 : 256);
+        }
+      }
+      pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_INC | ((ex + count) & RS_COUNT_MASK));
+    }
+    s_gdelta[d] = (int32_t)(p.offsets[pass * RS_RADIX + d] + ex) - (int32_t)s_dstart[d];
+  }
+
+  // 5. stage the tile in digit order
+#pragma unroll
+  for (int i = 0; i < PP_ITEMS; ++i) {
+    if (t0 + i < tile_n) {
+      const uint32_t d = dig(key[i]);
+      const uint32_t w = s_cnt[S::pad((int)(d % S::LANES) * RS_THREADS + tid)];
+      const uint32_t pos = ((w >> ((d / S::LANES) * 16)) & 0xFFFFu) +
+                           ((lrank[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
+      if (HAS_VALS) s_kv[pos] = make_uint2(key[i], val[i]);
+      else s_k[pos] = key[i];
+    }
+  }
+  __syncthreads();
+
+  // 6. each digit run written contiguously
+#pragma unroll 4
+  for (uint32_t i = tid; i < tile_n; i += RS_THREADS) {
+    const uint2 e = HAS_VALS ? s_kv[i] : make_uint2(s_k[i], 0u);
+    const uint32_t g = (uint32_t)(s_gdelta[dig(e.x)] + (int32_t)i);
+    dkey[g] = e.x;
+    if (HAS_VALS) dval[g] = e.y;
+  }
+}
+
+using PartKernel = void (*)(SortParams, uint32_t, uint32_t);
+template <int BITS>
+PartKernel pick_part_bits(bool vals, int key_mode) {
+  if (key_mode == PD_KEY_HASH0)
+    return vals ? k_part_pass<BITS, true, PD_KEY_HASH0> : k_part_pass<BITS, false, PD_KEY_HASH0>;
+  if (key_mode == PD_KEY_MULHASH)
+    return vals ? k_part_pass<BITS, true, PD_KEY_MULHASH> : k_part_pass<BITS, false, PD_KEY_MULHASH>;
+  return vals ? k_part_pass<BITS, true, PD_KEY_PLAIN> : k_part_pass<BITS, false, PD_KEY_PLAIN>;
+}
+// Digits of 1..6 bits (a 1-bit digit uses the 2-bit kernel: its upper
+// digits stay empty).
+PartKernel pick_part(uint32_t bits, bool vals, int key_mode) {
+  switch (bits) {
+    case 1: case 2: return pick_part_bits<2>(vals, key_mode);
+    case 3: return pick_part_bits<3>(vals, key_mode);
+    case 4: return pick_part_bits<4>(vals, key_mode);
+    case 5: return pick_part_bits<5>(vals, key_mode);
+    case 6: return pick_part_bits<6>(vals, key_mode);
+    default: return nullptr;
+  }
+}
+
 using PassKernel = void (*)(SortParams, uint32_t, uint32_t, uint32_t);
 PassKernel pick_pass(bool vals, int key_mode) {
   if (key_mode == PD_KEY_HASH0) return vals ? k_sort_pass<true, PD_KEY_HASH0> : k_sort_pass<false, PD_KEY_HASH0>;
@@ -619,6 +848,16 @@ int pd_sort_ex2(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode,
     pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
     unsigned cb = (unsigned)std::min<uint64_t>(pd_ceil_div(p.n, RS_THREADS), (uint64_t)ctx->sm_count * 8);
     k_sort_copy<<<cb ? cb : 1, RS_THREADS, 0, s>>>(p);
+  }
+  // A single digit of at most 6 bits over key columns (a radix partition):
+  // the small-radix pass.
+  if (l.npasses == 1 && p.end_bit - p.begin_bit <= 6 && !p.pairs) {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_PARTITION, s);
+    PartKernel k = pick_part(p.end_bit - p.begin_bit, p.has_vals != 0, key_mode);
+    const int smem = (p.has_vals ? 8 : 4) * RS_TILE;
+    PD_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k<<<(unsigned)l.tiles, RS_THREADS, smem, s>>>(p, 0, p.begin_bit);
+    return pd_launch_status(ctx);
   }
   for (uint32_t q = 0; q < l.npasses; ++q) {
     pd_launch_scope sc(ctx, PIMDAL_KERNEL_SORT_PASS, s);

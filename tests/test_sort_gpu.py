@@ -112,3 +112,25 @@ def test_sort_config2_full_size_uniform_and_zipf(ctx):
         assert np.all(r[1:][same] > r[:-1][same])
         assert np.array_equal(np.bincount(r, minlength=n), np.ones(n, np.int64))
         assert torch.equal(out, out2) and torch.equal(out_ptr, out_ptr2)
+
+
+@pytest.mark.parametrize("bits", [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize("n", [1, 5119, 5120, 5121, 300007])
+def test_single_small_digit_is_a_stable_partition(ctx, bits, n):
+    """A sort on one digit of <= 6 bits (the small-radix partition pass):
+    the stable order of the digit, rows carried, for signed and unsigned
+    keys, keys alone and with row ids, over ragged tile tails."""
+    keys = gen.generate_cpu(gen.Spec(L.GEN_UNIFORM, L.U32, seed=60 + bits, lo=0, hi=2**32 - 1), n)
+    lo = 32 - bits if bits % 2 else 11
+    for dtype in (L.U32, L.I32):
+        flip = np.uint32(0x80000000) if dtype == L.I32 else np.uint32(0)
+        digit = ((keys ^ flip) >> np.uint32(lo)) & np.uint32((1 << bits) - 1)
+        order = np.argsort(digit, kind="stable")
+        out, out_ptr = ops.sort_kernel(ctx, cuda_i32(keys), key_dtype=dtype, begin_bit=lo,
+                                       end_bit=lo + bits)
+        ko, _ = ops.sort_kernel(ctx, cuda_i32(keys), key_dtype=dtype, begin_bit=lo,
+                                end_bit=lo + bits, want_ptr=False)
+        ctx.sync()
+        assert np.array_equal(out.cpu().numpy().view(np.uint32), keys[order])
+        assert np.array_equal(out_ptr.cpu().numpy().view(np.uint32), order.astype(np.uint32))
+        assert np.array_equal(ko.cpu().numpy().view(np.uint32), keys[order])
