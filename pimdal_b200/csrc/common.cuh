@@ -451,3 +451,11 @@ int pd_sort_ex(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, 
                cudaStream_t s, uint32_t **offsets_out);
 int pd_sort_ex2(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
                 cudaStream_t s, uint32_t **offsets_out, const uint64_t *n_dev);
+// Stable radix partition of key columns by bits [a->begin_bit, a->end_bit) of
+// a key transform, in passes of at most PD_PART_DIGIT_BITS bits, carrying the
+// 32-bit column a->in_ptr -> a->out_ptr (row ids when a->in_ptr is NULL and
+// a->out_ptr is set) and/or the 64-bit column in_v64 -> out_v64.
+constexpr uint32_t PD_PART_DIGIT_BITS = 6;
+size_t pd_partition_workspace(const pimdal_sort_arguments_t *a, bool v64);
+int pd_partition(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
+                 cudaStream_t s, const uint64_t *in_v64, uint64_t *out_v64);

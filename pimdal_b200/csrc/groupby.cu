@@ -23,7 +23,18 @@
 //    lanes), so only a few lanes of one warp ever contend;
 //  - GB_SMEM (up to a few thousand groups): every row updates the CTA's
 //    shared-memory table (6144 slots, 192 KB, one 1024-thread CTA per SM);
-//  - GB_DIRECT (many groups): rows update the global table directly.  When
+//  - GB_PART (many groups): the rows (key and value) are first radix-
+//    partitioned by the top bits of a multiplicative hash of the key, in
+//    stable passes of at most 6 bits, into 2^b partitions of about 1024
+//    groups each.  Persistent CTAs then take chunks of consecutive rows (a
+//    chunk spans one or two partitions), aggregate each chunk in the
+//    shared-memory table and flush the slots it claimed into the global
+//    table -- about one global merge per group instead of global atomics
+//    per row.  This is the single-pass form of the reference's spill rounds
+//    (aggregate_hash.c:145-188), which re-aggregate the rows that did not
+//    fit the DPU's table;
+//  - GB_DIRECT (the batched form's many-group instances, or
+//    PIMDAL_GROUP_DIRECT=1): rows update the global table directly.  When
 //    the table is larger than an L2 budget it can be split into K sub-tables
 //    by the high hash bits and aggregated in K launches, each touching an
 //    L2-sized sub-table (PIMDAL_GROUP_L2_BUDGET_MB; one pass by default).
@@ -53,7 +64,9 @@ constexpr size_t GB_SMEM_BYTES = 32ull * GB_SMEM_SLOTS;      // 192 KB
 constexpr uint64_t GB_WARP_MAX_GROUPS = 64;                  // GB_WARP at or below
 constexpr uint64_t GB_SMEM_MAX_GROUPS = 4608;                // GB_SMEM at or below (load 3/4)
 constexpr uint64_t GB_L2_BUDGET = 1ull << 40;                // one pass unless overridden
-enum { GB_WARP = 0, GB_SMEM = 1, GB_DIRECT = 2 };
+enum { GB_WARP = 0, GB_SMEM = 1, GB_DIRECT = 2, GB_PART = 3 };
+constexpr uint64_t GB_PART_GROUPS = 1024;   // groups per hash partition
+constexpr uint32_t GB_PART_MAX_BITS = 12;
 
 struct GbParams {
   const uint32_t *key;
@@ -342,6 +355,49 @@ k_gb_aggregate(GbParams p, uint32_t pass) {
       if (k != GB_EMPTY)
         global_add(p, k, gb_h(k), 0, t.cnt[i], t.sum[i], t.mm[i].x, t.mm[i].y);
     }
+  }
+}
+
+// GB_PART: rows grouped by a hash digit.  Persistent CTAs claim chunks of
+// `chunk` consecutive rows; a chunk goes through the shared table and the
+// slots it claimed are flushed to the global table and reset.
+__global__ void __launch_bounds__(GB_THREADS, 1) k_gb_chunks(GbParams p, uint64_t chunk,
+                                                             uint32_t *claim) {
+  extern __shared__ __align__(16) unsigned char gb_smem[];
+  __shared__ uint32_t s_item, s_nlist;
+  SmemTable t = gb_smem_table(gb_smem);
+  t.list = reinterpret_cast<uint16_t *>(gb_smem + GB_SMEM_BYTES);
+  t.nlist = &s_nlist;
+  for (uint32_t i = threadIdx.x; i < GB_SMEM_SLOTS; i += GB_THREADS) gb_clear_slot(t, i);
+  if (threadIdx.x == 0) s_nlist = 0;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = threadIdx.x >> 5;
+  const uint64_t nchunks = pd_ceil_div(p.n, chunk);
+  while (true) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const uint32_t it = atomicAdd(claim, 1u);
+      if (it >= nchunks && atomicAdd(claim + 1, 1u) == gridDim.x - 1) {
+        claim[0] = 0;  // the last claimer of the launch resets the counters
+        claim[1] = 0;
+      }
+      s_item = it;
+    }
+    __syncthreads();
+    const uint64_t it = s_item;
+    if (it >= nchunks) break;
+    const uint64_t r0 = it * chunk, r1 = min(r0 + chunk, p.n);
+    gb_range<GB_SMEM>(p, t, 0, r0, r1, warp, GB_WARPS, lane, 0, GB_SMEM_SLOTS / 4);
+    __syncthreads();
+    const uint32_t nl = s_nlist;
+    for (uint32_t i = threadIdx.x; i < nl; i += GB_THREADS) {
+      const uint32_t j = t.list[i];
+      const uint32_t k = t.key[j];
+      global_add(p, k, gb_h(k), 0, t.cnt[j], t.sum[j], t.mm[j].x, t.mm[j].y);
+      gb_clear_slot(t, j);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) s_nlist = 0;
   }
 }
 
@@ -837,8 +893,29 @@ __global__ void __launch_bounds__(SR_THREADS) k_gb_segreduce(SegParams p) {
 struct GbLayout {
   int mode;
   uint32_t sub_cap, npasses, wrep;
-  size_t gtab, ngroups, ckey, cslot, skey, sslot, sort_ws, total;
+  uint32_t part_bits;   // GB_PART: hash partitions 2^part_bits
+  size_t gtab, ngroups, ckey, cslot, skey, sslot, sort_ws, pkey, pval, total;
 };
+
+bool gb_force_direct() {
+  static const bool d = [] {
+    const char *e = getenv("PIMDAL_GROUP_DIRECT");
+    return e && atoi(e) != 0;
+  }();
+  return d;
+}
+
+// The partition request of GB_PART (keys only; the values travel as 64-bit
+// words beside them).
+pimdal_sort_arguments_t gb_part_args(const pimdal_aggr_arguments_t *a, uint32_t bits) {
+  pimdal_sort_arguments_t sa{};
+  sa.nr_elements = a->size;
+  sa.key_dtype = PIMDAL_U32;
+  sa.layout = PIMDAL_LAYOUT_COLUMNS;
+  sa.begin_bit = 32 - bits;
+  sa.end_bit = 32;
+  return sa;
+}
 
 // Bytes of one global sub-table (an L2-sized slice of the table that one
 // aggregation launch updates); PIMDAL_GROUP_L2_BUDGET_MB overrides it.
@@ -870,11 +947,19 @@ bool gb_layout(const pimdal_aggr_arguments_t *a, GbLayout *l) {
   }
   uint64_t expect = a->expected_groups ? a->expected_groups : std::min<uint64_t>(a->size, 1ull << 22);
   expect = std::max<uint64_t>(expect, 1);
-  l->mode = expect <= GB_WARP_MAX_GROUPS ? GB_WARP : expect <= GB_SMEM_MAX_GROUPS ? GB_SMEM : GB_DIRECT;
+  l->mode = expect <= GB_WARP_MAX_GROUPS ? GB_WARP : expect <= GB_SMEM_MAX_GROUPS ? GB_SMEM
+          : gb_force_direct() ? GB_DIRECT : GB_PART;
+  l->part_bits = 0;
+  l->pkey = l->pval = 0;
+  if (l->mode == GB_PART) {
+    uint32_t b = 1;
+    while (b < GB_PART_MAX_BITS && (expect >> b) > GB_PART_GROUPS) ++b;
+    l->part_bits = b;
+  }
   // GB_WARP replicas: keep each replica's load at or below 1/3
   l->wrep = expect <= 16 ? 4 : expect <= 32 ? 2 : 1;
   // load factor 1/2 for the small tables, 3/4 for the large ones
-  uint64_t slots = l->mode == GB_DIRECT ? expect + expect / 3 + 1 : 2 * expect;
+  uint64_t slots = l->mode >= GB_DIRECT ? expect + expect / 3 + 1 : 2 * expect;
   slots = std::max<uint64_t>(slots, 2048);
   if (slots >= (1ull << 31)) return false;
   uint64_t np = 1;
@@ -890,6 +975,15 @@ bool gb_layout(const pimdal_aggr_arguments_t *a, GbLayout *l) {
   l->sslot = o; o += pd_align_up(4 * cap, 256);
   sa.nr_elements = cap;
   if (pimdal_sort_workspace_size(&sa, &w)) return false;
+  if (l->mode == GB_PART) {
+    // the partition's scratch and the final sort's run one after the other
+    const pimdal_sort_arguments_t pa = gb_part_args(a, l->part_bits);
+    const size_t pw = pd_partition_workspace(&pa, a->in_val != nullptr);
+    if (!pw) return false;
+    w = std::max(w, pw);
+    l->pkey = o; o += pd_align_up(4 * a->size, 256);
+    if (a->in_val) { l->pval = o; o += pd_align_up(8 * a->size, 256); }
+  }
   l->sort_ws = o; o += w;
   l->total = o;
   return true;
@@ -1049,7 +1143,26 @@ extern "C" int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_argument
     k_gb_init<<<init_grid, 256, 0, s>>>(p);
   }
   const uint64_t want = pd_ceil_div(a->size, (uint64_t)GB_THREADS * 4);
-  if (l.mode == GB_DIRECT) {
+  if (l.mode == GB_PART) {
+    // rows grouped by the top part_bits of the key's multiplicative hash
+    pimdal_sort_arguments_t pa = gb_part_args(a, l.part_bits);
+    pa.in = a->in;
+    pa.out = ws + l.pkey;
+    int64_t *pval = a->in_val ? (int64_t *)(ws + l.pval) : nullptr;
+    if ((st = pd_partition(ctx, &pa, PD_KEY_MULHASH, ws + l.sort_ws, s, (const uint64_t *)a->in_val,
+                           (uint64_t *)pval)))
+      return st;
+    p.key = (const uint32_t *)(ws + l.pkey);
+    p.val = pval;
+    p.vec = 1;
+    // a chunk holds about one partition's rows, so about GB_PART_GROUPS groups
+    const uint64_t chunk = std::max<uint64_t>(4096, pd_align_up(a->size >> l.part_bits, 1024));
+    const unsigned grid = (unsigned)std::min<uint64_t>(pd_ceil_div(a->size, chunk), ctx->sm_count);
+    const size_t smem = pd_gb_batch_shared_bytes();
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_GROUP, s);
+    PD_CHECK_CUDA(cudaFuncSetAttribute(k_gb_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_gb_chunks<<<grid ? grid : 1, GB_THREADS, smem, s>>>(p, chunk, ctx->d_counters + PD_COUNTER_GROUP);
+  } else if (l.mode == GB_DIRECT) {
     const unsigned grid = (unsigned)std::min<uint64_t>(want, (uint64_t)ctx->sm_count * 2);
     for (uint32_t q = 0; q < l.npasses; ++q) {
       pd_launch_scope sc(ctx, PIMDAL_KERNEL_GROUP, s);

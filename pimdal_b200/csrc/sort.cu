@@ -77,6 +77,10 @@ struct SortParams {
   void *out;
   uint32_t *out_ptr;
   uint32_t *alt_key, *alt_ptr;
+  // 64-bit values carried beside the keys (the small-radix pass only)
+  const unsigned long long *in_v64;
+  unsigned long long *out_v64, *alt_v64;
+  uint32_t dbits;       // digit width of every pass (8; at most 6 for partitions)
   uint64_t n;           // element count (upper bound when n_dev is set)
   const uint64_t *n_dev;  // device-resident element count, or NULL
   uint32_t flip;        // 0x80000000 for signed keys
@@ -117,8 +121,8 @@ __global__ void __launch_bounds__(RS_THREADS) k_sort_hist(SortParams p) {
   uint32_t shift[RS_MAX_PASSES], mask[RS_MAX_PASSES];
 #pragma unroll
   for (int q = 0; q < RS_MAX_PASSES; ++q) {
-    shift[q] = min(31u, p.begin_bit + q * RS_RADIX_BITS);
-    uint32_t bits = q < (int)p.npasses ? min((uint32_t)RS_RADIX_BITS, p.end_bit - shift[q]) : 0u;
+    shift[q] = min(31u, p.begin_bit + q * p.dbits);
+    uint32_t bits = q < (int)p.npasses ? min(p.dbits, p.end_bit - shift[q]) : 0u;
     mask[q] = (1u << bits) - 1u;
   }
   __syncthreads();
@@ -235,6 +239,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_sort_copy(SortParams p) {
     else {
       reinterpret_cast<uint32_t *>(p.out)[i] = k;
       if (p.has_vals) p.out_ptr[i] = v;
+      if (p.out_v64) p.out_v64[i] = p.in_v64[i];
     }
   }
 }
@@ -538,11 +543,16 @@ struct PartShape {
   static __device__ __forceinline__ int pad(int e) { return e + e / SEG; }
 };
 
-template <int BITS, bool HAS_VALS, int KEY_MODE>
-__global__ void __launch_bounds__(RS_THREADS, 3)
+enum : int { PV_NONE = 0, PV_U32 = 1, PV_U64 = 2 };  // values carried by the pass
+
+template <int BITS, int VAL, int KEY_MODE>
+__global__ void __launch_bounds__(RS_THREADS, VAL == PV_U64 ? 2 : 3)
 k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
   using S = PartShape<BITS>;
-  extern __shared__ __align__(16) uint2 pp_stage[];  // RS_TILE (key, value) words or keys
+  constexpr bool HAS_VALS = VAL == PV_U32;
+  constexpr bool V64 = VAL == PV_U64;
+  // staging: RS_TILE (key, value) words, keys alone, or keys then 64-bit values
+  extern __shared__ __align__(16) uint2 pp_stage[];
   __shared__ uint32_t s_cnt[S::WORDS];
   __shared__ uint32_t s_warp[RS_WARPS];
   __shared__ uint32_t s_dstart[S::B + 1];
@@ -550,6 +560,7 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
   __shared__ uint32_t s_tile;
   uint2 *s_kv = pp_stage;
   uint32_t *s_k = reinterpret_cast<uint32_t *>(pp_stage);
+  unsigned long long *s_v64 = reinterpret_cast<unsigned long long *>(s_k + RS_TILE);
 
   const SortPlan *plan = p.plan;
   if (!plan->active[pass]) return;
@@ -579,11 +590,16 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
   uint32_t *dval = dst == BUF_OUT ? p.out_ptr : p.alt_ptr;
   const bool gen_vals = first && src == BUF_IN && p.in_ptr == nullptr;
   const uint32_t vbase = (uint32_t)(p.ptr_base + base);
-  const bool vec = ((reinterpret_cast<uintptr_t>(skey) | reinterpret_cast<uintptr_t>(sval)) & 15u) == 0;
+  const unsigned long long *sv64 =
+      (src == BUF_IN ? p.in_v64 : src == BUF_OUT ? p.out_v64 : p.alt_v64) + (V64 ? base : 0);
+  unsigned long long *dv64 = dst == BUF_OUT ? p.out_v64 : p.alt_v64;
+  const bool vec = ((reinterpret_cast<uintptr_t>(skey) | reinterpret_cast<uintptr_t>(sval) |
+                     (V64 ? reinterpret_cast<uintptr_t>(sv64) : 0)) & 15u) == 0;
 
   // 1. load this thread's consecutive items
   uint32_t key[PP_ITEMS];
   uint32_t val[HAS_VALS ? PP_ITEMS : 1];
+  unsigned long long v64[V64 ? PP_ITEMS : 1];
   if (vec && t0 + PP_ITEMS <= tile_n) {
 #pragma unroll
     for (int j = 0; j < PP_ITEMS / 4; ++j) {
@@ -593,6 +609,11 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
         const uint4 b = __ldcs(reinterpret_cast<const uint4 *>(sval + t0) + j);
         val[4 * j] = b.x; val[4 * j + 1] = b.y; val[4 * j + 2] = b.z; val[4 * j + 3] = b.w;
       }
+      if (V64) {
+        const ulonglong2 b = __ldcs(reinterpret_cast<const ulonglong2 *>(sv64 + t0) + 2 * j);
+        const ulonglong2 c = __ldcs(reinterpret_cast<const ulonglong2 *>(sv64 + t0) + 2 * j + 1);
+        v64[4 * j] = b.x; v64[4 * j + 1] = b.y; v64[4 * j + 2] = c.x; v64[4 * j + 3] = c.y;
+      }
     }
   } else {
 #pragma unroll
@@ -600,6 +621,7 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
       const bool in = t0 + i < tile_n;
       key[i] = in ? __ldcs(skey + t0 + i) : 0u;
       if (HAS_VALS && !gen_vals) val[i] = in ? __ldcs(sval + t0 + i) : 0u;
+      if (V64) v64[i] = in ? __ldcs(sv64 + t0 + i) : 0ull;
     }
   }
   if (HAS_VALS && gen_vals) {
@@ -703,6 +725,7 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
                            ((lrank[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
       if (HAS_VALS) s_kv[pos] = make_uint2(key[i], val[i]);
       else s_k[pos] = key[i];
+      if (V64) s_v64[pos] = v64[i];
     }
   }
   __syncthreads();
@@ -714,27 +737,32 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
     const uint32_t g = (uint32_t)(s_gdelta[dig(e.x)] + (int32_t)i);
     dkey[g] = e.x;
     if (HAS_VALS) dval[g] = e.y;
+    if (V64) dv64[g] = s_v64[i];
   }
 }
 
 using PartKernel = void (*)(SortParams, uint32_t, uint32_t);
+template <int BITS, int VAL>
+PartKernel pick_part_mode(int key_mode) {
+  if (key_mode == PD_KEY_HASH0) return k_part_pass<BITS, VAL, PD_KEY_HASH0>;
+  if (key_mode == PD_KEY_MULHASH) return k_part_pass<BITS, VAL, PD_KEY_MULHASH>;
+  return k_part_pass<BITS, VAL, PD_KEY_PLAIN>;
+}
 template <int BITS>
-PartKernel pick_part_bits(bool vals, int key_mode) {
-  if (key_mode == PD_KEY_HASH0)
-    return vals ? k_part_pass<BITS, true, PD_KEY_HASH0> : k_part_pass<BITS, false, PD_KEY_HASH0>;
-  if (key_mode == PD_KEY_MULHASH)
-    return vals ? k_part_pass<BITS, true, PD_KEY_MULHASH> : k_part_pass<BITS, false, PD_KEY_MULHASH>;
-  return vals ? k_part_pass<BITS, true, PD_KEY_PLAIN> : k_part_pass<BITS, false, PD_KEY_PLAIN>;
+PartKernel pick_part_bits(int val, int key_mode) {
+  if (val == PV_U64) return pick_part_mode<BITS, PV_U64>(key_mode);
+  if (val == PV_U32) return pick_part_mode<BITS, PV_U32>(key_mode);
+  return pick_part_mode<BITS, PV_NONE>(key_mode);
 }
 // Digits of 1..6 bits (a 1-bit digit uses the 2-bit kernel: its upper
 // digits stay empty).
-PartKernel pick_part(uint32_t bits, bool vals, int key_mode) {
+PartKernel pick_part(uint32_t bits, int val, int key_mode) {
   switch (bits) {
-    case 1: case 2: return pick_part_bits<2>(vals, key_mode);
-    case 3: return pick_part_bits<3>(vals, key_mode);
-    case 4: return pick_part_bits<4>(vals, key_mode);
-    case 5: return pick_part_bits<5>(vals, key_mode);
-    case 6: return pick_part_bits<6>(vals, key_mode);
+    case 1: case 2: return pick_part_bits<2>(val, key_mode);
+    case 3: return pick_part_bits<3>(val, key_mode);
+    case 4: return pick_part_bits<4>(val, key_mode);
+    case 5: return pick_part_bits<5>(val, key_mode);
+    case 6: return pick_part_bits<6>(val, key_mode);
     default: return nullptr;
   }
 }
@@ -749,15 +777,19 @@ PassKernel pick_pass(bool vals, int key_mode) {
 
 struct SortLayout {
   size_t off_counters, off_hist, off_offsets, off_plan, off_status, off_alt_key, off_alt_ptr,
-      total, memset_bytes;
+      off_alt_v64, total, memset_bytes;
   uint64_t tiles;
   uint32_t npasses;
 };
 
-bool sort_layout(const pimdal_sort_arguments_t *a, SortLayout *l) {
+// dbits: digit width of each pass (8 for a sort; at most 6 for a partition,
+// which may also carry 64-bit values, v64).
+bool sort_layout(const pimdal_sort_arguments_t *a, SortLayout *l, uint32_t dbits = RS_RADIX_BITS,
+                 bool v64 = false) {
   uint32_t b = a->begin_bit, e = a->end_bit ? a->end_bit : 32;
-  if (b >= e || e > 32) return false;
-  l->npasses = (e - b + RS_RADIX_BITS - 1) / RS_RADIX_BITS;
+  if (b >= e || e > 32 || dbits == 0 || dbits > RS_RADIX_BITS) return false;
+  l->npasses = (e - b + dbits - 1) / dbits;
+  if (l->npasses > RS_MAX_PASSES) return false;
   l->tiles = pd_ceil_div(a->nr_elements ? a->nr_elements : 1, RS_TILE);
   size_t o = 0;
   l->off_counters = o; o += 256;
@@ -768,6 +800,7 @@ bool sort_layout(const pimdal_sort_arguments_t *a, SortLayout *l) {
   l->off_plan = o; o += 256;
   l->off_alt_key = o; o += pd_align_up(sizeof(uint32_t) * a->nr_elements, 256);
   l->off_alt_ptr = o; o += pd_align_up(sizeof(uint32_t) * a->nr_elements, 256);
+  l->off_alt_v64 = o; o += v64 ? pd_align_up(8 * a->nr_elements, 256) : 0;
   l->total = o;
   return true;
 }
@@ -797,12 +830,41 @@ int pd_sort_ex(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, 
   return pd_sort_ex2(ctx, a, key_mode, ws, s, offsets_out, nullptr);
 }
 
+namespace {
+int pd_sort_core(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
+                 cudaStream_t s, uint32_t **offsets_out, const uint64_t *n_dev, uint32_t dbits,
+                 const uint64_t *in_v64, uint64_t *out_v64);
+}
+
 // Same, with the element count read on the device from *n_dev (a->nr_elements
 // is then an upper bound that sizes the workspace and the grids).
 int pd_sort_ex2(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
                 cudaStream_t s, uint32_t **offsets_out, const uint64_t *n_dev) {
+  return pd_sort_core(ctx, a, key_mode, ws, s, offsets_out, n_dev, RS_RADIX_BITS, nullptr, nullptr);
+}
+
+// A stable radix partition of key columns by bits [begin_bit, end_bit) of a
+// key transform, in passes of at most PD_PART_DIGIT_BITS bits, carrying a
+// 32-bit value column (in_ptr/out_ptr) and/or a 64-bit one (in_v64/out_v64).
+size_t pd_partition_workspace(const pimdal_sort_arguments_t *a, bool v64) {
   SortLayout l;
-  if (!sort_layout(a, &l)) return PIMDAL_ERR_ARG;
+  return sort_layout(a, &l, PD_PART_DIGIT_BITS, v64) ? l.total : 0;
+}
+int pd_partition(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
+                 cudaStream_t s, const uint64_t *in_v64, uint64_t *out_v64) {
+  if (a->layout != PIMDAL_LAYOUT_COLUMNS || (in_v64 == nullptr) != (out_v64 == nullptr))
+    return PIMDAL_ERR_ARG;
+  return pd_sort_core(ctx, a, key_mode, ws, s, nullptr, nullptr, PD_PART_DIGIT_BITS, in_v64, out_v64);
+}
+
+namespace {
+int pd_sort_core(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
+                 cudaStream_t s, uint32_t **offsets_out, const uint64_t *n_dev, uint32_t dbits,
+                 const uint64_t *in_v64, uint64_t *out_v64) {
+  SortLayout l;
+  const bool v64 = out_v64 != nullptr;
+  if (!sort_layout(a, &l, dbits, v64)) return PIMDAL_ERR_ARG;
+  if (v64 && dbits > 6) return PIMDAL_ERR_ARG;  // only the small-radix pass carries them
   if (offsets_out) *offsets_out = (uint32_t *)((char *)ws + l.off_offsets);
   if (a->nr_elements > RS_COUNT_MASK) return PIMDAL_ERR_ARG;  // < 2^30 elements
   char *w = (char *)ws;
@@ -816,6 +878,10 @@ int pd_sort_ex2(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode,
   p.has_vals = p.pairs || p.out_ptr != nullptr;
   p.alt_key = (uint32_t *)(w + l.off_alt_key);
   p.alt_ptr = (uint32_t *)(w + l.off_alt_ptr);
+  p.in_v64 = (const unsigned long long *)in_v64;
+  p.out_v64 = (unsigned long long *)out_v64;
+  p.alt_v64 = v64 ? (unsigned long long *)(w + l.off_alt_v64) : nullptr;
+  p.dbits = dbits;
   p.n = a->nr_elements;
   p.n_dev = n_dev;
   p.flip = a->key_dtype == PIMDAL_I32 ? 0x80000000u : 0u;
@@ -849,14 +915,18 @@ int pd_sort_ex2(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode,
     unsigned cb = (unsigned)std::min<uint64_t>(pd_ceil_div(p.n, RS_THREADS), (uint64_t)ctx->sm_count * 8);
     k_sort_copy<<<cb ? cb : 1, RS_THREADS, 0, s>>>(p);
   }
-  // A single digit of at most 6 bits over key columns (a radix partition):
-  // the small-radix pass.
-  if (l.npasses == 1 && p.end_bit - p.begin_bit <= 6 && !p.pairs) {
-    pd_launch_scope sc(ctx, PIMDAL_KERNEL_PARTITION, s);
-    PartKernel k = pick_part(p.end_bit - p.begin_bit, p.has_vals != 0, key_mode);
-    const int smem = (p.has_vals ? 8 : 4) * RS_TILE;
-    PD_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    k<<<(unsigned)l.tiles, RS_THREADS, smem, s>>>(p, 0, p.begin_bit);
+  // Digits of at most 6 bits over key columns (a radix partition, or a sort
+  // on a single small digit): the small-radix pass.
+  if ((dbits <= 6 || (l.npasses == 1 && p.end_bit - p.begin_bit <= 6)) && !p.pairs) {
+    const int val = v64 ? PV_U64 : p.has_vals ? PV_U32 : PV_NONE;
+    const int smem = (v64 ? 12 : p.has_vals ? 8 : 4) * RS_TILE;
+    for (uint32_t q = 0; q < l.npasses; ++q) {
+      pd_launch_scope sc(ctx, PIMDAL_KERNEL_PARTITION, s);
+      const uint32_t shift = p.begin_bit + q * dbits;
+      PartKernel k = pick_part(std::min(dbits, p.end_bit - shift), val, key_mode);
+      PD_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      k<<<(unsigned)l.tiles, RS_THREADS, smem, s>>>(p, q, shift);
+    }
     return pd_launch_status(ctx);
   }
   for (uint32_t q = 0; q < l.npasses; ++q) {
@@ -871,6 +941,7 @@ int pd_sort_ex2(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode,
   }
   return pd_launch_status(ctx);
 }
+}  // namespace
 
 extern "C" int pimdal_sort_kernel(pimdal_ctx_t *ctx, const pimdal_sort_arguments_t *a,
                                   pimdal_stream_t stream) {

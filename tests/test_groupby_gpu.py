@@ -100,3 +100,25 @@ def test_group_by_all_ones_key_in_every_table_mode(ctx, expected):
     k, v = inputs(20000, min(expected, 8), 55)
     k[::3] = -1
     check(run(ctx, k, v, L.GROUP_HASH, expected=expected), oracle.group_by(k, v))
+
+
+@pytest.mark.parametrize("card,expected", [(1 << 13, 1 << 13), (1 << 15, 1 << 15),
+                                           (1 << 18, 1 << 18), (1 << 18, 1 << 20)])
+def test_partitioned_hash_group_by(ctx, card, expected):
+    """Many groups: rows radix-partitioned by a key hash, chunks aggregated in
+    shared memory.  Heavy hitters (a third of the rows on a few keys), the
+    all-ones key, int32 extremes, unsigned order and count-only, against the
+    oracle; partition counts from one pass (<= 6 bits) to two."""
+    n = (1 << 21) + 77
+    k, v = inputs(n, card, 54)
+    k[::3] = np.array([7, -1, 123456789], np.int32)[np.arange(k[::3].size) % 3]
+    k[::101] = np.iinfo(np.int32).min
+    k[::103] = np.iinfo(np.int32).max
+    v[::5] = -3 * 10**13
+    exp = oracle.group_by(k, v)
+    check(run(ctx, k, v, L.GROUP_HASH, expected=expected), exp)
+    check(run(ctx, k, None, L.GROUP_HASH, expected=expected), oracle.group_by(k, None))
+    got = run(ctx, k, v, L.GROUP_HASH, expected=expected, key_dtype=L.U32)
+    o = np.argsort(exp[0].view(np.uint32), kind="stable")
+    for name, a, b in zip(("key", "sum", "count", "min", "max"), got, exp):
+        assert np.array_equal(a, b[o]), name
