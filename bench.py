@@ -1019,7 +1019,8 @@ def _kernel_split(ctx, fn, iters=3) -> dict:
     """Mean device milliseconds per call of each library kernel class (the
     library's own CUDA events on the launching stream)."""
     from pimdal_b200 import _lib as L
-    names = {getattr(L, k): k[len("KERNEL_"):].lower() for k in dir(L) if k.startswith("KERNEL_")}
+    names = {getattr(L, k): k[len("KERNEL_"):].lower() for k in dir(L)
+             if k.startswith("KERNEL_") and k != "KERNEL_COUNT"}
     for k in names:
         ctx.kernel_time(k)
     ctx.set_profiling(True)

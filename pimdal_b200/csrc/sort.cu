@@ -252,6 +252,50 @@ __device__ __forceinline__ uint32_t sort_xform(uint32_t k, uint32_t flip) {
   return k ^ flip;
 }
 
+// Decoupled look-back of one digit: the sum of the digit's counts in tiles
+// before `tile`, read RS_LOOKBACK predecessor words per round (independent
+// relaxed loads -- every word carries its own count, nothing else is read),
+// then this tile's inclusive count published.  `st` is the digit's status
+// word of tile 0; `count` is the tile's own count.  A wait that gives up
+// sets the timeout bit and publishes what it has (the pass is then reported
+// as failed).
+constexpr int RS_LOOKBACK = 8;
+__device__ __forceinline__ uint32_t rs_lookback(uint32_t *st, uint64_t tile, uint32_t count,
+                                                uint32_t *d_error) {
+  uint32_t excl = 0;
+  int64_t t = (int64_t)tile - 1;
+  uint32_t spins = 0;
+  const uint64_t t0 = pd_globaltimer_ns();
+  while (t >= 0) {
+    uint32_t w[RS_LOOKBACK];
+#pragma unroll
+    for (int i = 0; i < RS_LOOKBACK; ++i)
+      w[i] = (t - i >= 0) ? pd_load_relaxed_u32(st + (uint64_t)(t - i) * RS_RADIX) : RS_FLAG_INC;
+    int used = 0;
+    bool done = false, stalled = false;
+#pragma unroll
+    for (int i = 0; i < RS_LOOKBACK; ++i) {
+      if (done || stalled) continue;
+      const uint32_t flag = w[i] & ~RS_COUNT_MASK;
+      if (flag == 0) {
+        stalled = true;
+        continue;
+      }
+      excl += w[i] & RS_COUNT_MASK;
+      ++used;
+      if (flag == RS_FLAG_INC) done = true;
+    }
+    if (done) break;
+    t -= used;
+    if (stalled) {
+      if (pd_wait_expired(d_error, t0, ++spins)) break;
+      __nanosleep(spins < 8 ? 64 : 256);
+    }
+  }
+  pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_INC | ((excl + count) & RS_COUNT_MASK));
+  return excl;
+}
+
 // Lanes of `members` whose digit equals this lane's: one ballot per digit
 // bit.  For 8-bit labels this is cheaper than the match.any instruction.
 __device__ __forceinline__ unsigned match_digit(uint32_t d, unsigned members) {
@@ -367,6 +411,10 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   // running counter, so the ranking below yields staged positions
 #pragma unroll
   for (int w = 0; w < RS_WARPS; ++w) s_wcnt[w][d] = (uint16_t)(s_whist[w][d] + dstart);
+  // The digit's global offset: looked back for now, before the ranking, so
+  // this tile's inclusive count reaches its successors as early as possible.
+  const uint32_t excl = tile > 0 ? rs_lookback(st, tile, count, p.d_error) : 0u;
+  s_gdelta[d] = (int32_t)(p.offsets[pass * RS_RADIX + d] + excl) - (int32_t)dstart;
   __syncthreads();
 
   // Warp-level stable ranking: the lanes of one digit are grouped, and the
@@ -440,44 +488,6 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
       __syncwarp();
     }
   }
-  __syncthreads();
-
-  // Look-back for digit d: four predecessor words per step (independent
-  // relaxed loads -- every word carries its own count, nothing else is read).
-  uint32_t excl = 0;
-  if (tile > 0) {
-    int64_t t = (int64_t)tile - 1;
-    uint32_t spins = 0;
-    const uint64_t t0 = pd_globaltimer_ns();
-    while (t >= 0) {
-      uint32_t w[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i)
-        w[i] = (t - i >= 0) ? pd_load_relaxed_u32(st + (uint64_t)(t - i) * RS_RADIX) : RS_FLAG_INC;
-      int used = 0;
-      bool done = false, stalled = false;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        if (done || stalled) continue;
-        const uint32_t flag = w[i] & ~RS_COUNT_MASK;
-        if (flag == 0) {
-          stalled = true;
-          continue;
-        }
-        excl += w[i] & RS_COUNT_MASK;
-        ++used;
-        if (flag == RS_FLAG_INC) done = true;
-      }
-      if (done) break;
-      t -= used;
-      if (stalled) {
-        if (pd_wait_expired(p.d_error, t0, ++spins)) break;
-        __nanosleep(spins < 8 ? 64 : 256);
-      }
-    }
-    pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_INC | ((excl + count) & RS_COUNT_MASK));
-  }
-  s_gdelta[d] = (int32_t)(p.offsets[pass * RS_RADIX + d] + excl) - (int32_t)dstart;
   __syncthreads();
 
   // Stage the tile in digit order.
@@ -681,36 +691,7 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
       pd_store_relaxed_u32(st, RS_FLAG_INC | count);
     } else {
       pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_AGG | count);
-      int64_t t = (int64_t)tile - 1;
-      uint32_t spins = 0;
-      const uint64_t tt0 = pd_globaltimer_ns();
-      while (t >= 0) {
-        uint32_t w[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i)
-          w[i] = (t - i >= 0) ? pd_load_relaxed_u32(st + (uint64_t)(t - i) * RS_RADIX) : RS_FLAG_INC;
-        int used = 0;
-        bool done = false, stalled = false;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          if (done || stalled) continue;
-          const uint32_t flag = w[i] & ~RS_COUNT_MASK;
-          if (flag == 0) {
-            stalled = true;
-            continue;
-          }
-          ex += w[i] & RS_COUNT_MASK;
-          ++used;
-          if (flag == RS_FLAG_INC) done = true;
-        }
-        if (done) break;
-        t -= used;
-        if (stalled) {
-          if (pd_wait_expired(p.d_error, tt0, ++spins)) break;
-          __nanosleep(spins < 8 ? 64 : 256);
-        }
-      }
-      pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_INC | ((ex + count) & RS_COUNT_MASK));
+      ex = rs_lookback(st, tile, count, p.d_error);
     }
     s_gdelta[d] = (int32_t)(p.offsets[pass * RS_RADIX + d] + ex) - (int32_t)s_dstart[d];
   }

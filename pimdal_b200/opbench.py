@@ -145,7 +145,8 @@ def main(argv=None) -> None:
         run()
     ctx.sync()
     stream = torch.cuda.current_stream()
-    names = {getattr(L, k): k[len("KERNEL_"):].lower() for k in dir(L) if k.startswith("KERNEL_")}
+    names = {getattr(L, k): k[len("KERNEL_"):].lower() for k in dir(L)
+             if k.startswith("KERNEL_") and k != "KERNEL_COUNT"}
     if a.kernels:
         for k in names:
             ctx.kernel_time(k)  # reset

@@ -103,3 +103,8 @@ def test_tpch_packed_dates_follow_the_reference_reader():
     assert tpch.packed("1994-01-01") == 1 + (1 << 5) + (94 << 9)
     assert tpch.packed("1998-09-02") == 2 + (9 << 5) + (98 << 9)
     assert tpch.packed(tpch.Q6_DATE_LO) < tpch.packed(tpch.Q6_DATE_HI)
+
+
+def test_kernel_ids_cover_the_count():
+    ids = sorted(getattr(L, k) for k in dir(L) if k.startswith("KERNEL_") and k != "KERNEL_COUNT")
+    assert ids == list(range(L.KERNEL_COUNT))
