@@ -28,7 +28,13 @@
 namespace {
 
 constexpr int SA_THREADS = 256;
-constexpr int SA_UNROLL = 4;
+#ifndef PD_SA_UNROLL
+#define PD_SA_UNROLL 4  // rows per thread per step
+#endif
+#ifndef PD_SA_EAGER
+#define PD_SA_EAGER 0   // 1: predicate columns read for every row, not only the selected ones
+#endif
+constexpr int SA_UNROLL = PD_SA_UNROLL;
 constexpr uint32_t SA_PRIVATE_BYTES = 96 * 1024;  // per-thread slots up to this much shared memory
 
 struct SaCol {
@@ -89,11 +95,12 @@ __global__ void __launch_bounds__(SA_THREADS) k_sa_scan(SaParams p) {
   const uint64_t step = (uint64_t)gridDim.x * SA_THREADS * SA_UNROLL;
   for (uint64_t base = (uint64_t)blockIdx.x * SA_THREADS * SA_UNROLL; base < p.n; base += step) {
     uint32_t row[SA_UNROLL];
-    bool ok[SA_UNROLL];
+    bool ok[SA_UNROLL], valid[SA_UNROLL];
 #pragma unroll
     for (int u = 0; u < SA_UNROLL; ++u) {
       const uint64_t i = base + (uint64_t)u * SA_THREADS + tid;
-      ok[u] = i < p.n;
+      valid[u] = i < p.n;
+      ok[u] = valid[u];
       row[u] = ok[u] ? (p.rows ? __ldg(p.rows + i) : (uint32_t)i) : 0u;
     }
     // predicates in order; a column is read only for rows still selected
@@ -102,7 +109,8 @@ __global__ void __launch_bounds__(SA_THREADS) k_sa_scan(SaParams p) {
       if (q < (int)p.npreds) {
         int64_t v[SA_UNROLL];
 #pragma unroll
-        for (int u = 0; u < SA_UNROLL; ++u) v[u] = ok[u] ? sa_load(p.pc[q], row[u]) : 0;
+        for (int u = 0; u < SA_UNROLL; ++u)
+          v[u] = (PD_SA_EAGER ? valid[u] : ok[u]) ? sa_load(p.pc[q], row[u]) : 0;
 #pragma unroll
         for (int u = 0; u < SA_UNROLL; ++u)
           ok[u] = ok[u] && ((v[u] >= p.plo[q] && v[u] <= p.phi[q]) != (p.pinv[q] != 0));
