@@ -456,6 +456,11 @@ int pd_sort_ex2(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode,
 // 32-bit column a->in_ptr -> a->out_ptr (row ids when a->in_ptr is NULL and
 // a->out_ptr is set) and/or the 64-bit column in_v64 -> out_v64.
 constexpr uint32_t PD_PART_DIGIT_BITS = 6;
+// Sort of (key, payload) where the payload of row i is pay64[i] - *pay_min
+// (int64 values whose range fits 32 bits; a->out_ptr receives the payloads,
+// a->in_ptr must be NULL); the element count is read from *n_dev when given.
+int pd_sort_pay64(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, void *ws, cudaStream_t s,
+                  const uint64_t *n_dev, const int64_t *pay64, const int64_t *pay_min);
 size_t pd_partition_workspace(const pimdal_sort_arguments_t *a, bool v64);
 int pd_partition(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
                  cudaStream_t s, const uint64_t *in_v64, uint64_t *out_v64);

@@ -632,8 +632,14 @@ __global__ void __launch_bounds__(256) k_gb_gather(GatherParams g) {
 }
 
 // ---------------------------------------------------------------------------
-// Sort method: reduce-by-key over (sorted key, row id), values gathered by
-// row id.  Tiles of 4096 sorted rows; a thread owns 16 consecutive rows.
+// Sort method.  When the values' range fits 32 bits (checked on the device:
+// k_vrange), each row's value - min travels through the sort as its payload
+// and the reduce-by-key reads the values from the sorted stream; otherwise
+// the sort carries row ids and the reduce gathers the values by row id.
+// Both paths are enqueued; the device sets one path's row count to n and
+// the other's to 0, and a path with no rows does nothing -- so the choice
+// needs no host round trip.  Without values (COUNT only) keys are sorted
+// alone.  Tiles of 4096 sorted rows; a thread owns 16 consecutive rows.
 //  1. k_sr_heads: group heads per tile;
 //  2. k_sr_scan (one block): exclusive head prefix per tile, group count G;
 //  3. k_sr_init: outputs 0..G-1 set to the aggregate identities;
@@ -647,8 +653,10 @@ constexpr int SR_ITEMS = 16;
 constexpr int SR_TILE = SR_THREADS * SR_ITEMS;
 
 struct SegParams {
-  const uint32_t *skey, *sidx;
-  const int64_t *val;
+  const uint32_t *skey, *sidx;  // sidx: row ids, or payloads (pay_min set); NULL: no values
+  const int64_t *val;           // gathered by row id (row-id path)
+  const long long *pay_min;     // payload path: value = *pay_min + payload
+  const uint64_t *n_dev;        // rows of this path (0: the path is not taken)
   uint64_t n;
   uint32_t *out_key;
   long long *out_sum, *out_min, *out_max;
@@ -664,8 +672,15 @@ __device__ __forceinline__ bool sr_head(const SegParams &p, uint64_t i) {
   return i < p.n && (i == 0 || p.skey[i] != p.skey[i - 1]);
 }
 
+// The path's row count; false when the path is not taken.
+__device__ __forceinline__ bool sr_active(SegParams &p) {
+  if (p.n_dev) p.n = *p.n_dev;
+  return p.n != 0;
+}
+
 __global__ void __launch_bounds__(SR_THREADS) k_sr_heads(SegParams p) {
   __shared__ uint32_t s_red[SR_THREADS / 32];
+  if (!sr_active(p)) return;
   const uint64_t r0 = (uint64_t)blockIdx.x * SR_TILE + threadIdx.x;
   uint32_t c = 0;
 #pragma unroll
@@ -684,6 +699,7 @@ __global__ void __launch_bounds__(SR_THREADS) k_sr_heads(SegParams p) {
 __global__ void __launch_bounds__(1024) k_sr_scan(SegParams p) {
   __shared__ uint64_t s_w[32];
   __shared__ uint64_t s_carry;
+  if (!sr_active(p)) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   if (tid == 0) s_carry = 0;
   __syncthreads();
@@ -715,6 +731,7 @@ __global__ void __launch_bounds__(1024) k_sr_scan(SegParams p) {
 }
 
 __global__ void __launch_bounds__(256) k_sr_init(SegParams p) {
+  if (!sr_active(p)) return;
   const uint64_t lim = min(*p.d_count, p.cap);
   const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
   for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < lim; i += stride) {
@@ -787,18 +804,21 @@ __device__ __forceinline__ void sr_store(const SegParams &p, uint64_t g, uint32_
 __global__ void __launch_bounds__(SR_THREADS) k_gb_segreduce(SegParams p) {
   __shared__ uint32_t s_heads[SR_THREADS / 32];
   __shared__ SrSeg s_seg[SR_THREADS / 32];
+  if (!sr_active(p)) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint64_t tile = blockIdx.x;
   const uint64_t t0 = tile * SR_TILE;
   const uint64_t r0 = t0 + (uint64_t)tid * SR_ITEMS;
   const bool full = t0 + SR_TILE <= p.n;
   uint32_t key[SR_ITEMS], idx[SR_ITEMS];
+  const bool has_idx = p.sidx != nullptr;
   if (full) {
     const uint4 *k4 = reinterpret_cast<const uint4 *>(p.skey + r0);
     const uint4 *i4 = reinterpret_cast<const uint4 *>(p.sidx + r0);
 #pragma unroll
     for (int j = 0; j < SR_ITEMS / 4; ++j) {
-      const uint4 a = __ldcs(k4 + j), b = __ldcs(i4 + j);
+      const uint4 a = __ldcs(k4 + j);
+      const uint4 b = has_idx ? __ldcs(i4 + j) : make_uint4(0, 0, 0, 0);
       key[4 * j] = a.x; key[4 * j + 1] = a.y; key[4 * j + 2] = a.z; key[4 * j + 3] = a.w;
       idx[4 * j] = b.x; idx[4 * j + 1] = b.y; idx[4 * j + 2] = b.z; idx[4 * j + 3] = b.w;
     }
@@ -806,13 +826,19 @@ __global__ void __launch_bounds__(SR_THREADS) k_gb_segreduce(SegParams p) {
 #pragma unroll
     for (int j = 0; j < SR_ITEMS; ++j) {
       key[j] = (r0 + j < p.n) ? p.skey[r0 + j] : 0u;
-      idx[j] = (r0 + j < p.n) ? p.sidx[r0 + j] : 0u;
+      idx[j] = (has_idx && r0 + j < p.n) ? p.sidx[r0 + j] : 0u;
     }
   }
   long long val[SR_ITEMS];
+  if (p.pay_min) {
+    const long long pmin = *p.pay_min;
 #pragma unroll
-  for (int j = 0; j < SR_ITEMS; ++j)
-    val[j] = (p.val && (full || r0 + j < p.n)) ? (long long)__ldg(p.val + idx[j]) : 1ll;
+    for (int j = 0; j < SR_ITEMS; ++j) val[j] = pmin + (long long)idx[j];
+  } else {
+#pragma unroll
+    for (int j = 0; j < SR_ITEMS; ++j)
+      val[j] = (p.val && (full || r0 + j < p.n)) ? (long long)__ldg(p.val + idx[j]) : 1ll;
+  }
   const uint32_t before = (r0 > 0 && r0 - 1 < p.n) ? p.skey[r0 - 1] : 0u;
   uint32_t heads = 0, nh = 0;
 #pragma unroll
@@ -890,11 +916,55 @@ __global__ void __launch_bounds__(SR_THREADS) k_gb_segreduce(SegParams p) {
   }
 }
 
+// Minimum and maximum of the values (mm[0], mm[1]).
+__global__ void k_vrange_init(long long *mm) {
+  mm[0] = INT64_MAX;
+  mm[1] = INT64_MIN;
+}
+
+__global__ void __launch_bounds__(256) k_vrange(const long long *v, uint64_t n, long long *mm) {
+  long long lo = INT64_MAX, hi = INT64_MIN;
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  uint64_t done = 0;
+  if (((uintptr_t)v & 15u) == 0) {
+    const longlong2 *v2 = reinterpret_cast<const longlong2 *>(v);
+    for (uint64_t i = i0; i < n / 2; i += stride) {
+      const longlong2 x = __ldcs(v2 + i);
+      lo = min(lo, min(x.x, x.y));
+      hi = max(hi, max(x.x, x.y));
+    }
+    done = n / 2 * 2;
+  }
+  for (uint64_t i = done + i0; i < n; i += stride) {
+    const long long x = v[i];
+    lo = min(lo, x);
+    hi = max(hi, x);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(mm, lo);
+    atomicMax(mm + 1, hi);
+  }
+}
+
+// The payload path takes the rows when max - min fits 32 bits, else the
+// row-id path does.
+__global__ void k_vrange_pick(const long long *mm, uint64_t n, uint64_t *n_pay, uint64_t *n_idx) {
+  const bool fits = (unsigned long long)mm[1] - (unsigned long long)mm[0] <= 0xFFFFFFFFull;
+  *n_pay = fits ? n : 0;
+  *n_idx = fits ? 0 : n;
+}
+
 struct GbLayout {
   int mode;
   uint32_t sub_cap, npasses, wrep;
   uint32_t part_bits;   // GB_PART: hash partitions 2^part_bits
-  size_t gtab, ngroups, ckey, cslot, skey, sslot, sort_ws, pkey, pval, total;
+  size_t gtab, ngroups, ckey, cslot, skey, sslot, sort_ws, pkey, pval, vrange, total;
 };
 
 bool gb_force_direct() {
@@ -938,6 +1008,7 @@ bool gb_layout(const pimdal_aggr_arguments_t *a, GbLayout *l) {
     if (pimdal_sort_workspace_size(&sa, &w)) return false;
     l->mode = -1;
     l->sub_cap = l->npasses = l->wrep = 0;
+    l->vrange = o; o += 256;  // min, max, rows of the payload and row-id paths
     l->ngroups = o; o += pd_align_up(8 * (pd_ceil_div(a->size, SR_TILE) + 1), 256);
     l->skey = o; o += pd_align_up(4 * a->size, 256);
     l->sslot = o; o += pd_align_up(4 * a->size, 256);
@@ -1083,16 +1154,14 @@ extern "C" int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_argument
   sa.layout = PIMDAL_LAYOUT_COLUMNS;
 
   if (a->method == PIMDAL_GROUP_SORT) {
+    long long *mm = (long long *)(ws + l.vrange);
+    uint64_t *n_pay = (uint64_t *)(mm + 2), *n_idx = n_pay + 1;
     sa.nr_elements = a->size;
     sa.in = a->in;
-    sa.in_ptr = nullptr;  // row ids
+    sa.in_ptr = nullptr;
     sa.out = ws + l.skey;
-    sa.out_ptr = (uint32_t *)(ws + l.sslot);
-    if ((st = pd_sort_with_workspace(ctx, &sa, ws + l.sort_ws, s))) return st;
     SegParams p{};
     p.skey = (const uint32_t *)(ws + l.skey);
-    p.sidx = (const uint32_t *)(ws + l.sslot);
-    p.val = a->in_val;
     p.n = a->size;
     p.out_key = (uint32_t *)a->out;
     p.out_sum = (long long *)a->out_sum;
@@ -1104,23 +1173,58 @@ extern "C" int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_argument
     p.tiles = pd_ceil_div(a->size, SR_TILE);
     p.d_error = ctx->d_error;
     p.d_count = &d_result->t_count;
-    {
-      pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
-      k_sr_heads<<<(unsigned)p.tiles, SR_THREADS, 0, s>>>(p);
+    auto reduce = [&](const SegParams &q) -> int {
+      {
+        pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+        k_sr_heads<<<(unsigned)q.tiles, SR_THREADS, 0, s>>>(q);
+      }
+      {
+        pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+        k_sr_scan<<<1, 1024, 0, s>>>(q);
+      }
+      {
+        pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+        k_sr_init<<<ctx->sm_count * 8, 256, 0, s>>>(q);
+      }
+      {
+        pd_launch_scope sc(ctx, PIMDAL_KERNEL_SEGREDUCE, s);
+        k_gb_segreduce<<<(unsigned)q.tiles, SR_THREADS, 0, s>>>(q);
+      }
+      return pd_launch_status(ctx);
+    };
+    if (!a->in_val) {  // COUNT only: the keys alone
+      sa.out_ptr = nullptr;
+      if ((st = pd_sort_with_workspace(ctx, &sa, ws + l.sort_ws, s))) return st;
+      return reduce(p);
     }
     {
       pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
-      k_sr_scan<<<1, 1024, 0, s>>>(p);
+      k_vrange_init<<<1, 1, 0, s>>>(mm);
     }
     {
       pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
-      k_sr_init<<<ctx->sm_count * 8, 256, 0, s>>>(p);
+      const unsigned g = (unsigned)std::min<uint64_t>(pd_ceil_div(a->size, 512), ctx->sm_count * 8ull);
+      k_vrange<<<g, 256, 0, s>>>((const long long *)a->in_val, a->size, mm);
     }
     {
-      pd_launch_scope sc(ctx, PIMDAL_KERNEL_SEGREDUCE, s);
-      k_gb_segreduce<<<(unsigned)p.tiles, SR_THREADS, 0, s>>>(p);
+      pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+      k_vrange_pick<<<1, 1, 0, s>>>(mm, a->size, n_pay, n_idx);
     }
-    return pd_launch_status(ctx);
+    sa.out_ptr = (uint32_t *)(ws + l.sslot);
+    p.sidx = (const uint32_t *)(ws + l.sslot);
+    // payload path: value - min sorted beside the key
+    if ((st = pd_sort_pay64(ctx, &sa, ws + l.sort_ws, s, n_pay, a->in_val, (const int64_t *)mm)))
+      return st;
+    SegParams q = p;
+    q.pay_min = mm;
+    q.n_dev = n_pay;
+    if ((st = reduce(q))) return st;
+    // row-id path: values gathered by row id
+    if ((st = pd_sort_ex2(ctx, &sa, PD_KEY_PLAIN, ws + l.sort_ws, s, nullptr, n_idx))) return st;
+    q = p;
+    q.val = a->in_val;
+    q.n_dev = n_idx;
+    return reduce(q);
   }
 
   GbParams p{};

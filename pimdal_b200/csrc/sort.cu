@@ -81,6 +81,11 @@ struct SortParams {
   const unsigned long long *in_v64;
   unsigned long long *out_v64, *alt_v64;
   uint32_t dbits;       // digit width of every pass (8; at most 6 for partitions)
+  // 32-bit payload of the first pass taken as pay64[i] - *pay_min (when
+  // pay64 is set and no row-id column is given): int64 values whose range
+  // fits 32 bits travel through the sort in place of row ids
+  const long long *pay64;
+  const long long *pay_min;
   uint64_t n;           // element count (upper bound when n_dev is set)
   const uint64_t *n_dev;  // device-resident element count, or NULL
   uint32_t flip;        // 0x80000000 for signed keys
@@ -233,7 +238,8 @@ __global__ void __launch_bounds__(RS_THREADS) k_sort_copy(SortParams p) {
       v = e.y;
     } else {
       k = reinterpret_cast<const uint32_t *>(p.in)[i];
-      v = p.in_ptr ? p.in_ptr[i] : (uint32_t)(p.ptr_base + i);
+      v = p.in_ptr ? p.in_ptr[i]
+          : p.pay64 ? (uint32_t)(p.pay64[i] - *p.pay_min) : (uint32_t)(p.ptr_base + i);
     }
     if (p.pairs) reinterpret_cast<uint2 *>(p.out)[i] = make_uint2(k, v);
     else {
@@ -366,6 +372,9 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   const uint32_t *sval32 = sval ? sval + base : nullptr;
   const bool gen_vals = first && src == BUF_IN && sval == nullptr && !src_pairs;
   const uint32_t vbase = (uint32_t)(p.ptr_base + base);
+  const bool pay = gen_vals && p.pay64 != nullptr;
+  const long long pmin = pay ? *p.pay_min : 0;
+  const long long *spay = pay ? p.pay64 + base : nullptr;
 
   // Load keys and values up front (all loads in flight together):
   // warp-striped, item k of lane l is tile element wl + 32k.
@@ -383,7 +392,8 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
         if (HAS_VALS) val[k] = e.y;
       } else {
         key[k] = __ldcs(skey32 + li);
-        if (HAS_VALS) val[k] = gen_vals ? vbase + li : __ldcs(sval32 + li);
+        if (HAS_VALS)
+          val[k] = pay ? (uint32_t)(__ldcs(spay + li) - pmin) : gen_vals ? vbase + li : __ldcs(sval32 + li);
       }
     }
   }
@@ -640,8 +650,15 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
     }
   }
   if (HAS_VALS && gen_vals) {
+    if (p.pay64) {
+      const long long pmin = *p.pay_min;
 #pragma unroll
-    for (int i = 0; i < PP_ITEMS; ++i) val[i] = vbase + t0 + i;
+      for (int i = 0; i < PP_ITEMS; ++i)
+        val[i] = t0 + i < tile_n ? (uint32_t)(__ldcs(p.pay64 + base + t0 + i) - pmin) : 0u;
+    } else {
+#pragma unroll
+      for (int i = 0; i < PP_ITEMS; ++i) val[i] = vbase + t0 + i;
+    }
   }
 
   // 2. thread-private counting: local rank of each item within its digit
@@ -819,7 +836,8 @@ int pd_sort_ex(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, 
 namespace {
 int pd_sort_core(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
                  cudaStream_t s, uint32_t **offsets_out, const uint64_t *n_dev, uint32_t dbits,
-                 const uint64_t *in_v64, uint64_t *out_v64);
+                 const uint64_t *in_v64, uint64_t *out_v64, const int64_t *pay64 = nullptr,
+                 const int64_t *pay_min = nullptr);
 }
 
 // Same, with the element count read on the device from *n_dev (a->nr_elements
@@ -836,6 +854,12 @@ size_t pd_partition_workspace(const pimdal_sort_arguments_t *a, bool v64) {
   SortLayout l;
   return sort_layout(a, &l, PD_PART_DIGIT_BITS, v64) ? l.total : 0;
 }
+int pd_sort_pay64(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, void *ws, cudaStream_t s,
+                  const uint64_t *n_dev, const int64_t *pay64, const int64_t *pay_min) {
+  return pd_sort_core(ctx, a, PD_KEY_PLAIN, ws, s, nullptr, n_dev, RS_RADIX_BITS, nullptr, nullptr,
+                      pay64, pay_min);
+}
+
 int pd_partition(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
                  cudaStream_t s, const uint64_t *in_v64, uint64_t *out_v64) {
   if (a->layout != PIMDAL_LAYOUT_COLUMNS || (in_v64 == nullptr) != (out_v64 == nullptr))
@@ -846,7 +870,8 @@ int pd_partition(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode
 namespace {
 int pd_sort_core(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
                  cudaStream_t s, uint32_t **offsets_out, const uint64_t *n_dev, uint32_t dbits,
-                 const uint64_t *in_v64, uint64_t *out_v64) {
+                 const uint64_t *in_v64, uint64_t *out_v64, const int64_t *pay64,
+                 const int64_t *pay_min) {
   SortLayout l;
   const bool v64 = out_v64 != nullptr;
   if (!sort_layout(a, &l, dbits, v64)) return PIMDAL_ERR_ARG;
@@ -868,6 +893,9 @@ int pd_sort_core(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode
   p.out_v64 = (unsigned long long *)out_v64;
   p.alt_v64 = v64 ? (unsigned long long *)(w + l.off_alt_v64) : nullptr;
   p.dbits = dbits;
+  p.pay64 = (const long long *)pay64;
+  p.pay_min = (const long long *)pay_min;
+  if (pay64 && (a->in_ptr || !pay_min)) return PIMDAL_ERR_ARG;
   p.n = a->nr_elements;
   p.n_dev = n_dev;
   p.flip = a->key_dtype == PIMDAL_I32 ? 0x80000000u : 0u;

@@ -122,3 +122,15 @@ def test_partitioned_hash_group_by(ctx, card, expected):
     o = np.argsort(exp[0].view(np.uint32), kind="stable")
     for name, a, b in zip(("key", "sum", "count", "min", "max"), got, exp):
         assert np.array_equal(a, b[o]), name
+
+
+@pytest.mark.parametrize("span", [2**32 - 1, 2**32])
+def test_sort_group_by_value_range_edges(ctx, span):
+    """Sort method: values whose range is exactly 2^32 - 1 travel through the
+    sort as 32-bit payloads; one more and the row-id path takes over -- the
+    same groups either way, against the oracle."""
+    k, v = inputs(200003, 1000, 55)
+    base = -(2**40) + 12345
+    v = (base + (v - 100) % 7).astype(np.int64)
+    v[5], v[777] = base, base + span
+    check(run(ctx, k, v, L.GROUP_SORT, expected=1000), oracle.group_by(k, v))
