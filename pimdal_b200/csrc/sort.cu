@@ -305,6 +305,43 @@ __device__ __forceinline__ uint32_t rs_lookback(uint32_t *st, uint64_t tile, uin
   return excl;
 }
 
+// Warp-cooperative look-back of one digit (all 32 lanes call it): lane i
+// reads the status word of tile - 1 - i - 32 r in round r, so one round
+// covers 32 predecessors.  Same result and publication as rs_lookback.
+__device__ __forceinline__ uint32_t rs_lookback_warp(uint32_t *st, uint64_t tile, uint32_t count,
+                                                     uint32_t *d_error) {
+  const int lane = threadIdx.x & 31;
+  uint32_t excl = 0;
+  int64_t base = (int64_t)tile - 1;
+  uint32_t spins = 0;
+  const uint64_t t0 = pd_globaltimer_ns();
+  while (true) {
+    const int64_t t = base - lane;
+    const uint32_t w = t >= 0 ? pd_load_relaxed_u32(st + (uint64_t)t * RS_RADIX) : RS_FLAG_INC;
+    const uint32_t flag = w & ~RS_COUNT_MASK;
+    const unsigned inc = __ballot_sync(0xffffffffu, flag == RS_FLAG_INC);
+    const unsigned inval = __ballot_sync(0xffffffffu, flag == 0);
+    const int first = inc ? __ffs(inc) - 1 : 31;            // nearest inclusive word
+    const unsigned need = first >= 31 ? 0xffffffffu : ((2u << first) - 1u);
+    if (inval & need) {                                     // a predecessor not yet published
+      bool give_up = false;
+      if (lane == 0) give_up = pd_wait_expired(d_error, t0, ++spins);
+      if (__shfl_sync(0xffffffffu, give_up, 0)) break;
+      __nanosleep(64);
+      continue;
+    }
+    uint32_t c = lane <= first ? (w & RS_COUNT_MASK) : 0u;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    excl += c;
+    if (inc) break;
+    base -= 32;
+  }
+  if (lane == 0)
+    pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_INC | ((excl + count) & RS_COUNT_MASK));
+  return excl;
+}
+
 // Lanes of `members` whose digit equals this lane's: one ballot per digit
 // bit.  For 8-bit labels this is cheaper than the match.any instruction.
 __device__ __forceinline__ unsigned match_digit(uint32_t d, unsigned members) {
@@ -703,19 +740,29 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
   if (tid == 0) s_dstart[S::B] = tile_n;
   __syncthreads();
 
-  // 4. publish the tile's digit counts; look back for the digits' global offsets
-  if (tid < S::B) {
-    const int d = tid;
-    const uint32_t count = s_dstart[d + 1] - s_dstart[d];
-    uint32_t *st = p.status + ((uint64_t)pass * p.tiles) * RS_RADIX + d;
-    uint32_t ex = 0;
-    if (tile == 0) {
-      pd_store_relaxed_u32(st, RS_FLAG_INC | count);
-    } else {
-      pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_AGG | count);
-      ex = rs_lookback(st, tile, count, p.d_error);
+  // 4. publish the tile's digit counts, then look back for the digits' global
+  //    offsets: warp w takes digits w, w + 8, ..., all its lanes reading 32
+  //    predecessors per round; the other warps go on to the staging, which
+  //    needs no offsets
+  {
+    const int warp = tid >> 5, lane = tid & 31;
+    // lane 0 of the warp publishes its digits' counts first, then looks back
+    // (both stores of a digit come from one lane, in order)
+    if (lane == 0) {
+      for (int d = warp; d < S::B; d += RS_WARPS) {
+        uint32_t *st = p.status + ((uint64_t)pass * p.tiles) * RS_RADIX + d;
+        pd_store_relaxed_u32(st + tile * RS_RADIX,
+                             (tile == 0 ? RS_FLAG_INC : RS_FLAG_AGG) | (s_dstart[d + 1] - s_dstart[d]));
+      }
     }
-    s_gdelta[d] = (int32_t)(p.offsets[pass * RS_RADIX + d] + ex) - (int32_t)s_dstart[d];
+    __syncwarp();
+    for (int d = warp; d < S::B; d += RS_WARPS) {
+      const uint32_t count = s_dstart[d + 1] - s_dstart[d];
+      uint32_t *st = p.status + ((uint64_t)pass * p.tiles) * RS_RADIX + d;
+      const uint32_t ex = tile > 0 ? rs_lookback_warp(st, tile, count, p.d_error) : 0u;
+      if (lane == 0)
+        s_gdelta[d] = (int32_t)(p.offsets[pass * RS_RADIX + d] + ex) - (int32_t)s_dstart[d];
+    }
   }
 
   // 5. stage the tile in digit order

@@ -8,6 +8,9 @@
     python -m pimdal_b200.opbench bloom     --rows 268435456 --parts 16384 --match-permille 50
                                              (build = rows / 8; both sides partitioned first,
                                               untimed; times filter + match)
+    python -m pimdal_b200.opbench tpch      --query q6|q1 [--orders 15000000]
+                                             (the fused pass over the lineitem-shaped table
+                                              of the served form; about 4 rows per order)
 
 The per-operator counterpart of the reference's benchmark programs
 (reference/db_operators/*.cpp main: generate, run the kernel a fixed number of
@@ -65,6 +68,9 @@ def _inputs(ctx: ops.Context, a) -> tuple:
         opk, oprow, pps = ops.part_kernel(ctx, pk, shift=32, part_n=a.parts)
         ctx.sync()
         return obk, bps, opk, oprow, pps
+    if a.op == "tpch":
+        from . import serve, tpch
+        return (tpch.Lineitem(ctx, serve.Tables(ctx, orders=a.orders)),)
     if a.op == "group":
         keys = g(gen.Spec(L.GEN_PERM_UNIFORM, L.I32, seed=a.seed, stream_id=10, lo=0,
                           hi=a.card - 1, perm_domain=0), n)
@@ -109,6 +115,20 @@ def _runner(ctx: ops.Context, a, inp):
             ops.match_kernel(ctx, filt, opk, pps, oprow, out=ok, out_row=orow, result=res)
         bloom.result = res
         return bloom
+    if a.op == "tpch":
+        from . import tpch
+        li = inp[0]
+        a.rows = li.n
+        res = torch.empty(1, dtype=torch.int64, device=dev)
+        if a.query == "q6":
+            preds, exprs = tpch.q6_args(li)
+            run = lambda: ops.select_aggregate(ctx, li.n, preds=preds, exprs=exprs, result=res)
+        else:
+            pred, group, exprs = tpch.q1_args(li)
+            run = lambda: ops.select_aggregate(ctx, li.n, preds=[pred], group=group,
+                                               key_space=tpch.N_RFLAG * tpch.N_LSTATUS,
+                                               exprs=exprs, result=res)
+        return run
     method = {"hash": L.GROUP_HASH, "sort": L.GROUP_SORT, "auto": L.GROUP_AUTO}[a.method]
     cap = 2 * a.card
     outs = {w: torch.empty(cap, dtype=torch.int64, device=dev) for w in ("sum", "count", "min", "max")}
@@ -120,7 +140,7 @@ def _runner(ctx: ops.Context, a, inp):
 
 def main(argv=None) -> None:
     p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    p.add_argument("op", choices=["select", "sort", "smj", "hash_join", "group", "bloom"])
+    p.add_argument("op", choices=["select", "sort", "smj", "hash_join", "group", "bloom", "tpch"])
     p.add_argument("--rows", type=int, default=1 << 24)
     p.add_argument("--iters", type=int, default=10)
     p.add_argument("--warmup", type=int, default=2)
@@ -133,6 +153,8 @@ def main(argv=None) -> None:
     p.add_argument("--load-factor", type=int, default=0, help="hash join table load factor, percent")
     p.add_argument("--parts", type=int, default=16384, help="bloom: partitions (power of 2)")
     p.add_argument("--match-permille", type=int, default=50, help="bloom: probe match rate")
+    p.add_argument("--query", default="q6", choices=["q6", "q1"], help="tpch: the query")
+    p.add_argument("--orders", type=int, default=15_000_000, help="tpch: orders of the table")
     p.add_argument("--device", type=int, default=0)
     p.add_argument("--kernels", action="store_true",
                    help="also print the mean time of each library kernel class")
