@@ -58,6 +58,8 @@ NCU_TRAFFIC = {
                               "profiles/k_gb_aggregate_2p25_rows.md (2^22 groups)"),
     "k_smj_merge": ((336.1e6 + 215.0e6) / 2**25, "outer row",
                     "profiles/k_smj_merge_2p25_outer.md"),
+    "k_gb_chunks": ((424.5e6 + 7.8e6) / 2**25, "row",
+                    "profiles/k_gb_chunks_2p25_rows.md (chunk aggregation after partitioning)"),
 }
 
 
@@ -1154,8 +1156,8 @@ def per_operator(ctx, dev, peak, iters=7) -> dict:
             alg = 12 * n + 36 * groups
             dom = "group" if method == L.GROUP_HASH else "sort_pass"
             tr = None
-            if method == L.GROUP_HASH:
-                tr = ncu_traffic("k_gb_aggregate_direct" if c > (1 << 16) else "k_gb_aggregate_shared", n)
+            if method == L.GROUP_HASH:  # above 4608 groups the rows are partitioned first
+                tr = ncu_traffic("k_gb_chunks" if c > 4608 else "k_gb_aggregate_shared", n)
             out[f"group_{mname}_{c}_cfg3"] = dict(
                 _op_record(n, t, alg, peak, split, dom, 12 * n if method == L.GROUP_HASH else None, tr),
                 groups=groups)

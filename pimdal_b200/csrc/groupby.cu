@@ -681,18 +681,21 @@ __device__ __forceinline__ bool sr_active(SegParams &p) {
 __global__ void __launch_bounds__(SR_THREADS) k_sr_heads(SegParams p) {
   __shared__ uint32_t s_red[SR_THREADS / 32];
   if (!sr_active(p)) return;
-  const uint64_t r0 = (uint64_t)blockIdx.x * SR_TILE + threadIdx.x;
-  uint32_t c = 0;
+  for (uint64_t tile = blockIdx.x; tile < p.tiles; tile += gridDim.x) {
+    const uint64_t r0 = tile * SR_TILE + threadIdx.x;
+    uint32_t c = 0;
 #pragma unroll
-  for (int j = 0; j < SR_ITEMS; ++j) c += sr_head(p, r0 + (uint64_t)j * SR_THREADS);
+    for (int j = 0; j < SR_ITEMS; ++j) c += sr_head(p, r0 + (uint64_t)j * SR_THREADS);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-  if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = c;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    uint32_t t = 0;
-    for (int w = 0; w < SR_THREADS / 32; ++w) t += s_red[w];
-    p.tile_heads[blockIdx.x] = t;
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    __syncthreads();  // s_red of the previous tile has been read
+    if ((threadIdx.x & 31) == 0) s_red[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t t = 0;
+      for (int w = 0; w < SR_THREADS / 32; ++w) t += s_red[w];
+      p.tile_heads[tile] = t;
+    }
   }
 }
 
@@ -806,7 +809,8 @@ __global__ void __launch_bounds__(SR_THREADS) k_gb_segreduce(SegParams p) {
   __shared__ SrSeg s_seg[SR_THREADS / 32];
   if (!sr_active(p)) return;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint64_t tile = blockIdx.x;
+  for (uint64_t tile = blockIdx.x; tile < p.tiles; tile += gridDim.x) {
+  __syncthreads();  // the previous tile's readers of shared memory are done
   const uint64_t t0 = tile * SR_TILE;
   const uint64_t r0 = t0 + (uint64_t)tid * SR_ITEMS;
   const bool full = t0 + SR_TILE <= p.n;
@@ -913,6 +917,7 @@ __global__ void __launch_bounds__(SR_THREADS) k_gb_segreduce(SegParams p) {
     } else {
       sr_store(p, p.tile_heads[tile] - 1, p.skey[t0], false, all.a);
     }
+  }
   }
 }
 
@@ -1174,9 +1179,10 @@ extern "C" int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_argument
     p.d_error = ctx->d_error;
     p.d_count = &d_result->t_count;
     auto reduce = [&](const SegParams &q) -> int {
+      const unsigned sr_grid = (unsigned)std::min<uint64_t>(q.tiles, ctx->sm_count * 8ull);
       {
         pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
-        k_sr_heads<<<(unsigned)q.tiles, SR_THREADS, 0, s>>>(q);
+        k_sr_heads<<<sr_grid, SR_THREADS, 0, s>>>(q);
       }
       {
         pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
@@ -1188,7 +1194,7 @@ extern "C" int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_argument
       }
       {
         pd_launch_scope sc(ctx, PIMDAL_KERNEL_SEGREDUCE, s);
-        k_gb_segreduce<<<(unsigned)q.tiles, SR_THREADS, 0, s>>>(q);
+        k_gb_segreduce<<<sr_grid, SR_THREADS, 0, s>>>(q);
       }
       return pd_launch_status(ctx);
     };

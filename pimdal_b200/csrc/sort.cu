@@ -266,9 +266,9 @@ __device__ __forceinline__ uint32_t sort_xform(uint32_t k, uint32_t flip) {
 // sets the timeout bit and publishes what it has (the pass is then reported
 // as failed).
 #ifndef PD_RS_LOOKBACK
-#define PD_RS_LOOKBACK 4  // predecessor words per look-back round
+#define PD_RS_LOOKBACK 4  // predecessor words per look-back round of the digit pass
 #endif
-constexpr int RS_LOOKBACK = PD_RS_LOOKBACK;
+template <int RS_LOOKBACK>
 __device__ __forceinline__ uint32_t rs_lookback(uint32_t *st, uint64_t tile, uint32_t count,
                                                 uint32_t *d_error) {
   uint32_t excl = 0;
@@ -302,43 +302,6 @@ __device__ __forceinline__ uint32_t rs_lookback(uint32_t *st, uint64_t tile, uin
     }
   }
   pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_INC | ((excl + count) & RS_COUNT_MASK));
-  return excl;
-}
-
-// Warp-cooperative look-back of one digit (all 32 lanes call it): lane i
-// reads the status word of tile - 1 - i - 32 r in round r, so one round
-// covers 32 predecessors.  Same result and publication as rs_lookback.
-__device__ __forceinline__ uint32_t rs_lookback_warp(uint32_t *st, uint64_t tile, uint32_t count,
-                                                     uint32_t *d_error) {
-  const int lane = threadIdx.x & 31;
-  uint32_t excl = 0;
-  int64_t base = (int64_t)tile - 1;
-  uint32_t spins = 0;
-  const uint64_t t0 = pd_globaltimer_ns();
-  while (true) {
-    const int64_t t = base - lane;
-    const uint32_t w = t >= 0 ? pd_load_relaxed_u32(st + (uint64_t)t * RS_RADIX) : RS_FLAG_INC;
-    const uint32_t flag = w & ~RS_COUNT_MASK;
-    const unsigned inc = __ballot_sync(0xffffffffu, flag == RS_FLAG_INC);
-    const unsigned inval = __ballot_sync(0xffffffffu, flag == 0);
-    const int first = inc ? __ffs(inc) - 1 : 31;            // nearest inclusive word
-    const unsigned need = first >= 31 ? 0xffffffffu : ((2u << first) - 1u);
-    if (inval & need) {                                     // a predecessor not yet published
-      bool give_up = false;
-      if (lane == 0) give_up = pd_wait_expired(d_error, t0, ++spins);
-      if (__shfl_sync(0xffffffffu, give_up, 0)) break;
-      __nanosleep(64);
-      continue;
-    }
-    uint32_t c = lane <= first ? (w & RS_COUNT_MASK) : 0u;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    excl += c;
-    if (inc) break;
-    base -= 32;
-  }
-  if (lane == 0)
-    pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_INC | ((excl + count) & RS_COUNT_MASK));
   return excl;
 }
 
@@ -378,6 +341,9 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   auto dig = [&](uint32_t k) { return (sort_xform<KEY_MODE>(k, flip) >> shift) & mask; };
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  // persistent: tiles are claimed in order until the input is exhausted
+  for (;;) {
+  __syncthreads();  // the previous tile's readers of shared memory are done
   if (tid == 0) s_tile = atomicAdd(&p.counters[pass], 1u);
 #pragma unroll
   for (int w = 0; w < RS_WARPS; ++w) {
@@ -392,7 +358,7 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   const uint64_t tile = s_tile;
   const uint64_t base = tile * (uint64_t)RS_TILE;
   const uint64_t n = sort_n(p);
-  if (base >= n) return;  // tile past a device-resident count: nothing to do
+  if (base >= n) break;  // past the (possibly device-resident) count: done
   const uint32_t tile_n = (uint32_t)min((uint64_t)RS_TILE, n - base);
   const bool full = tile_n == RS_TILE;
   const uint32_t wl = (uint32_t)warp * RS_WARP_TILE + lane;  // tile-local index of item 0
@@ -538,7 +504,7 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
 
   // The digit's global offset.  (Looking back before the ranking instead,
   // to publish the inclusive counts earlier, was measured no faster.)
-  const uint32_t excl = tile > 0 ? rs_lookback(st, tile, count, p.d_error) : 0u;
+  const uint32_t excl = tile > 0 ? rs_lookback<PD_RS_LOOKBACK>(st, tile, count, p.d_error) : 0u;
   s_gdelta[d] = (int32_t)(p.offsets[pass * RS_RADIX + d] + excl) - (int32_t)dstart;
   __syncthreads();
 
@@ -570,11 +536,12 @@ k_sort_pass(SortParams p, uint32_t pass, uint32_t shift, uint32_t mask) {
   if (full) {
 #pragma unroll
     for (int j = 0; j < RS_ITEMS; ++j) put(tid + j * RS_THREADS);
-    return;
+    continue;
   }
 #endif
 #pragma unroll 4
   for (uint32_t i = tid; i < tile_n; i += RS_THREADS) put(i);
+  }
 }
 
 // ------------------------------------------------- small-radix partition pass
@@ -633,13 +600,16 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
   auto dig = [&](uint32_t k) { return (sort_xform<KEY_MODE>(k, flip) >> shift) & mask; };
 
   const int tid = threadIdx.x;
+  // persistent: tiles are claimed in order until the input is exhausted
+  for (;;) {
+  __syncthreads();  // the previous tile's readers of shared memory are done
   if (tid == 0) s_tile = atomicAdd(&p.counters[pass], 1u);
   for (int i = tid; i < S::WORDS; i += RS_THREADS) s_cnt[i] = 0;
   __syncthreads();
   const uint64_t tile = s_tile;
   const uint64_t base = tile * (uint64_t)RS_TILE;
   const uint64_t n = sort_n(p);
-  if (base >= n) return;
+  if (base >= n) break;
   const uint32_t tile_n = (uint32_t)min((uint64_t)RS_TILE, n - base);
   const uint32_t t0 = (uint32_t)tid * PP_ITEMS;  // tile-local index of this thread's first item
 
@@ -740,29 +710,22 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
   if (tid == 0) s_dstart[S::B] = tile_n;
   __syncthreads();
 
-  // 4. publish the tile's digit counts, then look back for the digits' global
-  //    offsets: warp w takes digits w, w + 8, ..., all its lanes reading 32
-  //    predecessors per round; the other warps go on to the staging, which
-  //    needs no offsets
-  {
-    const int warp = tid >> 5, lane = tid & 31;
-    // lane 0 of the warp publishes its digits' counts first, then looks back
-    // (both stores of a digit come from one lane, in order)
-    if (lane == 0) {
-      for (int d = warp; d < S::B; d += RS_WARPS) {
-        uint32_t *st = p.status + ((uint64_t)pass * p.tiles) * RS_RADIX + d;
-        pd_store_relaxed_u32(st + tile * RS_RADIX,
-                             (tile == 0 ? RS_FLAG_INC : RS_FLAG_AGG) | (s_dstart[d + 1] - s_dstart[d]));
-      }
+  // 4. publish the tile's digit counts; look back for the digits' global
+  //    offsets (one thread per digit, 8 predecessor words per round; a warp
+  //    that spreads its digits sequentially over its lanes was measured
+  //    slower); the other threads go on to the staging, which needs none
+  if (tid < S::B) {
+    const int d = tid;
+    const uint32_t count = s_dstart[d + 1] - s_dstart[d];
+    uint32_t *st = p.status + ((uint64_t)pass * p.tiles) * RS_RADIX + d;
+    uint32_t ex = 0;
+    if (tile == 0) {
+      pd_store_relaxed_u32(st, RS_FLAG_INC | count);
+    } else {
+      pd_store_relaxed_u32(st + tile * RS_RADIX, RS_FLAG_AGG | count);
+      ex = rs_lookback<8>(st, tile, count, p.d_error);
     }
-    __syncwarp();
-    for (int d = warp; d < S::B; d += RS_WARPS) {
-      const uint32_t count = s_dstart[d + 1] - s_dstart[d];
-      uint32_t *st = p.status + ((uint64_t)pass * p.tiles) * RS_RADIX + d;
-      const uint32_t ex = tile > 0 ? rs_lookback_warp(st, tile, count, p.d_error) : 0u;
-      if (lane == 0)
-        s_gdelta[d] = (int32_t)(p.offsets[pass * RS_RADIX + d] + ex) - (int32_t)s_dstart[d];
-    }
+    s_gdelta[d] = (int32_t)(p.offsets[pass * RS_RADIX + d] + ex) - (int32_t)s_dstart[d];
   }
 
   // 5. stage the tile in digit order
@@ -788,6 +751,7 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
     dkey[g] = e.x;
     if (HAS_VALS) dval[g] = e.y;
     if (V64) dv64[g] = s_v64[i];
+  }
   }
 }
 
@@ -915,6 +879,18 @@ int pd_partition(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode
 }
 
 namespace {
+// Grid of a persistent pass: the CTAs that fit on the GPU at once (each
+// claims tiles until the input is exhausted), at most one per tile.
+unsigned resident_grid(const pimdal_ctx *ctx, const void *kernel, int smem, uint64_t tiles) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, RS_THREADS, smem) !=
+          cudaSuccess || per_sm <= 0) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(tiles, (uint64_t)per_sm * ctx->sm_count));
+}
+
 int pd_sort_core(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode, void *ws,
                  cudaStream_t s, uint32_t **offsets_out, const uint64_t *n_dev, uint32_t dbits,
                  const uint64_t *in_v64, uint64_t *out_v64, const int64_t *pay64,
@@ -986,7 +962,7 @@ int pd_sort_core(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode
       const uint32_t shift = p.begin_bit + q * dbits;
       PartKernel k = pick_part(std::min(dbits, p.end_bit - shift), val, key_mode);
       PD_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-      k<<<(unsigned)l.tiles, RS_THREADS, smem, s>>>(p, q, shift);
+      k<<<resident_grid(ctx, (const void *)k, smem, l.tiles), RS_THREADS, smem, s>>>(p, q, shift);
     }
     return pd_launch_status(ctx);
   }
@@ -998,7 +974,7 @@ int pd_sort_core(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode
     auto k = pick_pass(p.has_vals != 0, key_mode);
     const int smem = (p.has_vals ? 8 : 4) * RS_TILE;
     PD_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    k<<<(unsigned)l.tiles, RS_THREADS, smem, s>>>(p, q, shift, mask);
+    k<<<resident_grid(ctx, (const void *)k, smem, l.tiles), RS_THREADS, smem, s>>>(p, q, shift, mask);
   }
   return pd_launch_status(ctx);
 }
