@@ -15,9 +15,13 @@
 //    passed the earlier ones (a masked lane issues no load, so a sector whose
 //    rows all failed is never fetched) -- the reference's late
 //    materialisation, at sector granularity.
-//  * Sums accumulate in shared memory: for small key spaces each thread owns
-//    private slots (no atomics; [slot][thread] layout, conflict-free), else
-//    the CTA shares one table updated with shared-memory atomics.  Each CTA
+//  * Sums accumulate in shared memory in nsets copies of the table ([slot]
+//    [set] layout): thread t adds into set t mod nsets, with plain adds when
+//    every thread has its own set (nsets = 256) and shared-memory atomics
+//    otherwise.  The host picks the most sets whose tables fit in
+//    PD_SA_SMEM_TARGET bytes, so a small key space gets private slots and a
+//    mid-sized one (TPC-H Q1: 6 keys x 6 sums) keeps the CTA small enough for
+//    8 CTAs per SM; a large key space gets one shared table.  Each CTA
 //    then adds its non-zero slots to a global table with one atomic each, and
 //    one CTA emits the groups with rows, in key order.  Integer sums wrap mod
 //    2^64 and do not depend on the order of the additions.
@@ -35,7 +39,9 @@ constexpr int SA_THREADS = 256;
 #define PD_SA_EAGER 0   // 1: predicate columns read for every row, not only the selected ones
 #endif
 constexpr int SA_UNROLL = PD_SA_UNROLL;
-constexpr uint32_t SA_PRIVATE_BYTES = 96 * 1024;  // per-thread slots up to this much shared memory
+#ifndef PD_SA_SMEM_TARGET
+#define PD_SA_SMEM_TARGET (24 * 1024)  // shared-memory bytes of the table copies
+#endif
 
 struct SaCol {
   const void *p;
@@ -57,7 +63,7 @@ struct SaParams {
   uint32_t tneg[PIMDAL_SA_MAX_EXPRS][PIMDAL_SA_MAX_TERMS];
   uint32_t nterms[PIMDAL_SA_MAX_EXPRS];
   uint32_t nexprs;
-  uint32_t priv;                    // 1: per-thread private slots
+  uint32_t nsets;                   // table copies (a power of two, 1 .. SA_THREADS)
   unsigned long long *g_acc;        // [ks][nexprs + 1] (slot 0: COUNT)
   uint32_t *d_error;
 };
@@ -83,13 +89,15 @@ __global__ void __launch_bounds__(SA_THREADS) k_sa_scan(SaParams p) {
   const int tid = threadIdx.x;
   const uint32_t nv = p.nexprs + 1;
   const uint32_t slots = p.ks * nv;
-  const uint32_t words = p.priv ? slots * SA_THREADS : slots;
+  const uint32_t nsets = p.nsets;
+  const uint32_t words = slots * nsets;
+  const uint32_t set = tid & (nsets - 1);  // this thread's copy of the table
   for (uint32_t i = tid; i < words; i += SA_THREADS) sa_acc[i] = 0;
   __syncthreads();
-  auto acc_add = [&](uint32_t key, uint32_t slot, unsigned long long v) {
-    const uint32_t s = key * nv + slot;
-    if (p.priv) sa_acc[s * SA_THREADS + tid] += v;
-    else atomicAdd(&sa_acc[s], v);
+  auto acc_add = [=](uint32_t key, uint32_t slot, unsigned long long v) {
+    const uint32_t i = (key * nv + slot) * nsets + set;
+    if (nsets == SA_THREADS) sa_acc[i] += v;
+    else atomicAdd(&sa_acc[i], v);
   };
   bool bad = false;
   const uint64_t step = (uint64_t)gridDim.x * SA_THREADS * SA_UNROLL;
@@ -164,11 +172,7 @@ __global__ void __launch_bounds__(SA_THREADS) k_sa_scan(SaParams p) {
   __syncthreads();
   for (uint32_t s = tid; s < slots; s += SA_THREADS) {
     unsigned long long v = 0;
-    if (p.priv) {
-      for (int t = 0; t < SA_THREADS; ++t) v += sa_acc[s * SA_THREADS + t];
-    } else {
-      v = sa_acc[s];
-    }
+    for (uint32_t t = 0; t < nsets; ++t) v += sa_acc[s * nsets + t];
     if (v) atomicAdd(&p.g_acc[s], v);
   }
 }
@@ -274,8 +278,9 @@ extern "C" int pimdal_select_aggregate(pimdal_ctx_t *ctx,
   p.g_acc = (unsigned long long *)ws;
   p.d_error = ctx->d_error;
   const uint64_t slots = (uint64_t)a->key_space * nv;
-  p.priv = slots * SA_THREADS * 8 <= SA_PRIVATE_BYTES;
-  const size_t smem = p.priv ? slots * SA_THREADS * 8 : slots * 8;
+  p.nsets = SA_THREADS;
+  while (p.nsets > 1 && slots * p.nsets * 8 > PD_SA_SMEM_TARGET) p.nsets >>= 1;
+  const size_t smem = slots * p.nsets * 8;
   if (a->size) {
     PD_CHECK_CUDA(cudaFuncSetAttribute(k_sa_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem));
