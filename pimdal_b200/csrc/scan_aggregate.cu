@@ -52,7 +52,8 @@ struct SaParams {
   uint64_t n;
   const uint32_t *rows;
   SaCol pc[PIMDAL_SA_MAX_PREDS];
-  int64_t plo[PIMDAL_SA_MAX_PREDS], phi[PIMDAL_SA_MAX_PREDS];
+  int64_t plo[PIMDAL_SA_MAX_PREDS];
+  uint64_t prange[PIMDAL_SA_MAX_PREDS];  // selected: (v - lo) mod 2^64 <= range, xor pinv
   uint32_t pinv[PIMDAL_SA_MAX_PREDS];
   uint32_t npreds;
   SaCol gc[PIMDAL_SA_MAX_GROUP_COLS];
@@ -75,12 +76,23 @@ struct SaOut {
   uint64_t cap;
 };
 
-__device__ __forceinline__ int64_t sa_load(const SaCol &c, uint32_t r) {
+// A column's values at this step's rows (0 where take[u] is false); the
+// element type is resolved once per step, not once per row.
+template <typename T>
+__device__ __forceinline__ void sa_load_as(const void *col, const uint32_t (&row)[SA_UNROLL],
+                                           const bool (&take)[SA_UNROLL], int64_t (&v)[SA_UNROLL]) {
+  const T *q = reinterpret_cast<const T *>(col);
+#pragma unroll
+  for (int u = 0; u < SA_UNROLL; ++u) v[u] = take[u] ? (int64_t)__ldg(q + row[u]) : 0;
+}
+
+__device__ __forceinline__ void sa_load_rows(const SaCol &c, const uint32_t (&row)[SA_UNROLL],
+                                             const bool (&take)[SA_UNROLL], int64_t (&v)[SA_UNROLL]) {
   switch (c.dtype) {
-    case PIMDAL_I32: return (int64_t)__ldg(reinterpret_cast<const int32_t *>(c.p) + r);
-    case PIMDAL_U32: return (int64_t)__ldg(reinterpret_cast<const uint32_t *>(c.p) + r);
-    case PIMDAL_I64: return (int64_t)__ldg(reinterpret_cast<const long long *>(c.p) + r);
-    default: return (int64_t)__ldg(reinterpret_cast<const unsigned char *>(c.p) + r);
+    case PIMDAL_I32: sa_load_as<int32_t>(c.p, row, take, v); break;
+    case PIMDAL_U32: sa_load_as<uint32_t>(c.p, row, take, v); break;
+    case PIMDAL_I64: sa_load_as<long long>(c.p, row, take, v); break;
+    default: sa_load_as<unsigned char>(c.p, row, take, v); break;
   }
 }
 
@@ -99,6 +111,11 @@ __global__ void __launch_bounds__(SA_THREADS) k_sa_scan(SaParams p) {
     if (nsets == SA_THREADS) sa_acc[i] += v;
     else atomicAdd(&sa_acc[i], v);
   };
+  // one key (no group columns): the sums stay in registers until the end
+  const bool scalar = p.ks == 1;
+  unsigned long long racc[PIMDAL_SA_MAX_EXPRS + 1];
+#pragma unroll
+  for (int e = 0; e <= PIMDAL_SA_MAX_EXPRS; ++e) racc[e] = 0;
   bool bad = false;
   const uint64_t step = (uint64_t)gridDim.x * SA_THREADS * SA_UNROLL;
   for (uint64_t base = (uint64_t)blockIdx.x * SA_THREADS * SA_UNROLL; base < p.n; base += step) {
@@ -116,12 +133,13 @@ __global__ void __launch_bounds__(SA_THREADS) k_sa_scan(SaParams p) {
     for (int q = 0; q < PIMDAL_SA_MAX_PREDS; ++q) {
       if (q < (int)p.npreds) {
         int64_t v[SA_UNROLL];
+        sa_load_rows(p.pc[q], row, PD_SA_EAGER ? valid : ok, v);
+        const int64_t lo = p.plo[q];
+        const uint64_t range = p.prange[q];
+        const bool inv = p.pinv[q] != 0;
 #pragma unroll
         for (int u = 0; u < SA_UNROLL; ++u)
-          v[u] = (PD_SA_EAGER ? valid[u] : ok[u]) ? sa_load(p.pc[q], row[u]) : 0;
-#pragma unroll
-        for (int u = 0; u < SA_UNROLL; ++u)
-          ok[u] = ok[u] && ((v[u] >= p.plo[q] && v[u] <= p.phi[q]) != (p.pinv[q] != 0));
+          ok[u] = ok[u] && (((uint64_t)(v[u] - lo) <= range) != inv);
       }
     }
     uint32_t key[SA_UNROLL];
@@ -130,9 +148,10 @@ __global__ void __launch_bounds__(SA_THREADS) k_sa_scan(SaParams p) {
 #pragma unroll
     for (int g = 0; g < PIMDAL_SA_MAX_GROUP_COLS; ++g) {
       if (g < (int)p.ngroup) {
+        int64_t v[SA_UNROLL];
+        sa_load_rows(p.gc[g], row, ok, v);
 #pragma unroll
-        for (int u = 0; u < SA_UNROLL; ++u)
-          if (ok[u]) key[u] += (uint32_t)sa_load(p.gc[g], row[u]) * p.gmult[g];
+        for (int u = 0; u < SA_UNROLL; ++u) key[u] += (uint32_t)v[u] * p.gmult[g];
       }
     }
 #pragma unroll
@@ -141,7 +160,8 @@ __global__ void __launch_bounds__(SA_THREADS) k_sa_scan(SaParams p) {
         bad = true;
         ok[u] = false;
       }
-      if (ok[u]) acc_add(key[u], 0, 1ull);
+      if (scalar) racc[0] += ok[u] ? 1ull : 0ull;
+      else if (ok[u]) acc_add(key[u], 0, 1ull);
     }
 #pragma unroll
     for (int e = 0; e < PIMDAL_SA_MAX_EXPRS; ++e) {
@@ -155,18 +175,28 @@ __global__ void __launch_bounds__(SA_THREADS) k_sa_scan(SaParams p) {
           const SaCol c = p.tc[e][t];
           const uint32_t neg = p.tneg[e][t];
           const int64_t add = p.tadd[e][t];
+          int64_t x[SA_UNROLL];
+          if (c.p) {
+            sa_load_rows(c, row, ok, x);
+          } else {
 #pragma unroll
-          for (int u = 0; u < SA_UNROLL; ++u) {
-            int64_t x = (ok[u] && c.p) ? sa_load(c, row[u]) : 0;
-            x = (neg ? -x : x) + add;
-            val[u] *= (unsigned long long)x;
+            for (int u = 0; u < SA_UNROLL; ++u) x[u] = 0;
           }
+#pragma unroll
+          for (int u = 0; u < SA_UNROLL; ++u) val[u] *= (unsigned long long)((neg ? -x[u] : x[u]) + add);
         }
       }
 #pragma unroll
-      for (int u = 0; u < SA_UNROLL; ++u)
-        if (ok[u]) acc_add(key[u], 1 + e, val[u]);
+      for (int u = 0; u < SA_UNROLL; ++u) {
+        if (scalar) racc[1 + e] += ok[u] ? val[u] : 0ull;
+        else if (ok[u]) acc_add(key[u], 1 + e, val[u]);
+      }
     }
+  }
+  if (scalar) {
+#pragma unroll
+    for (int e = 0; e <= PIMDAL_SA_MAX_EXPRS; ++e)
+      if (e < (int)nv && racc[e]) acc_add(0, e, racc[e]);
   }
   if (bad) atomicOr(p.d_error, PD_DEVERR_ARG);
   __syncthreads();
@@ -243,7 +273,16 @@ extern "C" int pimdal_select_aggregate(pimdal_ctx_t *ctx,
   for (uint32_t q = 0; q < a->n_preds; ++q) {
     const pimdal_column_pred_t &c = a->pred[q];
     if (!sa_dtype_ok(c.dtype) || (a->size && !c.col)) return PIMDAL_ERR_ARG;
-    if (!pd_pred_interval(c.pred, &p.plo[q], &p.phi[q], &p.pinv[q])) return PIMDAL_ERR_ARG;
+    int64_t lo, hi;
+    if (!pd_pred_interval(c.pred, &lo, &hi, &p.pinv[q])) return PIMDAL_ERR_ARG;
+    if (lo > hi) {  // an empty interval: "everything, inverted"
+      p.plo[q] = 0;
+      p.prange[q] = UINT64_MAX;
+      p.pinv[q] ^= 1u;
+    } else {
+      p.plo[q] = lo;
+      p.prange[q] = (uint64_t)hi - (uint64_t)lo;
+    }
     p.pc[q] = {c.col, c.dtype};
   }
   p.ngroup = a->n_group;
