@@ -240,7 +240,10 @@ class SortSmjWorkload(Workload):
     32-bit keys and with Zipf(1.0) keys over 2^24 distinct values, then the
     sort-merge join of R = 2^24 unique int32 keys (a permutation of
     0..2^24-1) with int32 payloads against S = 2^26 keys drawn uniformly from
-    R's keys with int32 payloads.  One step runs all three."""
+    R's keys with int32 payloads.  One step runs all three.  The sorts' row
+    ids are the row index, made on the device by the sort (in_ptr = NULL), as
+    the reference's sort program makes them on the DPU from the uploaded keys
+    (create_ptr, pimdal/main/sort/dpu/kernel_sort.c:32-36,73)."""
     name = "sort_smj"
     N = 1 << 26
     NR = 1 << 24
@@ -262,7 +265,8 @@ class SortSmjWorkload(Workload):
         self.config = {
             "workload": "radix sort 2^26 (uint32 key, uint32 row id) pairs, uniform keys and "
                         "Zipf(1.0) over 2^24 keys; sort-merge join R=2^24 unique int32 keys + "
-                        "int32 payload vs S=2^26 keys uniform over R + int32 payload",
+                        "int32 payload vs S=2^26 keys uniform over R + int32 payload; the sorts' "
+                        "row ids are the row index, generated on the device",
             "sort_rows": self.N, "smj_inner_rows": self.NR, "smj_outer_rows": self.NS,
             "l2": "inputs larger than L2 (512 MiB per sorted array); L2 also flushed between steps"}
         self.rows_per_step = 2 * self.N + self.NR + self.NS
@@ -276,7 +280,6 @@ class SortSmjWorkload(Workload):
         self.spec_z.cdf = gen.zipf_cdf(1 << 24, 1.0)
         g = lambda spec, n: ops.gen_column(ctx, spec, n)
         self.ku, self.kz = g(self.spec_u, self.N), g(self.spec_z, self.N)
-        self.rows = torch.arange(self.N, dtype=torch.int32, device=dev)
         self.rk, self.rp = g(self.spec_rk, self.NR), g(self.spec_rp, self.NR)
         self.sk, self.sp = g(self.spec_sk, self.NS), g(self.spec_sp, self.NS)
         e = lambda n: torch.empty(n, dtype=torch.int32, device=dev)
@@ -288,16 +291,18 @@ class SortSmjWorkload(Workload):
         assert int(self.res.item()) == self.NS
         # pinned host copies for the end-to-end run
         pin = lambda t: t.cpu().pin_memory()
-        self.h_in = [pin(t) for t in (self.ku, self.rows, self.kz, self.rk, self.rp, self.sk, self.sp)]
-        self.d_in2 = [torch.empty_like(t) for t in (self.ku, self.rows, self.kz, self.rk, self.rp,
-                                                    self.sk, self.sp)]
+        self.h_in = [pin(t) for t in (self.ku, self.kz, self.rk, self.rp, self.sk, self.sp)]
+        self.d_in2 = [torch.empty_like(t) for t in (self.ku, self.kz, self.rk, self.rp, self.sk,
+                                                    self.sp)]
         self.h_out = [torch.empty(t.numel(), dtype=t.dtype).pin_memory()
                       for t in (self.ou, self.oup, self.oz, self.ozp, self.ji, self.jo)]
         # algorithmic bytes of the digit passes of one step: 16 B per pair per
-        # active pass (uniform and Zipf keys: 4 passes; R and S keys < 2^24: 3)
-        self.pass_bytes = 16 * (4 * self.N + 4 * self.N + 3 * self.NR + 3 * self.NS)
+        # active pass (uniform and Zipf keys: 4 passes; R and S keys < 2^24: 3),
+        # less the row ids the first pass of each index-id sort does not read
+        pairs = 4 * self.N + 4 * self.N + 3 * self.NR + 3 * self.NS
+        self.pass_bytes = 16 * pairs - 4 * 2 * self.N
         self.active_passes = 4 + 4 + 3 + 3
-        t = ncu_traffic("k_sort_pass", self.pass_bytes / 16 / self.active_passes)
+        t = ncu_traffic("k_sort_pass", pairs / self.active_passes)
         self.traffic_per_launch = t["bytes"]
         self.traffic_source = t
 
@@ -308,21 +313,24 @@ class SortSmjWorkload(Workload):
             if hasattr(self, name):
                 delattr(self, name)
 
-    def _run(self, ku, rows, kz, rk, rp, sk, sp):
+    def _run(self, ku, kz, rk, rp, sk, sp):
         ops = self.ops
-        ops.sort_kernel(self.ctx, ku, rows, out=self.ou, out_ptr=self.oup)
-        ops.sort_kernel(self.ctx, kz, rows, out=self.oz, out_ptr=self.ozp)
+        ops.sort_kernel(self.ctx, ku, None, out=self.ou, out_ptr=self.oup)
+        ops.sort_kernel(self.ctx, kz, None, out=self.oz, out_ptr=self.ozp)
         ops.sort_merge_join(self.ctx, rk, rp, sk, sp, out_inner=self.ji, out_outer=self.jo,
                             result=self.res)
 
     def step(self):
-        self._run(self.ku, self.rows, self.kz, self.rk, self.rp, self.sk, self.sp)
+        self._run(self.ku, self.kz, self.rk, self.rp, self.sk, self.sp)
 
     def step_e2e(self, stream):
         """Pinned host inputs -> device -> pinned host outputs through the public
         API, pipelined over three streams ordered by events: the upload of an
         operator's inputs, the previous operator's compute and the download of
-        an earlier operator's outputs overlap (PCIe is full duplex)."""
+        an earlier operator's outputs overlap (PCIe is full duplex).  The sorts
+        upload their keys only (the row ids are made on the device) and
+        download sorted keys and row ids; the join uploads keys and payloads
+        and downloads the (R payload, S payload) pairs."""
         import torch
         if not hasattr(self, "_streams"):
             self._streams = [torch.cuda.Stream() for _ in range(3)]
@@ -333,7 +341,7 @@ class SortSmjWorkload(Workload):
         for s in self._streams:
             s.wait_event(start)
         outs = (self.ou, self.oup, self.oz, self.ozp, self.ji, self.jo)
-        plan = [((0, 1), (0, 1)), ((2,), (2, 3)), ((3, 4, 5, 6), (4, 5))]
+        plan = [((0,), (0, 1)), ((1,), (2, 3)), ((2, 3, 4, 5), (4, 5))]
         for g, (ins, outs_idx) in enumerate(plan):
             with torch.cuda.stream(up):
                 for i in ins:
@@ -342,11 +350,11 @@ class SortSmjWorkload(Workload):
             e_in.record(up)
             comp.wait_event(e_in)
             if g == 0:
-                ops.sort_kernel(ctx, d[0], d[1], out=self.ou, out_ptr=self.oup, stream=comp)
+                ops.sort_kernel(ctx, d[0], None, out=self.ou, out_ptr=self.oup, stream=comp)
             elif g == 1:
-                ops.sort_kernel(ctx, d[2], d[1], out=self.oz, out_ptr=self.ozp, stream=comp)
+                ops.sort_kernel(ctx, d[1], None, out=self.oz, out_ptr=self.ozp, stream=comp)
             else:
-                ops.sort_merge_join(ctx, d[3], d[4], d[5], d[6], out_inner=self.ji,
+                ops.sort_merge_join(ctx, d[2], d[3], d[4], d[5], out_inner=self.ji,
                                     out_outer=self.jo, result=self.res, stream=comp)
             e_c = torch.cuda.Event()
             e_c.record(comp)
@@ -1214,7 +1222,19 @@ def per_operator(ctx, dev, peak, iters=7) -> dict:
                                 selected=sel)
     t = _timed(lambda: tpch.q1(ctx, li, staged=True), 5, flush, stream)
     out["tpch_q1_staged"] = _op_record(n, t, alg, peak)
-    del li, sw
+    # the multi-table pipelines (Q4, Q3, Q5): chains of plain operators with
+    # the counts read back between steps, as the reference reads its DPUs'
+    # result sizes between launches
+    schema = tpch.Schema(ctx, li)
+    for q in ("q4", "q3", "q5"):
+        fn = getattr(tpch, q)
+        run = lambda fn=fn: fn(ctx, schema)
+        run()
+        t = _timed(run, 5, flush, stream)
+        out[f"tpch_{q}"] = dict(_op_record(n, t, tpch.column_bytes(q, schema), peak,
+                                           _kernel_split(ctx, run, iters=1)),
+                                bytes="columns read once in full (tpch.column_bytes)")
+    del li, sw, schema
     torch.cuda.empty_cache()
     return out
 

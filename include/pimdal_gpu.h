@@ -638,6 +638,34 @@ int pimdal_select_aggregate(pimdal_ctx_t *ctx, const pimdal_select_aggregate_arg
                             pimdal_aggr_results_t *d_result, pimdal_stream_t stream);
 
 /* ------------------------------------------------------------------------- */
+/* Per-row arithmetic: replaces arithmetic_kernel (pimdal/general/            */
+/* arithmetic.c:35-67, arithmetic.h:7-19), which multiplies two columns       */
+/* element by element, and the DPU pipelines' per-row projections such as the */
+/* revenue price * (100 - discount) of                                        */
+/* pimdal/main/tpc_h/query3/dpu/kernel_q3_5.c:107 or the comparison column of */
+/* query4/dpu/kernel_q4_2.c:104-106 (commit - receipt < 0).                    */
+/*                                                                            */
+/* out[i] = expr - minus (each as in pimdal_select_aggregate: the int64       */
+/* product, wrapping, of its terms; minus with 0 terms is 0) at row           */
+/* r = rows ? rows[i] : i, for i < size, shifted right (arithmetically) by    */
+/* shift bits; out_dtype PIMDAL_I64 stores it whole, PIMDAL_I32 its low 32    */
+/* bits (shift = 32: the high word).  With a single column term this is a     */
+/* gather (a load_next) of any column type.                                   */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+  uint64_t size;                /* rows (< 2^32)                                 */
+  const uint32_t *rows;         /* NULL: row i is i                              */
+  pimdal_expr_t expr;           /* 1..PIMDAL_SA_MAX_TERMS terms                  */
+  pimdal_expr_t minus;          /* 0..PIMDAL_SA_MAX_TERMS terms                  */
+  void *out;                    /* size values of out_dtype                      */
+  int32_t out_dtype;            /* PIMDAL_I64 or PIMDAL_I32                      */
+  uint32_t shift;               /* 0..63                                         */
+} pimdal_project_arguments_t;
+
+int pimdal_project(pimdal_ctx_t *ctx, const pimdal_project_arguments_t *args,
+                   pimdal_stream_t stream);
+
+/* ------------------------------------------------------------------------- */
 /* Batched form: many independent group-by or hash-join instances, each phase */
 /* one persistent launch fed by a device work queue.  No reference counterpart */
 /* (the reference runs one operator instance per DPU launch, e.g. the        */

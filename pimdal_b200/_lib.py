@@ -182,6 +182,11 @@ class SelectAggregateArguments(C.Structure):
     ]
 
 
+class ProjectArguments(C.Structure):
+    _fields_ = [("size", C.c_uint64), ("rows", C.c_void_p), ("expr", Expr), ("minus", Expr),
+                ("out", C.c_void_p), ("out_dtype", C.c_int32), ("shift", C.c_uint32)]
+
+
 GROUP_AUTO, GROUP_HASH, GROUP_SORT = 0, 1, 2
 
 
@@ -243,6 +248,7 @@ SIGNATURES = {
     "pimdal_select_join_aggregate_workspace_size": (_I, [C.POINTER(SelectJoinAggregateArguments),
                                                         C.POINTER(_SZ)]),
     "pimdal_select_aggregate": (_I, [_VP, C.POINTER(SelectAggregateArguments), _VP, _VP]),
+    "pimdal_project": (_I, [_VP, C.POINTER(ProjectArguments), _VP]),
     "pimdal_select_aggregate_workspace_size": (_I, [C.POINTER(SelectAggregateArguments),
                                                    C.POINTER(_SZ)]),
     "pimdal_match_workspace_size": (_I, [C.POINTER(MatchArguments), C.POINTER(_SZ)]),

@@ -242,6 +242,74 @@ __global__ void __launch_bounds__(1024) k_sa_emit(const unsigned long long *g_ac
 
 static_assert(PIMDAL_SA_MAX_KEYS <= 1024, "one emit thread per key");
 
+// pimdal_project: the expression at every row, grid-stride, the same term
+// evaluation as the scan above; the output is written coalesced.
+struct PjExpr {
+  SaCol tc[PIMDAL_SA_MAX_TERMS];
+  int64_t tadd[PIMDAL_SA_MAX_TERMS];
+  uint32_t tneg[PIMDAL_SA_MAX_TERMS];
+  uint32_t nterms;  // 0: the expression is absent (0)
+};
+
+struct PjParams {
+  uint64_t n;
+  const uint32_t *rows;
+  PjExpr x[2];  // out = x[0] - x[1]
+  uint32_t out64;
+  uint32_t shift;
+  void *out;
+};
+
+__device__ __forceinline__ void pj_eval(const PjExpr &e, const uint32_t (&row)[SA_UNROLL],
+                                        const bool (&ok)[SA_UNROLL],
+                                        unsigned long long (&val)[SA_UNROLL]) {
+#pragma unroll
+  for (int u = 0; u < SA_UNROLL; ++u) val[u] = e.nterms ? 1ull : 0ull;
+#pragma unroll
+  for (int t = 0; t < PIMDAL_SA_MAX_TERMS; ++t) {
+    if (t < (int)e.nterms) {
+      int64_t x[SA_UNROLL];
+      if (e.tc[t].p) {
+        sa_load_rows(e.tc[t], row, ok, x);
+      } else {
+#pragma unroll
+        for (int u = 0; u < SA_UNROLL; ++u) x[u] = 0;
+      }
+#pragma unroll
+      for (int u = 0; u < SA_UNROLL; ++u)
+        val[u] *= (unsigned long long)((e.tneg[t] ? -x[u] : x[u]) + e.tadd[t]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(SA_THREADS) k_sa_project(PjParams p) {
+  const int tid = threadIdx.x;
+  const uint64_t step = (uint64_t)gridDim.x * SA_THREADS * SA_UNROLL;
+  for (uint64_t base = (uint64_t)blockIdx.x * SA_THREADS * SA_UNROLL; base < p.n; base += step) {
+    uint32_t row[SA_UNROLL];
+    bool ok[SA_UNROLL];
+#pragma unroll
+    for (int u = 0; u < SA_UNROLL; ++u) {
+      const uint64_t i = base + (uint64_t)u * SA_THREADS + tid;
+      ok[u] = i < p.n;
+      row[u] = ok[u] ? (p.rows ? __ldg(p.rows + i) : (uint32_t)i) : 0u;
+    }
+    unsigned long long val[SA_UNROLL], sub[SA_UNROLL];
+    pj_eval(p.x[0], row, ok, val);
+    pj_eval(p.x[1], row, ok, sub);
+#pragma unroll
+    for (int u = 0; u < SA_UNROLL; ++u) val[u] -= sub[u];
+#pragma unroll
+    for (int u = 0; u < SA_UNROLL; ++u) {
+      if (!ok[u]) continue;
+      const uint64_t i = base + (uint64_t)u * SA_THREADS + tid;
+      const long long v = (long long)val[u] >> p.shift;
+      if (p.out64) reinterpret_cast<long long *>(p.out)[i] = v;
+      else reinterpret_cast<uint32_t *>(p.out)[i] = (uint32_t)v;
+    }
+  }
+}
+
 bool sa_dtype_ok(int32_t d) {
   return d == PIMDAL_I32 || d == PIMDAL_U32 || d == PIMDAL_I64 || d == PIMDAL_U8;
 }
@@ -342,6 +410,43 @@ extern "C" int pimdal_select_aggregate(pimdal_ctx_t *ctx,
     pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
     k_sa_emit<<<1, 1024, 0, s>>>(p.g_acc, a->key_space, a->n_exprs, o, &d_result->t_count,
                                  ctx->d_error);
+  }
+  return pd_launch_status(ctx);
+}
+
+extern "C" int pimdal_project(pimdal_ctx_t *ctx, const pimdal_project_arguments_t *a,
+                              pimdal_stream_t stream) {
+  if (!ctx || !a) return PIMDAL_ERR_ARG;
+  if (a->size >= (1ull << 32) || (a->size && !a->out)) return PIMDAL_ERR_ARG;
+  if (a->out_dtype != PIMDAL_I64 && a->out_dtype != PIMDAL_I32) return PIMDAL_ERR_ARG;
+  if (a->shift > 63) return PIMDAL_ERR_ARG;
+  if (a->expr.n_terms == 0) return PIMDAL_ERR_ARG;
+  PjParams p{};
+  p.n = a->size;
+  p.rows = a->rows;
+  for (int k = 0; k < 2; ++k) {
+    const pimdal_expr_t &x = k ? a->minus : a->expr;
+    if (x.n_terms > PIMDAL_SA_MAX_TERMS) return PIMDAL_ERR_ARG;
+    p.x[k].nterms = x.n_terms;
+    for (uint32_t t = 0; t < x.n_terms; ++t) {
+      const pimdal_term_t &term = x.term[t];
+      if (term.col && !sa_dtype_ok(term.dtype)) return PIMDAL_ERR_ARG;
+      p.x[k].tc[t] = {term.col, term.dtype};
+      p.x[k].tadd[t] = term.add;
+      p.x[k].tneg[t] = term.negate != 0;
+    }
+  }
+  p.out64 = a->out_dtype == PIMDAL_I64;
+  p.shift = a->shift;
+  p.out = a->out;
+  if (a->size == 0) return PIMDAL_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaSetDevice(ctx->device);
+  const uint64_t want = pd_ceil_div(a->size, (uint64_t)SA_THREADS * SA_UNROLL);
+  const unsigned grid = (unsigned)std::min<uint64_t>(want, (uint64_t)ctx->sm_count * 8);
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    k_sa_project<<<grid, SA_THREADS, 0, s>>>(p);
   }
   return pd_launch_status(ctx);
 }

@@ -8,9 +8,10 @@
     python -m pimdal_b200.opbench bloom     --rows 268435456 --parts 16384 --match-permille 50
                                              (build = rows / 8; both sides partitioned first,
                                               untimed; times filter + match)
-    python -m pimdal_b200.opbench tpch      --query q6|q1 [--orders 15000000]
-                                             (the fused pass over the lineitem-shaped table
-                                              of the served form; about 4 rows per order)
+    python -m pimdal_b200.opbench tpch      --query q6|q1|q4|q3|q5 [--orders 15000000]
+                                             (q6, q1: the fused pass over the lineitem-shaped
+                                              table of the served form, about 4 rows per order;
+                                              q4, q3, q5: the multi-table pipelines over it)
 
 The per-operator counterpart of the reference's benchmark programs
 (reference/db_operators/*.cpp main: generate, run the kernel a fixed number of
@@ -70,7 +71,8 @@ def _inputs(ctx: ops.Context, a) -> tuple:
         return obk, bps, opk, oprow, pps
     if a.op == "tpch":
         from . import serve, tpch
-        return (tpch.Lineitem(ctx, serve.Tables(ctx, orders=a.orders)),)
+        li = tpch.Lineitem(ctx, serve.Tables(ctx, orders=a.orders))
+        return (li, tpch.Schema(ctx, li) if a.query in ("q3", "q4", "q5") else None)
     if a.op == "group":
         keys = g(gen.Spec(L.GEN_PERM_UNIFORM, L.I32, seed=a.seed, stream_id=10, lo=0,
                           hi=a.card - 1, perm_domain=0), n)
@@ -117,9 +119,11 @@ def _runner(ctx: ops.Context, a, inp):
         return bloom
     if a.op == "tpch":
         from . import tpch
-        li = inp[0]
+        li, schema = inp
         a.rows = li.n
         res = torch.empty(1, dtype=torch.int64, device=dev)
+        if schema is not None:  # the multi-table pipelines: chains of plain operators
+            return lambda: getattr(tpch, a.query)(ctx, schema)
         if a.query == "q6":
             preds, exprs = tpch.q6_args(li)
             run = lambda: ops.select_aggregate(ctx, li.n, preds=preds, exprs=exprs, result=res)
@@ -153,7 +157,8 @@ def main(argv=None) -> None:
     p.add_argument("--load-factor", type=int, default=0, help="hash join table load factor, percent")
     p.add_argument("--parts", type=int, default=16384, help="bloom: partitions (power of 2)")
     p.add_argument("--match-permille", type=int, default=50, help="bloom: probe match rate")
-    p.add_argument("--query", default="q6", choices=["q6", "q1"], help="tpch: the query")
+    p.add_argument("--query", default="q6", choices=["q6", "q1", "q4", "q3", "q5"],
+                   help="tpch: the query")
     p.add_argument("--orders", type=int, default=15_000_000, help="tpch: orders of the table")
     p.add_argument("--device", type=int, default=0)
     p.add_argument("--kernels", action="store_true",

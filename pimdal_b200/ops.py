@@ -445,15 +445,7 @@ def select_aggregate(ctx: Context, size: int, *, preds=(), group=(), key_space: 
     a.key_space = key_space
     a.n_exprs = len(exprs)
     for e, terms in enumerate(exprs):
-        a.expr[e].n_terms = len(terms)
-        for t, term in enumerate(terms):
-            if isinstance(term, int):
-                term = (None, 0, term)
-            elif isinstance(term, torch.Tensor):
-                term = (term, 0, 0)
-            col, neg, add = term[0], term[1], term[2]
-            dt = 0 if col is None else _col_dtype(col, term[3] if len(term) > 3 else None)
-            a.expr[e].term[t] = L.Term(col=_ptr(col), dtype=dt, negate=neg, add=add)
+        a.expr[e] = _expr(terms)
     if outs is None:
         outs = {"key": torch.empty(key_space, dtype=torch.int32, device=dev),
                 "count": torch.empty(key_space, dtype=torch.int64, device=dev)}
@@ -470,6 +462,36 @@ def select_aggregate(ctx: Context, size: int, *, preds=(), group=(), key_space: 
     L.check(ctx.lib.pimdal_select_aggregate(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
             "pimdal_select_aggregate")
     return result, outs
+
+
+def _expr(terms) -> L.Expr:
+    """Expression struct of a list of terms (as select_aggregate's exprs)."""
+    x = L.Expr()
+    x.n_terms = len(terms)
+    for t, term in enumerate(terms):
+        if isinstance(term, int):
+            term = (None, 0, term)
+        elif isinstance(term, torch.Tensor):
+            term = (term, 0, 0)
+        col, neg, add = term[0], term[1], term[2]
+        dt = 0 if col is None else _col_dtype(col, term[3] if len(term) > 3 else None)
+        x.term[t] = L.Term(col=_ptr(col), dtype=dt, negate=neg, add=add)
+    return x
+
+
+def project(ctx: Context, size: int, terms, *, minus=(), rows=None, out=None,
+            out_dtype: int = L.I64, shift: int = 0, stream=None) -> torch.Tensor:
+    """Per-row arithmetic (pimdal_project): out[i] = (the product of `terms`)
+    - (the product of `minus`, 0 when empty) at row rows[i] (or i), shifted
+    right by shift bits.  Terms as select_aggregate's expressions; a single
+    column term makes it a gather of that column."""
+    if out is None:
+        dt = torch.int64 if out_dtype == L.I64 else torch.int32
+        out = torch.empty(max(size, 1), dtype=dt, device=f"cuda:{ctx.device}")
+    a = L.ProjectArguments(size=size, rows=_ptr(rows), expr=_expr(terms), minus=_expr(minus),
+                           out=_ptr(out), out_dtype=out_dtype, shift=shift)
+    L.check(ctx.lib.pimdal_project(ctx.handle, C.byref(a), _stream(stream)), "pimdal_project")
+    return out
 
 
 def revenue_keys(ctx: Context, n: int, match_row, match_attr, sel_rows, price, discount, flag,

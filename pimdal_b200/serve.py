@@ -98,7 +98,7 @@ class Tables:
         dev = f"cuda:{ctx.device}"
         g = lambda spec, n: ops.gen_column(ctx, spec, n)
         U = lambda sid, lo, hi, dt=L.I32: gen.Spec(L.GEN_UNIFORM, dt, seed=seed, stream_id=sid, lo=lo, hi=hi)
-        self.n_orders, self.n_parts = orders, parts
+        self.n_orders, self.n_parts, self.n_supps = orders, parts, supps
         # orders dimension: distinct keys (a seeded sample of [0, 2^31)), date, priority
         self.o_key = g(gen.Spec(L.GEN_PERM, L.I32, seed=seed, perm_domain=1 << 31), orders)
         self.o_date = g(U(1, 0, DAYS - 1), orders)

@@ -1,4 +1,4 @@
-"""The reference's TPC-H Q1 and Q6 pipelines on the C ABI.
+"""The reference's TPC-H pipelines (Q1, Q3, Q4, Q5, Q6) on the C ABI.
 
 The reference runs them as DPU programs over parquet-loaded lineitem columns
 (pimdal/main/tpc_h/query6, pimdal/main/tpc_h/query1).  Here they run over a
@@ -30,6 +30,15 @@ date_to_int("1998-09-02"); per (return flag, line status) group SUM(quantity),
 SUM(price), SUM(price * (100 - discount)), SUM(price * (100 - discount) *
 (100 + tax)), SUM(discount) and COUNT; the averages are the sums divided by
 the count on the host, as aggr_host does (:236-261).
+
+Q4, Q3 and Q5 join several tables; they run over a Schema (lineitem plus
+orders, customer, supplier, nation and region columns of own synthetic
+distributions) as the reference's chains of plain operators: a selection per
+filter, load_next gathers (pimdal_gather_u32, pimdal_project), a hash join
+per join (pimdal_hash_join), per-row arithmetic (pimdal_project) and a
+group-by (pimdal_group_kernel, pimdal_select_aggregate), with the counts read
+back between steps as the reference's hosts read their DPUs' result sizes.
+Market segments, regions and nations are dictionary codes.
 """
 from __future__ import annotations
 
@@ -182,3 +191,276 @@ def algorithmic_bytes_q1(n: int, selected: int) -> int:
     """The ship date of every row; flag, status (1 B each), quantity,
     discount, tax (4 B) and price (8 B) of the selected rows."""
     return 4 * n + 22 * selected
+
+
+# ---------------------------------------------------------------------------
+# Q4, Q3 and Q5: the reference's multi-table pipelines
+# ---------------------------------------------------------------------------
+Q4_DATE_LO, Q4_DATE_HI = "1993-07-01", "1993-10-01"  # host_q4.cpp:47-48 (populate_mram_1)
+Q3_DATE = "1995-03-15"                               # host_q3.cpp:72,98
+Q5_DATE_LO, Q5_DATE_HI = "1994-01-01", "1995-01-01"  # host_q5.cpp:83-84
+N_SEGMENT, N_NATION, N_REGION = 5, 25, 5
+Q3_SEGMENT = 1  # the market-segment code the query selects (host_q3.cpp:46 names one segment)
+Q5_REGION = 2   # the region code the query selects (host_q5.cpp:58 names one region)
+DATE_SLACK = 31  # days before the first and after the last ship day the date columns reach
+
+
+class Schema:
+    """Lineitem plus the orders, customer, supplier, nation and region columns
+    the multi-table pipelines read, all resident in HBM.
+
+    Own synthetic distributions (seeded; no TPC-H data or generator exists
+    here): orders keep the served table's keys, order day and priority code
+    and add a customer key U[1, customers] and a ship-priority code U[0, 3];
+    customers are keyed 1..customers with a market-segment code
+    U[0, N_SEGMENT) and a nation U[0, N_NATION); suppliers are keyed
+    1..suppliers (the lineitem's supplier keys) with a nation
+    U[0, N_NATION); nation k lies in region k mod N_REGION; a lineitem's
+    commit day is its ship day + U[-30, 30], its receipt day its ship day +
+    U[1, 30].  Dates are packed as the reference's reader packs them
+    (date_to_int)."""
+
+    def __init__(self, ctx: ops.Context, li: Lineitem, customers: int | None = None,
+                 seed: int = 0xB20B):
+        t = li.tables
+        dev = f"cuda:{ctx.device}"
+        g = lambda spec, n: ops.gen_column(ctx, spec, n)
+        U = lambda sid, lo, hi: gen.Spec(L.GEN_UNIFORM, L.I32, seed=seed, stream_id=sid, lo=lo, hi=hi)
+        self.li = li
+        self.n = li.n
+        self.n_orders = t.n_orders
+        self.n_cust = customers if customers is not None else max(t.n_orders // 10, 1)
+        self.n_supp = t.n_supps
+        first = (FIRST_DAY - np.datetime64("1970-01-01")).astype(np.int64) - DATE_SLACK
+        days = first + np.arange(serve.DAYS + 2 * DATE_SLACK)
+        lut = torch.from_numpy(np.ascontiguousarray(
+            ingest.date_to_int(pa.array(days.astype(np.int32), type=pa.date32())), np.int32)).to(dev)
+        # orders
+        self.o_orderkey, self.o_orderpriority = t.o_key, t.o_prio
+        self.o_orderdate = lut[t.o_date.long() + DATE_SLACK].contiguous()
+        self.o_custkey = g(U(1, 1, self.n_cust), self.n_orders)
+        self.o_shippriority = g(U(2, 0, 3), self.n_orders)
+        # customers
+        self.c_custkey = torch.arange(1, self.n_cust + 1, dtype=torch.int32, device=dev)
+        self.c_mktsegment = g(U(3, 0, N_SEGMENT - 1), self.n_cust)
+        self.c_nationkey = g(U(4, 0, N_NATION - 1), self.n_cust)
+        # suppliers, nations, regions
+        self.s_suppkey = torch.arange(1, self.n_supp + 1, dtype=torch.int32, device=dev)
+        self.s_nationkey = g(U(5, 0, N_NATION - 1), self.n_supp)
+        self.n_nationkey = torch.arange(N_NATION, dtype=torch.int32, device=dev)
+        self.n_regionkey = (self.n_nationkey % N_REGION).contiguous()
+        self.r_regionkey = torch.arange(N_REGION, dtype=torch.int32, device=dev)
+        self.r_name = self.r_regionkey.clone()  # region name codes
+        # lineitem commit and receipt dates around the ship day
+        day = t.l_date.long() + DATE_SLACK
+        self.l_commitdate = lut[day + g(U(6, -30, 30), self.n).long()].contiguous()
+        self.l_receiptdate = lut[day + g(U(7, 1, 30), self.n).long()].contiguous()
+        del day
+        ctx.sync()
+
+
+def _count(ctx, res, stream) -> int:
+    ctx.sync(stream)
+    return int(res.item())
+
+
+@dataclass
+class Q4Result:
+    priority: np.ndarray    # order-priority codes present, ascending
+    order_count: np.ndarray  # orders of the date range with a late lineitem, per priority
+
+
+def q4(ctx: ops.Context, s: Schema, stream=None) -> Q4Result:
+    """Q4 after pimdal/main/tpc_h/query4/dpu/kernel_q4_1.c..kernel_q4_4.c and
+    host/host_q4.cpp:210-233: the orders whose order date lies in
+    [Q4_DATE_LO, Q4_DATE_HI) (kernel_q4_1.c: pred_o) that have at least one
+    lineitem with commit date < receipt date (kernel_q4_2.c: pred_l), joined
+    on the order key and made distinct per order (kernel_q4_3.c: hash_kernel,
+    merge_kernel, group_kernel with `unique`), counted per order priority
+    (kernel_q4_4.c, aggr_host) and ordered by priority."""
+    lo, hi = packed(Q4_DATE_LO), packed(Q4_DATE_HI)
+    r_o, _, o_rows = ops.sel_kernel(ctx, s.o_orderdate, ops.make_pred(L.PRED_RANGE, lo, hi),
+                                    stream=stream)
+    late = ops.project(ctx, s.n, [s.l_commitdate], minus=[s.l_receiptdate], out_dtype=L.I32,
+                       stream=stream)  # commit - receipt
+    r_l, _, l_rows = ops.sel_kernel(ctx, late, ops.make_pred(L.PRED_LT, 0), stream=stream)
+    k_o, k_l = _count(ctx, r_o, stream), _count(ctx, r_l, stream)
+    del late
+    if k_o == 0 or k_l == 0:
+        return Q4Result(np.zeros(0, np.int64), np.zeros(0, np.int64))
+    o_keys = ops.gather_u32(ctx, s.o_orderkey, o_rows, k_o, stream=stream)
+    l_keys = ops.gather_u32(ctx, s.li.tables.l_orderkey, l_rows, k_l, stream=stream)
+    r_j, o_match, _ = ops.hash_join(ctx, o_keys[:k_o], o_rows[:k_o], l_keys[:k_l], capacity=k_l,
+                                    stream=stream)
+    m = _count(ctx, r_j, stream)
+    if m == 0:
+        return Q4Result(np.zeros(0, np.int64), np.zeros(0, np.int64))
+    r_g, outs = ops.group_kernel(ctx, o_match[:m], None, want=("count",), expected_groups=k_o,
+                                 capacity=k_o, stream=stream)
+    nd = _count(ctx, r_g, stream)
+    r_p, po = ops.select_aggregate(ctx, nd, rows=outs["key"][:nd],
+                                   group=[(s.o_orderpriority, 1)], key_space=serve.N_PRIO,
+                                   stream=stream)
+    gp = _count(ctx, r_p, stream)
+    return Q4Result(po["key"][:gp].cpu().numpy().astype(np.int64),
+                    po["count"][:gp].cpu().numpy())
+
+
+@dataclass
+class Q3Result:
+    orderkey: np.ndarray      # the 10 orders of the largest revenue, descending
+    revenue: np.ndarray       # SUM(price * (100 - discount)) over the order's lineitems
+    orderdate: np.ndarray
+    shippriority: np.ndarray
+    groups: int               # orders with a qualifying lineitem
+
+
+def q3(ctx: ops.Context, s: Schema, top: int = 10, stream=None) -> Q3Result:
+    """Q3 after pimdal/main/tpc_h/query3/dpu/kernel_q3_1.c..kernel_q3_5.c and
+    host/host_q3.cpp:46,72,98,279-315: customers of one market segment
+    (kernel_q3_1.c: pred_c); their orders dated before Q3_DATE
+    (kernel_q3_2.c: pred_o, kernel_q3_3.c: the join on the customer key);
+    the lineitems shipped after Q3_DATE (kernel_q3_4.c: pred_l) of those
+    orders (kernel_q3_5.c: the join on the order key) with revenue
+    price * (100 - discount) (kernel_q3_5.c:107) summed per order
+    (group_kernel with sum), then the `top` orders by revenue, descending
+    (the per-DPU sort_kernel and the host's merge of the DPUs' lists).
+    Equal revenues are ordered by ascending order row."""
+    d = packed(Q3_DATE)
+    li, t = s.li, s.li.tables
+    r_c, _, c_rows = ops.sel_kernel(ctx, s.c_mktsegment, ops.make_pred(L.PRED_EQ, Q3_SEGMENT),
+                                    stream=stream)
+    r_o, _, o_rows = ops.sel_kernel(ctx, s.o_orderdate, ops.make_pred(L.PRED_LT, d), stream=stream)
+    r_l, _, l_rows = ops.sel_kernel(ctx, li.shipdate, ops.make_pred(L.PRED_GT, d), stream=stream)
+    k_c, k_o, k_l = _count(ctx, r_c, stream), _count(ctx, r_o, stream), _count(ctx, r_l, stream)
+    empty = Q3Result(*(np.zeros(0, np.int64) for _ in range(4)), 0)
+    if min(k_c, k_o, k_l) == 0:
+        return empty
+    c_keys = ops.gather_u32(ctx, s.c_custkey, c_rows, k_c, stream=stream)
+    o_cust = ops.gather_u32(ctx, s.o_custkey, o_rows, k_o, stream=stream)
+    # orders of those customers: build the customer keys, probe the orders' customer keys
+    r1, _, o_idx = ops.hash_join(ctx, c_keys[:k_c], c_rows[:k_c], o_cust[:k_o], capacity=k_o,
+                                 stream=stream)
+    m1 = _count(ctx, r1, stream)
+    if m1 == 0:
+        return empty
+    q_rows = ops.gather_u32(ctx, o_rows, o_idx, m1, stream=stream)
+    q_keys = ops.gather_u32(ctx, s.o_orderkey, q_rows, m1, stream=stream)
+    l_keys = ops.gather_u32(ctx, t.l_orderkey, l_rows, k_l, stream=stream)
+    # lineitems of those orders: build the order keys (payload: order row)
+    r2, o_of, l_idx = ops.hash_join(ctx, q_keys[:m1], q_rows[:m1], l_keys[:k_l], capacity=k_l,
+                                    stream=stream)
+    m2 = _count(ctx, r2, stream)
+    if m2 == 0:
+        return empty
+    l_row = ops.gather_u32(ctx, l_rows, l_idx, m2, stream=stream)
+    rev = ops.project(ctx, m2, [li.price, (li.discount, 1, 100)], rows=l_row, stream=stream)
+    r3, outs = ops.group_kernel(ctx, o_of[:m2], rev[:m2], want=("sum",), expected_groups=m1,
+                                capacity=m1, stream=stream)
+    ng = _count(ctx, r3, stream)
+    # descending revenue: two stable sorts of the 64-bit key ~revenue, by its
+    # low word (unsigned) and then by its high word (signed)
+    sums = outs["sum"][:ng]
+    lo32 = ops.project(ctx, ng, [(sums, 1, -1)], out_dtype=L.I32, stream=stream)
+    hi32 = ops.project(ctx, ng, [(sums, 1, -1)], out_dtype=L.I32, shift=32, stream=stream)
+    _, perm1 = ops.sort_kernel(ctx, lo32[:ng], None, key_dtype=L.U32, stream=stream)
+    hi_p = ops.gather_u32(ctx, hi32, perm1, ng, stream=stream)
+    _, perm = ops.sort_kernel(ctx, hi_p[:ng], perm1, key_dtype=L.I32, stream=stream)
+    k = min(top, ng)
+    ctx.sync(stream)
+    sel = perm[:k].long()
+    rows = outs["key"][:ng][sel]
+    c = lambda x: x.cpu().numpy().astype(np.int64)
+    return Q3Result(c(s.o_orderkey[rows.long()]), c(sums[sel]), c(s.o_orderdate[rows.long()]),
+                    c(s.o_shippriority[rows.long()]), ng)
+
+
+@dataclass
+class Q5Result:
+    nation: np.ndarray   # nation codes, by revenue descending (ties: ascending code)
+    revenue: np.ndarray  # SUM(price * (100 - discount))
+
+
+def q5(ctx: ops.Context, s: Schema, stream=None) -> Q5Result:
+    """Q5 after pimdal/main/tpc_h/query5/dpu/kernel_q5_1.c..kernel_q5_7.c and
+    host/host_q5.cpp:58,83-84,440-500: the nations of one region
+    (kernel_q5_1.c: pred_r, the joins region-nation and nation-customer),
+    their customers' orders dated in [Q5_DATE_LO, Q5_DATE_HI), those orders'
+    lineitems, and their suppliers, keeping the lineitems whose supplier
+    lies in the customer's nation; revenue price * (100 - discount) summed
+    per nation (hash_sum by n_nationkey) and ordered by revenue, descending."""
+    lo, hi = packed(Q5_DATE_LO), packed(Q5_DATE_HI)
+    li, t = s.li, s.li.tables
+    empty = Q5Result(np.zeros(0, np.int64), np.zeros(0, np.int64))
+    r_r, _, r_rows = ops.sel_kernel(ctx, s.r_name, ops.make_pred(L.PRED_EQ, Q5_REGION), stream=stream)
+    k_r = _count(ctx, r_r, stream)
+    if k_r == 0:
+        return empty
+    r_keys = ops.gather_u32(ctx, s.r_regionkey, r_rows, k_r, stream=stream)
+    # nations of the region (payload: nation key), then their customers
+    r1, _, n_idx = ops.hash_join(ctx, r_keys[:k_r], r_keys[:k_r], s.n_regionkey, stream=stream)
+    k_n = _count(ctx, r1, stream)
+    if k_n == 0:
+        return empty
+    n_keys = ops.gather_u32(ctx, s.n_nationkey, n_idx, k_n, stream=stream)
+    r2, c_nat, c_rows = ops.hash_join(ctx, n_keys[:k_n], n_keys[:k_n], s.c_nationkey, stream=stream)
+    k_c = _count(ctx, r2, stream)
+    r_o, _, o_rows = ops.sel_kernel(ctx, s.o_orderdate, ops.make_pred(L.PRED_RANGE, lo, hi),
+                                    stream=stream)
+    k_o = _count(ctx, r_o, stream)
+    if k_c == 0 or k_o == 0:
+        return empty
+    c_keys = ops.gather_u32(ctx, s.c_custkey, c_rows, k_c, stream=stream)
+    o_cust = ops.gather_u32(ctx, s.o_custkey, o_rows, k_o, stream=stream)
+    # orders of those customers (payload: the customer's nation)
+    r3, o_nat, o_idx = ops.hash_join(ctx, c_keys[:k_c], c_nat[:k_c], o_cust[:k_o], capacity=k_o,
+                                     stream=stream)
+    m_o = _count(ctx, r3, stream)
+    if m_o == 0:
+        return empty
+    q_rows = ops.gather_u32(ctx, o_rows, o_idx, m_o, stream=stream)
+    q_keys = ops.gather_u32(ctx, s.o_orderkey, q_rows, m_o, stream=stream)
+    # their lineitems (payload: the customer's nation)
+    r4, l_nat, l_row = ops.hash_join(ctx, q_keys[:m_o], o_nat[:m_o], t.l_orderkey, stream=stream)
+    m_l = _count(ctx, r4, stream)
+    if m_l == 0:
+        return empty
+    # the lineitems' suppliers (payload: the supplier's nation)
+    l_supp = ops.gather_u32(ctx, t.l_suppkey, l_row, m_l, stream=stream)
+    r5, s_nat, s_idx = ops.hash_join(ctx, s.s_suppkey, s.s_nationkey, l_supp[:m_l], capacity=m_l,
+                                     stream=stream)
+    m_s = _count(ctx, r5, stream)
+    c_nat2 = ops.gather_u32(ctx, l_nat, s_idx, m_s, stream=stream)
+    row2 = ops.gather_u32(ctx, l_row, s_idx, m_s, stream=stream)
+    same = ops.project(ctx, m_s, [s_nat], minus=[c_nat2], out_dtype=L.I32, stream=stream)
+    r6, _, keep = ops.sel_kernel(ctx, same[:m_s], ops.make_pred(L.PRED_EQ, 0), stream=stream)
+    k = _count(ctx, r6, stream)
+    rev = ops.project(ctx, m_s, [li.price, (li.discount, 1, 100)], rows=row2, stream=stream)
+    r7, outs = ops.select_aggregate(ctx, k, rows=keep[:k] if k else keep,
+                                    group=[(c_nat2, 1)], key_space=N_NATION, exprs=[[rev]],
+                                    stream=stream)
+    g = _count(ctx, r7, stream)
+    nation = outs["key"][:g].cpu().numpy().astype(np.int64)
+    revenue = outs["sum0"][:g].cpu().numpy()
+    order = np.lexsort((nation, -revenue))  # host_q5.cpp:493: order by revenue, descending
+    return Q5Result(nation[order], revenue[order])
+
+
+def column_bytes(query: str, s: Schema) -> int:
+    """Bytes of the columns a multi-table query reads, each once in full (4 B
+    per key, date, code or discount, 8 B per price): Q4 reads the orders'
+    date, key and priority and the lineitems' commit date, receipt date and
+    order key; Q3 the customers' segment and key, the orders' date, customer
+    key, key and ship priority, and the lineitems' ship date, order key,
+    price and discount; Q5 the customers' nation and key, the orders' date,
+    customer key and key, the lineitems' order key, supplier key, price and
+    discount, the suppliers' key and nation, and the nation and region
+    columns."""
+    o, n, c, sp = s.n_orders, s.n, s.n_cust, s.n_supp
+    if query == "q4":
+        return 12 * o + 12 * n
+    if query == "q3":
+        return 8 * c + 16 * o + 20 * n
+    if query == "q5":
+        return 8 * c + 12 * o + 20 * n + 8 * sp + 8 * N_NATION + 8 * N_REGION
+    raise ValueError(query)

@@ -97,6 +97,13 @@ def test_select_aggregate_layout_and_argument_errors_need_no_gpu():
     assert lib.pimdal_select_aggregate_workspace_size(ctypes.byref(a), ctypes.byref(sz)) == 1
 
 
+def test_project_layout_and_argument_errors_need_no_gpu():
+    lib = L.lib()
+    a = L.ProjectArguments()
+    assert ctypes.sizeof(a) == 8 + 8 + 2 * (L.SA_MAX_TERMS * 24 + 8) + 8 + 4 + 4
+    assert lib.pimdal_project(None, ctypes.byref(a), None) == 1
+
+
 def test_tpch_packed_dates_follow_the_reference_reader():
     from pimdal_b200 import tpch
     # read_table.cpp:8-16: day + (month << 5) + ((year - 1900) << 9)
