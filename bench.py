@@ -1128,6 +1128,10 @@ def per_operator(ctx, dev, peak, iters=7) -> dict:
                            ("hash_join_zipf_cfg3", 3, gen.zipf_cdf(nb, 0.75))):
         pk = g(gen.Spec(L.GEN_PROBE, L.I32, seed=s3, stream_id=sid, lo=nb, perm_domain=2 * nb,
                         match_permille=500, cdf=cdf), npr)
+        # the autotuner picks the partition fan-out and load factor for this
+        # shape (the Zipf probe has the uniform one's shape: the cached choice)
+        tuning, _, _, _, _ = ops.hash_join_autotune(ctx, bk, bp, pk, capacity=npr,
+                                                    out_payload=opay, out_row=orow, result=res)
         run = lambda: ops.hash_join(ctx, bk, bp, pk, capacity=npr, out_payload=opay,
                                     out_row=orow, result=res)
         run()
@@ -1138,7 +1142,7 @@ def per_operator(ctx, dev, peak, iters=7) -> dict:
         alg = 8 * nb + 4 * npr + 8 * m
         out[name] = dict(_op_record(nb + npr, t, alg, peak, split, "hj_probe",
                                     8 * npr + 8 * m, ncu_traffic("k_hj_probe", npr)),
-                         matches=m, build_rows=nb, probe_rows=npr)
+                         matches=m, build_rows=nb, probe_rows=npr, tuning=tuning)
         del pk
     del bk, bp, opay, orow
     torch.cuda.empty_cache()
@@ -1154,6 +1158,11 @@ def per_operator(ctx, dev, peak, iters=7) -> dict:
         keys = g(gen.Spec(L.GEN_PERM_UNIFORM, L.I32, seed=s3, stream_id=10 + i, lo=0, hi=c - 1,
                           perm_domain=0), n)
         for mname, method in (("hash", L.GROUP_HASH), ("sort", L.GROUP_SORT)):
+            tuning = None
+            if method == L.GROUP_HASH:  # the autotuner's mode for this shape (if any choice)
+                tuning, _, _, _ = ops.group_autotune(ctx, keys, vals, method=method,
+                                                     expected_groups=c, capacity=cap, outs=outs,
+                                                     result=res)
             run = lambda: ops.group_kernel(ctx, keys, vals, method=method, expected_groups=c,
                                            capacity=cap, outs=outs, result=res)
             run()
@@ -1168,7 +1177,7 @@ def per_operator(ctx, dev, peak, iters=7) -> dict:
                 tr = ncu_traffic("k_gb_chunks" if c > 4608 else "k_gb_aggregate_shared", n)
             out[f"group_{mname}_{c}_cfg3"] = dict(
                 _op_record(n, t, alg, peak, split, dom, 12 * n if method == L.GROUP_HASH else None, tr),
-                groups=groups)
+                groups=groups, **({"tuning": tuning} if tuning else {}))
         del keys
     del vals, outs
     torch.cuda.empty_cache()

@@ -713,6 +713,39 @@ int pimdal_batch_autotune(pimdal_ctx_t *ctx, int kind, const void *args, uint32_
                           void *d_results, pimdal_batch_tuning_t *best, int *cached,
                           pimdal_stream_t stream);
 
+/* ------------------------------------------------------------------------- */
+/* Autotuner of the plain operators (the batch autotuner's counterpart for    */
+/* single calls).  The hash join's partition fan-out and table load factor    */
+/* and the high-cardinality hash group-by's mode (hash-partitioned chunks or  */
+/* one direct global table) and partition count are chosen per input shape.   */
+/* pimdal_*_autotune runs the call once per candidate on the given arguments  */
+/* (writing the outputs; the last run is the chosen candidate's), keeps the   */
+/* fastest in the context under the call's shape (the log2 of its sizes; for  */
+/* the join also the L2 budget; for the group-by the expected groups and      */
+/* whether values are given), and returns it.  A later call of the same       */
+/* shape whose arguments leave the choice to the library (hash join:          */
+/* partition_bits = 0 and load_factor_pct = 0; group-by: method HASH or AUTO) */
+/* uses it; a later autotune of a cached shape returns it without running     */
+/* (*cached = 1).  The workspace-size queries of such calls cover every       */
+/* candidate.  A group-by with nothing to choose (few groups, the sort       */
+/* method) runs once with the library's choice and returns group_mode 0.     */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+  uint32_t partition_bits;   /* hash join: 0xFFFFFFFF = unpartitioned, else 1..8       */
+  uint32_t load_factor_pct;  /* hash join: table load factor in percent                */
+  uint32_t group_mode;       /* group-by: 0 library's choice, 1 partitioned, 2 direct  */
+  uint32_t group_part_bits;  /* group-by, partitioned: log2 of the hash partitions     */
+  float ms;                  /* the chosen candidate's device time (0 when not timed)  */
+  uint32_t candidates;       /* candidates timed (0 when cached or nothing to choose)  */
+} pimdal_tuning_t;
+
+int pimdal_hash_join_autotune(pimdal_ctx_t *ctx, const pimdal_hash_join_arguments_t *args,
+                              pimdal_merge_results_t *d_result, pimdal_tuning_t *best,
+                              int *cached, pimdal_stream_t stream);
+int pimdal_group_autotune(pimdal_ctx_t *ctx, const pimdal_aggr_arguments_t *args,
+                          pimdal_aggr_results_t *d_result, pimdal_tuning_t *best, int *cached,
+                          pimdal_stream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -215,6 +215,15 @@ class BatchTuning(C.Structure):
 
 BATCH_GROUP, BATCH_HASH_JOIN = 0, 1
 
+
+class Tuning(C.Structure):
+    _fields_ = [("partition_bits", C.c_uint32), ("load_factor_pct", C.c_uint32),
+                ("group_mode", C.c_uint32), ("group_part_bits", C.c_uint32),
+                ("ms", C.c_float), ("candidates", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
 # Exported symbols and their ctypes signatures.
 _VP, _SZ, _U64, _I = C.c_void_p, C.c_size_t, C.c_uint64, C.c_int
 SIGNATURES = {
@@ -267,6 +276,10 @@ SIGNATURES = {
     "pimdal_batch_device_bytes": (_I, [_VP, C.POINTER(_SZ)]),
     "pimdal_batch_destroy": (_I, [_VP]),
     "pimdal_batch_autotune": (_I, [_VP, _I, _VP, C.c_uint32, _VP, C.POINTER(BatchTuning),
+                                   C.POINTER(_I), _VP]),
+    "pimdal_hash_join_autotune": (_I, [_VP, C.POINTER(HashJoinArguments), _VP,
+                                       C.POINTER(Tuning), C.POINTER(_I), _VP]),
+    "pimdal_group_autotune": (_I, [_VP, C.POINTER(AggrArguments), _VP, C.POINTER(Tuning),
                                    C.POINTER(_I), _VP]),
 }
 

@@ -67,6 +67,8 @@ struct pimdal_ctx {
   double prof_ms[PIMDAL_KERNEL_COUNT] = {};
   // batch autotuner: best tuning per batch shape
   std::map<std::vector<uint64_t>, pimdal_batch_tuning_t> tune_cache;
+  // plain-operator autotuner: best tuning per call shape
+  std::map<std::vector<uint64_t>, pimdal_tuning_t> op_tune;
   // pimdal_ingest: pinned staging buffers (one per host copy thread) and the
   // events of their last transfers
   void *stage[PD_INGEST_MAX_THREADS] = {};
@@ -86,6 +88,33 @@ struct pd_launch_scope {
 // Returns a workspace of at least `bytes` (256-byte aligned) or nullptr with
 // *status set.  Grows an owned workspace; a caller-provided one is never grown.
 void *pd_workspace(pimdal_ctx *ctx, size_t bytes, cudaStream_t stream, int *status);
+
+// ceil(log2(x)) for x >= 1 (0 for x <= 1): the size class of a tuning shape.
+inline uint64_t pd_log2_ceil(uint64_t x) {
+  uint64_t b = 0;
+  while ((1ull << b) < x && b < 63) ++b;
+  return b;
+}
+
+// Device milliseconds of run() on stream s (events around it, waited for);
+// a negative value when run() or the device reported an error, which is then
+// read and cleared from the context.
+template <typename F>
+float pd_time_call(pimdal_ctx *ctx, cudaStream_t s, F run) {
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return -1.f;
+  if (cudaEventCreate(&e1) != cudaSuccess) { cudaEventDestroy(e0); return -1.f; }
+  cudaEventRecord(e0, s);
+  const int st = run();
+  cudaEventRecord(e1, s);
+  float ms = -1.f;
+  if (st == PIMDAL_OK && pimdal_ctx_sync_status(ctx, s) == PIMDAL_OK &&
+      cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess)
+    ms = -1.f;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return st == PIMDAL_OK ? ms : -1.f;
+}
 
 // Next lookback epoch (1..65535); clears the status words when it wraps.
 uint32_t pd_next_epoch(pimdal_ctx *ctx, cudaStream_t stream, int *status);

@@ -1003,7 +1003,14 @@ uint64_t gb_l2_budget() {
   return b;
 }
 
-bool gb_layout(const pimdal_aggr_arguments_t *a, GbLayout *l) {
+// An autotuned choice for the high-cardinality hash modes: mode GB_PART with
+// 2^part_bits partitions, or GB_DIRECT; mode < 0 keeps the library's choice.
+struct GbTune {
+  int mode = -1;
+  uint32_t part_bits = 0;
+};
+
+bool gb_layout(const pimdal_aggr_arguments_t *a, GbLayout *l, const GbTune *tune = nullptr) {
   const bool sort = a->method == PIMDAL_GROUP_SORT;
   size_t o = 0;
   pimdal_sort_arguments_t sa{};
@@ -1025,11 +1032,14 @@ bool gb_layout(const pimdal_aggr_arguments_t *a, GbLayout *l) {
   expect = std::max<uint64_t>(expect, 1);
   l->mode = expect <= GB_WARP_MAX_GROUPS ? GB_WARP : expect <= GB_SMEM_MAX_GROUPS ? GB_SMEM
           : gb_force_direct() ? GB_DIRECT : GB_PART;
+  if (tune && tune->mode >= 0 && l->mode >= GB_DIRECT) l->mode = tune->mode;
   l->part_bits = 0;
   l->pkey = l->pval = 0;
   if (l->mode == GB_PART) {
     uint32_t b = 1;
     while (b < GB_PART_MAX_BITS && (expect >> b) > GB_PART_GROUPS) ++b;
+    if (tune && tune->mode == GB_PART && tune->part_bits >= 1 && tune->part_bits <= GB_PART_MAX_BITS)
+      b = tune->part_bits;
     l->part_bits = b;
   }
   // GB_WARP replicas: keep each replica's load at or below 1/3
@@ -1126,16 +1136,116 @@ int pd_gb_batch_run(pimdal_ctx *ctx, const pd_gb_batch &b, cudaStream_t s) {
   return pd_launch_status(ctx);
 }
 
+namespace {
+// The autotuner's candidates for a high-cardinality hash group-by: the
+// partitioned mode at the suggested partition count and its neighbours, and
+// the direct global table.  Empty when there is nothing to choose.
+std::vector<GbTune> gb_candidates(const pimdal_aggr_arguments_t *a) {
+  std::vector<GbTune> c;
+  GbLayout l;
+  if (a->method == PIMDAL_GROUP_SORT || !gb_layout(a, &l) || l.mode < GB_DIRECT) return c;
+  GbLayout p;
+  GbTune t;
+  t.mode = GB_PART;
+  if (!gb_layout(a, &p, &t)) return c;
+  for (int d = -1; d <= 1; ++d) {
+    const int b = (int)p.part_bits + d;
+    if (b < 1 || b > (int)GB_PART_MAX_BITS) continue;
+    t.part_bits = (uint32_t)b;
+    c.push_back(t);
+  }
+  t.mode = GB_DIRECT;
+  t.part_bits = 0;
+  c.push_back(t);
+  return c;
+}
+
+std::vector<uint64_t> gb_shape(const pimdal_aggr_arguments_t *a) {
+  const uint64_t outs = (a->out_sum != nullptr) | (a->out_count != nullptr) << 1 |
+                        (a->out_min != nullptr) << 2 | (a->out_max != nullptr) << 3;
+  return {2, pd_log2_ceil(a->size), pd_log2_ceil(a->expected_groups), a->in_val != nullptr, outs};
+}
+
+GbTune gb_cached(const pimdal_ctx *ctx, const pimdal_aggr_arguments_t *a) {
+  GbTune t;
+  if (a->method == PIMDAL_GROUP_SORT) return t;
+  const auto it = ctx->op_tune.find(gb_shape(a));
+  if (it != ctx->op_tune.end() && it->second.group_mode) {
+    t.mode = it->second.group_mode == 1 ? GB_PART : GB_DIRECT;
+    t.part_bits = it->second.group_part_bits;
+  }
+  return t;
+}
+}  // namespace
+
 extern "C" int pimdal_group_workspace_size(const pimdal_aggr_arguments_t *a, size_t *bytes) {
   if (!a || !bytes) return PIMDAL_ERR_ARG;
   GbLayout l;
   if (!gb_layout(a, &l)) return PIMDAL_ERR_ARG;
   *bytes = l.total;
+  for (const auto &t : gb_candidates(a)) {  // a tuned choice may be used instead
+    GbLayout m;
+    if (gb_layout(a, &m, &t)) *bytes = std::max(*bytes, m.total);
+  }
   return PIMDAL_OK;
 }
 
+namespace {
+int group_kernel_tuned(pimdal_ctx_t *ctx, const pimdal_aggr_arguments_t *a,
+                       pimdal_aggr_results_t *d_result, pimdal_stream_t stream,
+                       const GbTune &tune);
+}  // namespace
+
 extern "C" int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_arguments_t *a,
                                    pimdal_aggr_results_t *d_result, pimdal_stream_t stream) {
+  if (!ctx || !a || !d_result) return PIMDAL_ERR_ARG;
+  return group_kernel_tuned(ctx, a, d_result, stream, gb_cached(ctx, a));
+}
+
+extern "C" int pimdal_group_autotune(pimdal_ctx_t *ctx, const pimdal_aggr_arguments_t *a,
+                                     pimdal_aggr_results_t *d_result, pimdal_tuning_t *best,
+                                     int *cached, pimdal_stream_t stream) {
+  if (!ctx || !a || !d_result || !best) return PIMDAL_ERR_ARG;
+  if (cached) *cached = 0;
+  *best = pimdal_tuning_t{};
+  const auto cands = gb_candidates(a);
+  if (cands.empty())  // nothing to choose: the library's choice
+    return pimdal_group_kernel(ctx, a, d_result, stream);
+  const auto key = gb_shape(a);
+  const auto it = ctx->op_tune.find(key);
+  if (it != ctx->op_tune.end()) {
+    *best = it->second;
+    best->candidates = 0;
+    if (cached) *cached = 1;
+    return PIMDAL_OK;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  float best_ms = -1.f;
+  size_t best_i = 0;
+  for (size_t i = 0; i < cands.size(); ++i) {
+    auto run = [&] { return group_kernel_tuned(ctx, a, d_result, stream, cands[i]); };
+    if (pd_time_call(ctx, s, run) < 0.f) continue;  // warm-up
+    const float ms = pd_time_call(ctx, s, run);
+    if (ms >= 0.f && (best_ms < 0.f || ms < best_ms)) {
+      best_ms = ms;
+      best_i = i;
+    }
+  }
+  if (best_ms < 0.f) return PIMDAL_ERR_CUDA;
+  pimdal_tuning_t t{};
+  t.group_mode = cands[best_i].mode == GB_PART ? 1 : 2;
+  t.group_part_bits = cands[best_i].part_bits;
+  t.ms = best_ms;
+  t.candidates = (uint32_t)cands.size();
+  ctx->op_tune[key] = t;
+  *best = t;
+  return group_kernel_tuned(ctx, a, d_result, stream, cands[best_i]);
+}
+
+namespace {
+int group_kernel_tuned(pimdal_ctx_t *ctx, const pimdal_aggr_arguments_t *a,
+                       pimdal_aggr_results_t *d_result, pimdal_stream_t stream,
+                       const GbTune &tune) {
   if (!ctx || !a || !d_result) return PIMDAL_ERR_ARG;
   if (a->key_dtype != PIMDAL_I32 && a->key_dtype != PIMDAL_U32) return PIMDAL_ERR_ARG;
   if (a->method != PIMDAL_GROUP_AUTO && a->method != PIMDAL_GROUP_HASH &&
@@ -1150,7 +1260,7 @@ extern "C" int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_argument
     return PIMDAL_OK;
   }
   GbLayout l;
-  if (!gb_layout(a, &l)) return PIMDAL_ERR_ARG;
+  if (!gb_layout(a, &l, &tune)) return PIMDAL_ERR_ARG;
   int st;
   char *ws = (char *)pd_workspace(ctx, l.total, s, &st);
   if (!ws) return st;
@@ -1316,3 +1426,4 @@ extern "C" int pimdal_group_kernel(pimdal_ctx_t *ctx, const pimdal_aggr_argument
   }
   return pd_launch_status(ctx);
 }
+}  // namespace

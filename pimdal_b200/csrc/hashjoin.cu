@@ -146,12 +146,17 @@ __device__ __forceinline__ void hj_insert(const JoinParams &p, uint32_t k, uint3
   bool dup = false;
   for (uint64_t t = 0; t <= gmask && !done; ++t) {
     unsigned long long *b = p.table + 4 * (uint64_t)g;
+    // the whole bucket (one 32-byte sector) in two loads from L2; a slot a
+    // concurrent insert has filled may still read empty, and its CAS then
+    // returns the filled word, so duplicates are still seen
+    const ulonglong2 lo = __ldcg(reinterpret_cast<const ulonglong2 *>(b));
+    const ulonglong2 hi = __ldcg(reinterpret_cast<const ulonglong2 *>(b) + 1);
+    const unsigned long long cur[4] = {lo.x, lo.y, hi.x, hi.y};
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       if (done) break;
-      const unsigned long long cur = b[j];
-      if (cur != HJ_EMPTY) {
-        dup |= (uint32_t)cur == k;
+      if (cur[j] != HJ_EMPTY) {
+        dup |= (uint32_t)cur[j] == k;
         continue;
       }
       const unsigned long long old = atomicCAS(b + j, HJ_EMPTY, e);
@@ -638,17 +643,64 @@ int pd_hj_batch_run(pimdal_ctx *ctx, const pd_hj_batch &b, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // pimdal_hash_join
 // ---------------------------------------------------------------------------
+namespace {
+// The autotuner's candidates: the partition fan-out the L2 budget suggests
+// (at load factor 1/2) and its neighbours, times load factors 35/50/70 %.
+std::vector<pimdal_hash_join_arguments_t> hj_candidates(const pimdal_hash_join_arguments_t *a) {
+  std::vector<pimdal_hash_join_arguments_t> c;
+  pimdal_hash_join_arguments_t t = *a;
+  t.partition_bits = 0;
+  t.load_factor_pct = 50;
+  HjLayout l;
+  if (!hj_layout(&t, &l)) return c;
+  for (int d = -1; d <= 1; ++d) {
+    const int pb = (int)l.part_bits + d;
+    if (pb < 0 || pb > 8) continue;
+    for (uint32_t lf : {35u, 50u, 70u}) {
+      t.partition_bits = pb == 0 ? 0xFFFFFFFFu : (uint32_t)pb;
+      t.load_factor_pct = lf;
+      HjLayout m;
+      if (hj_layout(&t, &m)) c.push_back(t);
+    }
+  }
+  return c;
+}
+
+std::vector<uint64_t> hj_shape(const pimdal_hash_join_arguments_t *a) {
+  return {1, pd_log2_ceil(a->size_build), pd_log2_ceil(a->size_probe), a->l2_budget_bytes};
+}
+
+bool hj_auto(const pimdal_hash_join_arguments_t *a) {
+  return a->partition_bits == 0 && a->load_factor_pct == 0;
+}
+}  // namespace
+
 extern "C" int pimdal_hash_join_workspace_size(const pimdal_hash_join_arguments_t *a, size_t *bytes) {
   if (!a || !bytes) return PIMDAL_ERR_ARG;
   HjLayout l;
   if (!hj_layout(a, &l)) return PIMDAL_ERR_ARG;
   *bytes = l.total;
+  if (hj_auto(a)) {  // a tuned choice may be used instead: cover every candidate
+    for (const auto &c : hj_candidates(a)) {
+      HjLayout m;
+      if (hj_layout(&c, &m)) *bytes = std::max(*bytes, m.total);
+    }
+  }
   return PIMDAL_OK;
 }
 
-extern "C" int pimdal_hash_join(pimdal_ctx_t *ctx, const pimdal_hash_join_arguments_t *a,
+extern "C" int pimdal_hash_join(pimdal_ctx_t *ctx, const pimdal_hash_join_arguments_t *a_in,
                                 pimdal_merge_results_t *d_result, pimdal_stream_t stream) {
-  if (!ctx || !a || !d_result) return PIMDAL_ERR_ARG;
+  if (!ctx || !a_in || !d_result) return PIMDAL_ERR_ARG;
+  pimdal_hash_join_arguments_t eff = *a_in;
+  if (hj_auto(a_in)) {  // the autotuner's choice for this shape, if any
+    const auto it = ctx->op_tune.find(hj_shape(a_in));
+    if (it != ctx->op_tune.end()) {
+      eff.partition_bits = it->second.partition_bits;
+      eff.load_factor_pct = it->second.load_factor_pct;
+    }
+  }
+  const pimdal_hash_join_arguments_t *a = &eff;
   if ((a->size_build && !a->build_key) || (a->size_probe && !a->probe_key)) return PIMDAL_ERR_ARG;
   if (a->out_capacity && (!a->out_build_payload || !a->out_probe_ptr)) return PIMDAL_ERR_ARG;
   if (a->size_build >= (1ull << 32) || a->size_probe >= (1ull << 30)) return PIMDAL_ERR_ARG;
@@ -1178,4 +1230,43 @@ extern "C" int pimdal_select_join_aggregate(pimdal_ctx_t *ctx,
                                   a->out_count, a->out_capacity, &d_result->t_count, ctx->d_error);
   }
   return pd_launch_status(ctx);
+}
+
+extern "C" int pimdal_hash_join_autotune(pimdal_ctx_t *ctx, const pimdal_hash_join_arguments_t *a,
+                                         pimdal_merge_results_t *d_result, pimdal_tuning_t *best,
+                                         int *cached, pimdal_stream_t stream) {
+  if (!ctx || !a || !d_result || !best) return PIMDAL_ERR_ARG;
+  if (cached) *cached = 0;
+  const auto key = hj_shape(a);
+  const auto it = ctx->op_tune.find(key);
+  if (it != ctx->op_tune.end()) {
+    *best = it->second;
+    best->candidates = 0;
+    if (cached) *cached = 1;
+    return PIMDAL_OK;
+  }
+  const auto cands = hj_candidates(a);
+  if (cands.empty()) return PIMDAL_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  float best_ms = -1.f;
+  size_t best_i = 0;
+  for (size_t i = 0; i < cands.size(); ++i) {
+    auto run = [&] { return pimdal_hash_join(ctx, &cands[i], d_result, stream); };
+    if (pd_time_call(ctx, s, run) < 0.f) continue;  // warm-up (workspace, caches)
+    const float ms = pd_time_call(ctx, s, run);
+    if (ms >= 0.f && (best_ms < 0.f || ms < best_ms)) {
+      best_ms = ms;
+      best_i = i;
+    }
+  }
+  if (best_ms < 0.f) return PIMDAL_ERR_CUDA;
+  pimdal_tuning_t t{};
+  t.partition_bits = cands[best_i].partition_bits;
+  t.load_factor_pct = cands[best_i].load_factor_pct;
+  t.ms = best_ms;
+  t.candidates = (uint32_t)cands.size();
+  ctx->op_tune[key] = t;
+  *best = t;
+  // the outputs are the chosen candidate's
+  return pimdal_hash_join(ctx, &cands[best_i], d_result, stream);
 }

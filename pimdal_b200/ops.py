@@ -369,6 +369,37 @@ def hash_join(ctx: Context, build_key, build_payload, probe_key, probe_ptr=None,
     return result, out_payload, out_row
 
 
+def hash_join_autotune(ctx: Context, build_key, build_payload, probe_key, probe_ptr=None, *,
+                       capacity: int | None = None, l2_budget_bytes: int = 0, out_payload=None,
+                       out_row=None, result=None, stream=None):
+    """pimdal_hash_join_autotune: times the candidate partition fan-outs and
+    load factors on these inputs (writing the outputs) and caches the fastest
+    for this shape; later hash_join calls of the shape with partition_bits=0
+    and load_factor_pct=0 use it.  Returns (tuning dict, cached, result,
+    out_payload, out_row)."""
+    dev = probe_key.device
+    if capacity is None:
+        capacity = max(probe_key.numel(), 1)
+    if out_payload is None:
+        out_payload = torch.empty(capacity, dtype=torch.int32, device=dev)
+    if out_row is None:
+        out_row = torch.empty(capacity, dtype=torch.int32, device=dev)
+    if result is None:
+        result = torch.empty(1, dtype=torch.int64, device=dev)
+    a = L.HashJoinArguments(build_key=_ptr(build_key), build_payload=_ptr(build_payload),
+                            size_build=build_key.numel(), probe_key=_ptr(probe_key),
+                            probe_ptr=_ptr(probe_ptr), size_probe=probe_key.numel(),
+                            out_build_payload=_ptr(out_payload), out_probe_ptr=_ptr(out_row),
+                            out_capacity=capacity, partition_bits=0, load_factor_pct=0,
+                            l2_budget_bytes=l2_budget_bytes)
+    _workspace(ctx, ctx.lib.pimdal_hash_join_workspace_size, a)
+    t, cached = L.Tuning(), C.c_int()
+    L.check(ctx.lib.pimdal_hash_join_autotune(ctx.handle, C.byref(a), _ptr(result), C.byref(t),
+                                              C.byref(cached), _stream(stream)),
+            "pimdal_hash_join_autotune")
+    return t.as_dict(), bool(cached.value), result, out_payload, out_row
+
+
 # ---------------------------------------------------------------------------
 # Group-by (group_kernel, pimdal/aggregate/aggregate.h:25)
 # ---------------------------------------------------------------------------
@@ -395,6 +426,36 @@ def group_kernel(ctx: Context, keys, vals=None, *, method: int = L.GROUP_HASH,
     L.check(ctx.lib.pimdal_group_kernel(ctx.handle, C.byref(a), _ptr(result), _stream(stream)),
             "pimdal_group_kernel")
     return result, outs
+
+
+def group_autotune(ctx: Context, keys, vals=None, *, method: int = L.GROUP_HASH,
+                   key_dtype: int = L.I32, expected_groups: int = 0, capacity: int | None = None,
+                   want=("sum", "count", "min", "max"), outs=None, result=None, stream=None):
+    """pimdal_group_autotune: for a high-cardinality hash group-by, times the
+    partitioned mode at a few partition counts and the direct global table on
+    these inputs (writing the outputs) and caches the fastest for this shape;
+    later group_kernel calls of the shape use it.  Returns (tuning dict,
+    cached, result, outs)."""
+    dev = keys.device
+    n = keys.numel()
+    if capacity is None:
+        capacity = max(1, min(n, expected_groups * 2 if expected_groups else n))
+    if outs is None:
+        outs = {w: torch.empty(capacity, dtype=torch.int64, device=dev) for w in want}
+        outs["key"] = torch.empty(capacity, dtype=torch.int32, device=dev)
+    if result is None:
+        result = torch.empty(1, dtype=torch.int64, device=dev)
+    a = L.AggrArguments(size=n, in_=_ptr(keys), in_val=_ptr(vals), out=_ptr(outs.get("key")),
+                        out_sum=_ptr(outs.get("sum")), out_count=_ptr(outs.get("count")),
+                        out_min=_ptr(outs.get("min")), out_max=_ptr(outs.get("max")),
+                        out_capacity=capacity, expected_groups=expected_groups,
+                        key_dtype=key_dtype, method=method)
+    _workspace(ctx, ctx.lib.pimdal_group_workspace_size, a)
+    t, cached = L.Tuning(), C.c_int()
+    L.check(ctx.lib.pimdal_group_autotune(ctx.handle, C.byref(a), _ptr(result), C.byref(t),
+                                          C.byref(cached), _stream(stream)),
+            "pimdal_group_autotune")
+    return t.as_dict(), bool(cached.value), result, outs
 
 
 # ---------------------------------------------------------------------------

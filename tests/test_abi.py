@@ -104,6 +104,15 @@ def test_project_layout_and_argument_errors_need_no_gpu():
     assert lib.pimdal_project(None, ctypes.byref(a), None) == 1
 
 
+def test_autotune_layout_and_argument_errors_need_no_gpu():
+    lib = L.lib()
+    assert ctypes.sizeof(L.Tuning) == 24
+    t, c = L.Tuning(), ctypes.c_int()
+    assert lib.pimdal_hash_join_autotune(None, None, None, ctypes.byref(t), ctypes.byref(c),
+                                         None) == 1
+    assert lib.pimdal_group_autotune(None, None, None, ctypes.byref(t), ctypes.byref(c), None) == 1
+
+
 def test_tpch_packed_dates_follow_the_reference_reader():
     from pimdal_b200 import tpch
     # read_table.cpp:8-16: day + (month << 5) + ((year - 1900) << 9)

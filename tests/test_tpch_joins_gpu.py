@@ -27,9 +27,12 @@ def host(s: tpch.Schema) -> dict:
 
 
 def order_row_of(h, keys):
-    """Row of each order key in the orders table (keys must exist)."""
+    """Row of each order key in the orders table (keys must exist); the
+    queries are searched in sorted order, which keeps large lookups fast."""
     srt = np.argsort(h["o_key"], kind="stable")
-    pos = np.searchsorted(h["o_key"][srt], keys)
+    qo = np.argsort(keys, kind="stable")
+    pos = np.empty(keys.size, np.int64)
+    pos[qo] = np.searchsorted(h["o_key"][srt], keys[qo])
     return srt[pos]
 
 
@@ -42,21 +45,26 @@ def numpy_q4(h):
     return pr, cnt[pr]
 
 
+def group_sum(keys, vals):
+    """(distinct keys ascending, exact int64 sums) by a stable sort."""
+    o = np.argsort(keys, kind="stable")
+    k, v = keys[o], vals[o]
+    if k.size == 0:
+        return k, v
+    starts = np.concatenate(([0], np.nonzero(k[1:] != k[:-1])[0] + 1))
+    return k[starts], np.add.reduceat(v, starts)
+
+
 def numpy_q3(h, top=10):
     d = tpch.packed(tpch.Q3_DATE)
     custs = np.nonzero(h["c_seg"] == tpch.Q3_SEGMENT)[0] + 1          # customer keys
     o_ok = (h["o_date"] < d) & np.isin(h["o_cust"], custs)
     l_ok = (h["l_ship"] > d) & np.isin(h["l_okey"], h["o_key"][o_ok])
     orow = order_row_of(h, h["l_okey"][l_ok])
-    rev = h["price"][l_ok] * (100 - h["disc"][l_ok])
-    sums = np.zeros(h["o_key"].size, np.int64)
-    np.add.at(sums, orow, rev)
-    has = np.zeros(h["o_key"].size, bool)
-    has[orow] = True
-    rows = np.nonzero(has)[0]
-    order = np.lexsort((rows, -sums[rows]))[:top]
+    rows, sums = group_sum(orow, h["price"][l_ok] * (100 - h["disc"][l_ok]))
+    order = np.lexsort((rows, -sums))[:top]
     r = rows[order]
-    return h["o_key"][r], sums[r], h["o_date"][r], h["o_ship"][r], rows.size
+    return h["o_key"][r], sums[order], h["o_date"][r], h["o_ship"][r], rows.size
 
 
 def numpy_q5(h):
@@ -69,12 +77,9 @@ def numpy_q5(h):
     cn = cust_nat[orow]
     sn = h["s_nat"][h["l_supp"] - 1]
     keep = l_ok & (cn == sn)
-    rev = np.zeros(tpch.N_NATION, np.int64)
-    np.add.at(rev, cn[keep], h["price"][keep] * (100 - h["disc"][keep]))
-    has = np.bincount(cn[keep], minlength=tpch.N_NATION) > 0
-    nat = np.nonzero(has)[0]
-    order = np.lexsort((nat, -rev[nat]))
-    return nat[order], rev[nat][order]
+    nat, rev = group_sum(cn[keep], h["price"][keep] * (100 - h["disc"][keep]))
+    order = np.lexsort((nat, -rev))
+    return nat[order], rev[order]
 
 
 @pytest.fixture(scope="module")
@@ -112,6 +117,24 @@ def test_q5_matches_numpy(ctx, schema):
     nat, rev = numpy_q5(h)
     got = tpch.q5(ctx, s)
     assert nat.size > 0
+    assert np.array_equal(got.nation, nat) and np.array_equal(got.revenue, rev)
+
+
+def test_q4_q3_q5_full_schema(ctx):
+    """The 6e7-row lineitem table of the served form with 1.5e7 orders and
+    1.5e6 customers: every query equals its numpy restatement."""
+    s = tpch.Schema(ctx, tpch.Lineitem(ctx))
+    h = host(s)
+    pr, cnt = numpy_q4(h)
+    got = tpch.q4(ctx, s)
+    assert np.array_equal(got.priority, pr) and np.array_equal(got.order_count, cnt)
+    okey, rev, odate, ship, ng = numpy_q3(h)
+    got = tpch.q3(ctx, s)
+    assert got.groups == ng and np.array_equal(got.orderkey, okey)
+    assert np.array_equal(got.revenue, rev) and np.array_equal(got.orderdate, odate)
+    assert np.array_equal(got.shippriority, ship)
+    nat, rev = numpy_q5(h)
+    got = tpch.q5(ctx, s)
     assert np.array_equal(got.nation, nat) and np.array_equal(got.revenue, rev)
 
 
