@@ -564,6 +564,10 @@ int probe_grid(pimdal_ctx *ctx) {
   return per_sm * ctx->sm_count;
 }
 
+#ifndef PD_HJ_ONE_TABLE
+#define PD_HJ_ONE_TABLE 1
+#endif
+
 struct HjLayout {
   uint32_t bits, part_bits;
   size_t table, side, boff, poff, tilebase, bk, bp, pk, pr, sort_ws, total;
@@ -582,7 +586,11 @@ bool hj_layout(const pimdal_hash_join_arguments_t *a, HjLayout *l) {
   }
   if (pb > 8 || pb >= bits) return false;
   l->part_bits = pb;
+#if PD_HJ_ONE_TABLE
+  l->bits = bits;  // one table; partition q's rows touch only its slice q
+#else
   l->bits = bits - pb;  // slots of one partition's table
+#endif
   size_t o = 0;
   l->table = o; o += pd_align_up(8ull << l->bits, 256);
   l->side = o; o += 256;
@@ -645,7 +653,8 @@ int pd_hj_batch_run(pimdal_ctx *ctx, const pd_hj_batch &b, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 namespace {
 // The autotuner's candidates: the partition fan-out the L2 budget suggests
-// (at load factor 1/2) and its neighbours, times load factors 35/50/70 %.
+// (at load factor 1/2) and two neighbours either side, times load factors
+// 35/50/70 %.
 std::vector<pimdal_hash_join_arguments_t> hj_candidates(const pimdal_hash_join_arguments_t *a) {
   std::vector<pimdal_hash_join_arguments_t> c;
   pimdal_hash_join_arguments_t t = *a;
@@ -653,7 +662,7 @@ std::vector<pimdal_hash_join_arguments_t> hj_candidates(const pimdal_hash_join_a
   t.load_factor_pct = 50;
   HjLayout l;
   if (!hj_layout(&t, &l)) return c;
-  for (int d = -1; d <= 1; ++d) {
+  for (int d = -2; d <= 2; ++d) {
     const int pb = (int)l.part_bits + d;
     if (pb < 0 || pb > 8) continue;
     for (uint32_t lf : {35u, 50u, 70u}) {
@@ -781,6 +790,36 @@ extern "C" int pimdal_hash_join(pimdal_ctx_t *ctx, const pimdal_hash_join_argume
   const unsigned clear_grid = (unsigned)std::min<uint64_t>(pd_ceil_div(1ull << l.bits, 512), ctx->sm_count * 8ull);
   const unsigned build_grid = ctx->sm_count * 8;
   const int pgrid = probe_grid(ctx);
+#if PD_HJ_ONE_TABLE
+  if (l.part_bits) {
+    // One table of 2^bits slots for all partitions, one build and one probe
+    // launch over the partitioned rows.  A key's home bucket is the top bits
+    // of the same hash whose top part_bits chose its partition, so the rows of
+    // partition q touch only slice q of the table: the slice being built or
+    // probed stays L2-resident, and no launch waits for a partition's tail.
+    p.boff = p.poff = nullptr;
+    p.tilebase = nullptr;
+    p.part_bits = 0;
+    p.part = 0;
+    {
+      pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+      k_hj_clear<<<clear_grid, 256, 0, s>>>(p);
+    }
+    {
+      pd_launch_scope sc(ctx, PIMDAL_KERNEL_HJ_BUILD, s);
+      k_hj_build<<<build_grid, 256, 0, s>>>(p);
+    }
+    {
+      pd_launch_scope sc(ctx, PIMDAL_KERNEL_HJ_PROBE, s);
+      k_hj_probe<<<pgrid, HJ_THREADS, 0, s>>>(p);
+    }
+    {
+      pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+      k_hj_count<<<1, 1, 0, s>>>(p.status, nullptr, 1, total_tiles_direct, p.epoch, p.d_count);
+    }
+    return pd_launch_status(ctx);
+  }
+#endif
   for (uint32_t q = 0; q < parts; ++q) {
     p.part = q;
     {
