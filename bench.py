@@ -50,7 +50,7 @@ NCU_TRAFFIC = {
                     "profiles/k_sort_pass_2p25_pairs.md"),
     "k_select_coop": ((537.0e6 + 39.6e6) / 2**26, "row",
                       "profiles/k_select_coop_2p26.md (2^26 rows; at 2^24 the second read hits L2)"),
-    "k_hj_probe": ((170.2e6 + 24.4e6) / 2**24, "partitioned probe row",
+    "k_hj_probe": ((339.5e6 + 90.9e6) / 2**25, "partitioned probe row",
                    "profiles/k_hj_probe_2p25_probe.md"),
     "k_gb_aggregate_shared": ((403.1e6 + 5.9e6) / 2**25, "row",
                               "profiles/k_gb_aggregate_2p25_rows.md (4096 groups)"),
