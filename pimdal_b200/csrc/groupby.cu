@@ -1375,8 +1375,12 @@ int group_kernel_tuned(pimdal_ctx_t *ctx, const pimdal_aggr_arguments_t *a,
     p.key = (const uint32_t *)(ws + l.pkey);
     p.val = pval;
     p.vec = 1;
-    // a chunk holds about one partition's rows, so about GB_PART_GROUPS groups
-    const uint64_t chunk = std::max<uint64_t>(4096, pd_align_up(a->size >> l.part_bits, 1024));
+    // a chunk holds at most about one partition's rows, so at most about
+    // 2 * GB_PART_GROUPS groups; with few partitions it is cut further so
+    // that every SM gets several chunks
+    const uint64_t per_sm = pd_ceil_div(a->size, 8ull * ctx->sm_count);
+    const uint64_t chunk = std::max<uint64_t>(
+        4096, pd_align_up(std::min<uint64_t>(a->size >> l.part_bits, per_sm), 1024));
     const unsigned grid = (unsigned)std::min<uint64_t>(pd_ceil_div(a->size, chunk), ctx->sm_count);
     const size_t smem = pd_gb_batch_shared_bytes();
     pd_launch_scope sc(ctx, PIMDAL_KERNEL_GROUP, s);
