@@ -375,12 +375,14 @@ int pimdal_hj_probe(pimdal_ctx_t *ctx, const pimdal_probe_arguments_t *args,
 
 /* Whole hash join (the pipeline of pimdal/main/join/hash and
  * reference/db_operators/hash_join.cpp:159-219).  A table that fits
- * l2_budget_bytes is built and probed directly; a larger one is processed
- * partition by partition (both relations radix-partitioned by hash bits), so
- * every table being probed is L2-resident.  Output per match: build payload
- * and probe row id; partitions in order, probe order within a partition
- * (probe order overall when not partitioned).  With duplicate build keys the
- * matches of one probe row come in table order. */
+ * l2_budget_bytes is built and probed directly; for a larger one both
+ * relations are first radix-partitioned by the top bits of the key hash
+ * whose next bits give a key's home bucket, so the rows of one partition
+ * touch one L2-sized slice of the table, and the partitioned rows are built
+ * and probed in partition order.  Output per match: build payload and probe
+ * row id; partitions in order, probe order within a partition (probe order
+ * overall when not partitioned).  With duplicate build keys the matches of
+ * one probe row come in table order. */
 typedef struct {
   const void *build_key;          /* uint32 / int32 keys                          */
   const uint32_t *build_payload;  /* NULL = build row id                          */
