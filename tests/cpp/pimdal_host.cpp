@@ -209,11 +209,53 @@ void run_group_by(const std::string &dir) {
   write_file(dir + "/gb_max.i64", x.fetch(a.out_max, g).data(), g);
 }
 
+// TPC-H Q6 as the reference's pipeline runs it (pimdal/main/tpc_h/query6/
+// dpu/kernel_q6.c:112-156: three selections, the product price * discount,
+// the sum), here one pimdal_select_aggregate call over the resident columns.
+void run_q6(const std::string &dir, int64_t date_lo, int64_t date_hi, int64_t quantity,
+            int64_t discount) {
+  Session x;
+  const auto date = read_file<int32_t>(dir + "/q6_date.i32");
+  const auto qty = read_file<int32_t>(dir + "/q6_qty.i32");
+  const auto disc = read_file<int32_t>(dir + "/q6_disc.i32");
+  const auto price = read_file<int64_t>(dir + "/q6_price.i64");
+  pimdal_select_aggregate_arguments_t a = {};
+  a.size = date.size();
+  a.n_preds = 3;
+  a.pred[0] = {x.populate(date), PIMDAL_I32, 0, {PIMDAL_PRED_RANGE, 0, date_lo, date_hi}};
+  a.pred[1] = {x.populate(qty), PIMDAL_I32, 0, {PIMDAL_PRED_LT, 0, quantity, 0}};
+  a.pred[2] = {x.populate(disc), PIMDAL_I32, 0,
+               {PIMDAL_PRED_BETWEEN, 0, discount - 1, discount + 1}};
+  a.key_space = 1;
+  a.n_exprs = 1;
+  a.expr[0].n_terms = 2;
+  a.expr[0].term[0] = {x.populate(price), PIMDAL_I64, 0, 0};
+  a.expr[0].term[1] = {a.pred[2].col, PIMDAL_I32, 0, 0};
+  a.out_key = x.alloc<uint32_t>(1);
+  a.out_count = x.alloc<int64_t>(1);
+  a.out_sum[0] = x.alloc<int64_t>(1);
+  a.out_capacity = 1;
+  size_t ws = 0;
+  check(pimdal_select_aggregate_workspace_size(&a, &ws), "pimdal_select_aggregate_workspace_size");
+  check(pimdal_ctx_set_workspace(x.ctx, x.alloc<char>(ws), ws), "pimdal_ctx_set_workspace");
+  auto *d_res = x.alloc<pimdal_aggr_results_t>(1);
+  check(pimdal_select_aggregate(x.ctx, &a, d_res, x.s), "pimdal_select_aggregate");
+  const uint64_t g = x.count(&d_res->t_count);
+  int64_t out[2] = {0, 0};  // revenue, rows
+  if (g) {
+    out[0] = x.fetch(a.out_sum[0], 1)[0];
+    out[1] = x.fetch(a.out_count, 1)[0];
+  }
+  write_file(dir + "/q6_out.i64", out, 2);
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
   if (argc < 3) {
-    std::fprintf(stderr, "usage: %s <dir> select <lo> <hi> | sort | hash_join | group_by\n", argv[0]);
+    std::fprintf(stderr,
+                 "usage: %s <dir> select <lo> <hi> | sort | hash_join | group_by |"
+                 " q6 <date_lo> <date_hi> <quantity> <discount>\n", argv[0]);
     return PIMDAL_ERR_ARG;
   }
   const std::string dir = argv[1], op = argv[2];
@@ -222,6 +264,8 @@ int main(int argc, char **argv) {
     else if (op == "sort") run_sort(dir);
     else if (op == "hash_join") run_hash_join(dir);
     else if (op == "group_by") run_group_by(dir);
+    else if (op == "q6" && argc == 7)
+      run_q6(dir, std::atoll(argv[3]), std::atoll(argv[4]), std::atoll(argv[5]), std::atoll(argv[6]));
     else throw Failure{PIMDAL_ERR_ARG, "unknown operation " + op};
   } catch (const Failure &f) {
     std::fprintf(stderr, "%s: %s\n", f.where.c_str(), pimdal_status_string(f.status));

@@ -2,8 +2,9 @@
 includes include/pimdal_gpu.h and links libpimdal_b200.so, as the reference's
 host programs (pimdal/main/*/host) would after the drop-in.  It is built with
 g++ here (no GPU needed) and, on a GPU, runs selection, sort, hash join and
-group-by on the golden fixtures' inputs; its outputs must equal the golden
-outputs, which come from the reference's own CPU operators."""
+group-by on the golden fixtures' inputs -- its outputs must equal the golden
+outputs, which come from the reference's own CPU operators -- and the TPC-H
+Q6 pipeline through the fused scan, checked against a numpy restatement."""
 import os
 import shutil
 import subprocess
@@ -97,3 +98,25 @@ def test_cpp_caller_group_by_matches_golden(host_exe, tmp_path):
         assert np.array_equal(np.fromfile(tmp_path / "gb_key.i32", np.int32), g[f"key_{i}"])
         for c in ("sum", "count", "min", "max"):
             assert np.array_equal(np.fromfile(tmp_path / f"gb_{c}.i64", np.int64), g[f"{c}_{i}"]), c
+
+
+@pytest.mark.gpu
+def test_cpp_caller_tpch_q6_matches_numpy(host_exe, tmp_path, ctx):
+    """The Q6 pipeline of pimdal/main/tpc_h/query6 run by the C++ host through
+    pimdal_select_aggregate, on the synthetic lineitem columns, against the
+    numpy restatement of host_q6.cpp:70-100."""
+    from pimdal_b200 import serve, tpch
+    li = tpch.Lineitem(ctx, serve.Tables(ctx, orders=100_000, parts=5_000, supps=1_000, seed=17))
+    h = {"date": li.shipdate.cpu().numpy(), "qty": li.quantity.cpu().numpy(),
+         "disc": li.discount.cpu().numpy(), "price": li.price.cpu().numpy()}
+    h["date"].astype(np.int32).tofile(tmp_path / "q6_date.i32")
+    h["qty"].astype(np.int32).tofile(tmp_path / "q6_qty.i32")
+    h["disc"].astype(np.int32).tofile(tmp_path / "q6_disc.i32")
+    h["price"].astype(np.int64).tofile(tmp_path / "q6_price.i64")
+    lo, hi = tpch.packed(tpch.Q6_DATE_LO), tpch.packed(tpch.Q6_DATE_HI)
+    run(host_exe, tmp_path, "q6", lo, hi, tpch.Q6_QUANTITY, tpch.Q6_DISCOUNT)
+    revenue, rows = np.fromfile(tmp_path / "q6_out.i64", np.int64)
+    m = (h["date"] >= lo) & (h["date"] < hi) & (h["qty"] < tpch.Q6_QUANTITY)
+    m &= (h["disc"] >= tpch.Q6_DISCOUNT - 1) & (h["disc"] <= tpch.Q6_DISCOUNT + 1)
+    assert rows == m.sum() > 0
+    assert revenue == int((h["disc"][m].astype(np.int64) * h["price"][m]).sum())
