@@ -574,15 +574,31 @@ struct PartShape {
 
 enum : int { PV_NONE = 0, PV_U32 = 1, PV_U64 = 2 };  // values carried by the pass
 
+// Dynamic shared memory of a partition pass: the staging buffer; with 64-bit
+// values the packed counters share it (they are dead once the positions are
+// computed), so that three CTAs fit on an SM.
+constexpr size_t pp_smem_bytes(int bits, int val) {
+  const int b = bits < 2 ? 2 : bits;
+  const size_t stage = (size_t)(val == PV_U64 ? 12 : val == PV_U32 ? 8 : 4) * RS_TILE;
+  const size_t cnt = val == PV_U64 ? 4 * ((size_t)(1 << (b - 1)) * RS_THREADS + RS_THREADS) : 0;
+  return stage > cnt ? stage : cnt;
+}
+
+__device__ __forceinline__ void prefetch_l2(const void *ptr) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+}
+
 template <int BITS, int VAL, int KEY_MODE>
-__global__ void __launch_bounds__(RS_THREADS, VAL == PV_U64 ? 2 : 3)
+__global__ void __launch_bounds__(RS_THREADS, 3)
 k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
   using S = PartShape<BITS>;
   constexpr bool HAS_VALS = VAL == PV_U32;
   constexpr bool V64 = VAL == PV_U64;
-  // staging: RS_TILE (key, value) words, keys alone, or keys then 64-bit values
+  // staging: RS_TILE (key, value) words, keys alone, or keys then 64-bit
+  // values (and, before the staging, their packed counters)
   extern __shared__ __align__(16) uint2 pp_stage[];
-  __shared__ uint32_t s_cnt[S::WORDS];
+  __shared__ uint32_t s_cnt_own[V64 ? 1 : S::WORDS];
+  uint32_t *s_cnt = V64 ? reinterpret_cast<uint32_t *>(pp_stage) : s_cnt_own;
   __shared__ uint32_t s_warp[RS_WARPS];
   __shared__ uint32_t s_dstart[S::B + 1];
   __shared__ int32_t s_gdelta[S::B];
@@ -631,7 +647,13 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
   // 1. load this thread's consecutive items
   uint32_t key[PP_ITEMS];
   uint32_t val[HAS_VALS ? PP_ITEMS : 1];
-  unsigned long long v64[V64 ? PP_ITEMS : 1];
+  if (V64) {
+    // 64-bit values are loaded only when they are staged (step 5), which
+    // keeps them out of the registers meanwhile; their lines go to L2 now
+    const char *vb = reinterpret_cast<const char *>(sv64);
+    const uint32_t lines = (tile_n * 8u + 127u) / 128u;
+    for (uint32_t l = tid; l < lines; l += RS_THREADS) prefetch_l2(vb + 128ull * l);
+  }
   if (vec && t0 + PP_ITEMS <= tile_n) {
 #pragma unroll
     for (int j = 0; j < PP_ITEMS / 4; ++j) {
@@ -641,11 +663,6 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
         const uint4 b = __ldcs(reinterpret_cast<const uint4 *>(sval + t0) + j);
         val[4 * j] = b.x; val[4 * j + 1] = b.y; val[4 * j + 2] = b.z; val[4 * j + 3] = b.w;
       }
-      if (V64) {
-        const ulonglong2 b = __ldcs(reinterpret_cast<const ulonglong2 *>(sv64 + t0) + 2 * j);
-        const ulonglong2 c = __ldcs(reinterpret_cast<const ulonglong2 *>(sv64 + t0) + 2 * j + 1);
-        v64[4 * j] = b.x; v64[4 * j + 1] = b.y; v64[4 * j + 2] = c.x; v64[4 * j + 3] = c.y;
-      }
     }
   } else {
 #pragma unroll
@@ -653,7 +670,6 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
       const bool in = t0 + i < tile_n;
       key[i] = in ? __ldcs(skey + t0 + i) : 0u;
       if (HAS_VALS && !gen_vals) val[i] = in ? __ldcs(sval + t0 + i) : 0u;
-      if (V64) v64[i] = in ? __ldcs(sv64 + t0 + i) : 0ull;
     }
   }
   if (HAS_VALS && gen_vals) {
@@ -713,7 +729,7 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
   // 4. publish the tile's digit counts; look back for the digits' global
   //    offsets (one thread per digit, 8 predecessor words per round; a warp
   //    that spreads its digits sequentially over its lanes was measured
-  //    slower); the other threads go on to the staging, which needs none
+  //    slower); the other threads go on to the positions, which need none
   if (tid < S::B) {
     const int d = tid;
     const uint32_t count = s_dstart[d + 1] - s_dstart[d];
@@ -729,19 +745,51 @@ k_part_pass(SortParams p, uint32_t pass, uint32_t shift) {
   }
 
   // 5. stage the tile in digit order
+  if (!V64) {
 #pragma unroll
-  for (int i = 0; i < PP_ITEMS; ++i) {
-    if (t0 + i < tile_n) {
-      const uint32_t d = dig(key[i]);
-      const uint32_t w = s_cnt[S::pad((int)(d % S::LANES) * RS_THREADS + tid)];
-      const uint32_t pos = ((w >> ((d / S::LANES) * 16)) & 0xFFFFu) +
-                           ((lrank[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
-      if (HAS_VALS) s_kv[pos] = make_uint2(key[i], val[i]);
-      else s_k[pos] = key[i];
-      if (V64) s_v64[pos] = v64[i];
+    for (int i = 0; i < PP_ITEMS; ++i) {
+      if (t0 + i < tile_n) {
+        const uint32_t d = dig(key[i]);
+        const uint32_t w = s_cnt[S::pad((int)(d % S::LANES) * RS_THREADS + tid)];
+        const uint32_t pos = ((w >> ((d / S::LANES) * 16)) & 0xFFFFu) +
+                             ((lrank[i >> 1] >> (16 * (i & 1))) & 0xFFFFu);
+        if (HAS_VALS) s_kv[pos] = make_uint2(key[i], val[i]);
+        else s_k[pos] = key[i];
+      }
     }
+    __syncthreads();
+  } else {
+    // 64-bit values: each item's position in the digit-ordered tile (kept
+    // in lrank); once every thread has read its counters, keys and values
+    // are staged over them
+#pragma unroll
+    for (int i = 0; i < PP_ITEMS; ++i) {
+      if (t0 + i < tile_n) {
+        const uint32_t d = dig(key[i]);
+        const uint32_t w = s_cnt[S::pad((int)(d % S::LANES) * RS_THREADS + tid)];
+        const uint32_t sh = 16 * (i & 1);
+        const uint32_t pos = ((w >> ((d / S::LANES) * 16)) & 0xFFFFu) + ((lrank[i >> 1] >> sh) & 0xFFFFu);
+        lrank[i >> 1] = (lrank[i >> 1] & ~(0xFFFFu << sh)) | (pos << sh);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < PP_ITEMS; ++i)
+      if (t0 + i < tile_n) s_k[(lrank[i >> 1] >> (16 * (i & 1))) & 0xFFFFu] = key[i];
+    if (vec && t0 + PP_ITEMS <= tile_n) {
+#pragma unroll
+      for (int j = 0; j < PP_ITEMS / 2; ++j) {
+        const ulonglong2 b = __ldcs(reinterpret_cast<const ulonglong2 *>(sv64 + t0) + j);
+        s_v64[lrank[j] & 0xFFFFu] = b.x;
+        s_v64[lrank[j] >> 16] = b.y;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < PP_ITEMS; ++i)
+        if (t0 + i < tile_n) s_v64[(lrank[i >> 1] >> (16 * (i & 1))) & 0xFFFFu] = __ldcs(sv64 + t0 + i);
+    }
+    __syncthreads();
   }
-  __syncthreads();
 
   // 6. each digit run written contiguously
 #pragma unroll 4
@@ -956,11 +1004,12 @@ int pd_sort_core(pimdal_ctx *ctx, const pimdal_sort_arguments_t *a, int key_mode
   // on a single small digit): the small-radix pass.
   if ((dbits <= 6 || (l.npasses == 1 && p.end_bit - p.begin_bit <= 6)) && !p.pairs) {
     const int val = v64 ? PV_U64 : p.has_vals ? PV_U32 : PV_NONE;
-    const int smem = (v64 ? 12 : p.has_vals ? 8 : 4) * RS_TILE;
     for (uint32_t q = 0; q < l.npasses; ++q) {
       pd_launch_scope sc(ctx, PIMDAL_KERNEL_PARTITION, s);
       const uint32_t shift = p.begin_bit + q * dbits;
-      PartKernel k = pick_part(std::min(dbits, p.end_bit - shift), val, key_mode);
+      const uint32_t qbits = std::min(dbits, p.end_bit - shift);
+      PartKernel k = pick_part(qbits, val, key_mode);
+      const int smem = (int)pp_smem_bytes((int)qbits, val);
       PD_CHECK_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
       k<<<resident_grid(ctx, (const void *)k, smem, l.tiles), RS_THREADS, smem, s>>>(p, q, shift);
     }
