@@ -382,7 +382,14 @@ int pimdal_hj_probe(pimdal_ctx_t *ctx, const pimdal_probe_arguments_t *args,
  * and probed in partition order.  Output per match: build payload and probe
  * row id; partitions in order, probe order within a partition (probe order
  * overall when not partitioned).  With duplicate build keys the matches of
- * one probe row come in table order. */
+ * one probe row come in table order.
+ * partition_bits 9..16 selects shared-memory partitions instead: both
+ * relations are partitioned 2^partition_bits ways (stable passes of at most
+ * 6 bits) so that one partition's build rows fit a table in one CTA's shared
+ * memory (the reference CPU join's 16384 cache-sized partitions,
+ * hash_join.cpp:57-157); load_factor_pct and l2_budget_bytes are then
+ * unused.  Same output order, except that a partition with more than 12288
+ * build rows is joined in chunks of build rows, its output chunk-major. */
 typedef struct {
   const void *build_key;          /* uint32 / int32 keys                          */
   const uint32_t *build_payload;  /* NULL = build row id                          */
@@ -393,7 +400,8 @@ typedef struct {
   uint32_t *out_build_payload;
   uint32_t *out_probe_ptr;
   uint64_t out_capacity;
-  uint32_t partition_bits;        /* 0 = auto, 0xFFFFFFFF = never partition, else 1..8 */
+  uint32_t partition_bits;        /* 0 = auto, 0xFFFFFFFF = never partition, 1..8   */
+                                  /* (L2-sized) or 9..16 (shared-memory partitions) */
   uint32_t load_factor_pct;       /* table load factor in percent; 0 = 50          */
   uint64_t l2_budget_bytes;       /* 0 = 48 MiB                                   */
 } pimdal_hash_join_arguments_t;
@@ -718,7 +726,8 @@ int pimdal_batch_autotune(pimdal_ctx_t *ctx, int kind, const void *args, uint32_
 /* ------------------------------------------------------------------------- */
 /* Autotuner of the plain operators (the batch autotuner's counterpart for    */
 /* single calls).  The hash join's partition fan-out and table load factor    */
-/* and the high-cardinality hash group-by's mode (hash-partitioned chunks or  */
+/* (L2-sized partitions) or shared-memory partition count, and the           */
+/* high-cardinality hash group-by's mode (hash-partitioned chunks or         */
 /* one direct global table) and partition count are chosen per input shape.   */
 /* pimdal_*_autotune runs the call once per candidate on the given arguments  */
 /* (writing the outputs; the last run is the chosen candidate's), keeps the   */
@@ -733,7 +742,7 @@ int pimdal_batch_autotune(pimdal_ctx_t *ctx, int kind, const void *args, uint32_
 /* method) runs once with the library's choice and returns group_mode 0.     */
 /* ------------------------------------------------------------------------- */
 typedef struct {
-  uint32_t partition_bits;   /* hash join: 0xFFFFFFFF = unpartitioned, else 1..8       */
+  uint32_t partition_bits;   /* hash join: 0xFFFFFFFF = unpartitioned, else 1..16      */
   uint32_t load_factor_pct;  /* hash join: table load factor in percent                */
   uint32_t group_mode;       /* group-by: 0 library's choice, 1 partitioned, 2 direct  */
   uint32_t group_part_bits;  /* group-by, partitioned: log2 of the hash partitions     */

@@ -312,7 +312,12 @@ __device__ __forceinline__ void hj_probe_tile(const JoinParams &p, uint64_t row0
       const int k = b + i;
       const uint64_t r = wbase + (uint64_t)k * 32 + lane;
       uint32_t ci = c[i];
-      if (r < hi && key[i] == 0xFFFFFFFFu) ci += side;
+      if (r < hi && key[i] == 0xFFFFFFFFu) {
+        // the side rows follow the table's matches; with none in the table
+        // the first payload is the side row's (all ones)
+        if (ci == 0 && side) fk[i] = 0xFFFFFFFFu;
+        ci += side;
+      }
       s_first[k][tid] = fk[i];
 #if !PD_HJ_KEYS_FIRST
       s_row[k][tid] = rowv[i];
@@ -564,16 +569,344 @@ int probe_grid(pimdal_ctx *ctx) {
   return per_sm * ctx->sm_count;
 }
 
+// ---------------------------------------------------------------------------
+// Shared-memory partitions (partition_bits HJS_MIN_BITS..HJS_MAX_BITS): both
+// relations are radix-partitioned (stable passes of at most 6 bits) by the
+// top partition_bits of the multiplicative hash, so that one partition's
+// build rows fit a linear-probing table in one CTA's shared memory -- the
+// cache-sized partitions of the reference's CPU join
+// (reference/db_operators/hash_join.cpp:57-157, 16384 ways) and the
+// bucket-sized ones of its DPU join (pimdal/join/hash_join.c:40-115).  A
+// persistent CTA per SM claims partitions in order; for each it fills the
+// table, counts the matches of the partition's probe rows, resolves the
+// partition's output offset by a decoupled look-back over the partitions,
+// then probes the rows again (now from L2) and writes the pairs in probe
+// order.  A partition with more than HJS_CHUNK build rows is joined one
+// chunk of build rows at a time (its output is then chunk-major).
+// ---------------------------------------------------------------------------
+constexpr int HJS_THREADS = 1024;
+constexpr int HJS_WARPS = HJS_THREADS / 32;
+constexpr uint32_t HJS_SLOT_BITS = 14;
+constexpr uint32_t HJS_SLOTS = 1u << HJS_SLOT_BITS;  // 128 KB of 8-byte slots
+constexpr uint32_t HJS_CHUNK = HJS_SLOTS / 4 * 3;    // build rows per table fill
+#ifndef PD_HJS_ITEMS
+#define PD_HJS_ITEMS 8    // probe rows per thread and tile of the writing pass
+#endif
+#ifndef PD_HJS_CITEMS
+#define PD_HJS_CITEMS 8   // probe rows per thread and tile of the counting pass
+#endif
+constexpr int HJS_ITEMS = PD_HJS_ITEMS;
+constexpr int HJS_CITEMS = PD_HJS_CITEMS;
+constexpr uint32_t HJS_MIN_BITS = 9, HJS_MAX_BITS = 16;
+constexpr size_t HJS_SMEM = 8ull * HJS_SLOTS;
+
+struct JoinSmemParams {
+  const uint32_t *bkey, *bpay;  // partitioned build rows
+  const uint32_t *pkey, *prow;  // partitioned probe rows
+  const uint32_t *boff, *poff;  // parts + 1 partition offsets each
+  uint32_t part_bits, parts;
+  uint32_t *out_pay, *out_row;
+  uint64_t cap;
+  uint64_t *status;
+  uint32_t epoch;
+  uint32_t *claim;
+  uint32_t *d_error;
+  uint64_t *d_count;
+};
+
+// off[q] = the first row whose partition (top `bits` of the multiplicative
+// hash) is >= q, for q = 0..parts.
+__global__ void __launch_bounds__(256) k_hjs_bounds(const uint32_t *key, uint64_t n, uint32_t bits,
+                                                    uint32_t parts, uint32_t *off) {
+  const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q > parts) return;
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if ((pd_mulhash32(key[mid]) >> (32 - bits)) < q) lo = mid + 1;
+    else hi = mid;
+  }
+  off[q] = (uint32_t)lo;
+}
+
+// A key's home slot: the hash bits just below the ones that chose its
+// partition.
+__device__ __forceinline__ uint32_t hjs_slot(uint32_t key, uint32_t part_bits) {
+  return (pd_mulhash32(key) << part_bits) >> (32 - HJS_SLOT_BITS);
+}
+
+// Clears the table and inserts build rows [r0, r1), r1 - r0 <= HJS_CHUNK (so
+// every walk finds a free slot), after every thread is done with the table's
+// previous contents.  The one row whose slot word would equal the empty word
+// is counted in *s_side; *s_dup is set when a key occurs twice.
+__device__ void hjs_fill(unsigned long long *tab, const JoinSmemParams &p, uint64_t r0, uint64_t r1,
+                         uint32_t *s_side, uint32_t *s_dup) {
+  __syncthreads();
+  const ulonglong2 e2 = make_ulonglong2(HJ_EMPTY, HJ_EMPTY);
+  for (uint32_t i = threadIdx.x; i < HJS_SLOTS / 2; i += HJS_THREADS)
+    reinterpret_cast<ulonglong2 *>(tab)[i] = e2;
+  if (threadIdx.x == 0) {
+    *s_side = 0;
+    *s_dup = 0;
+  }
+  __syncthreads();
+  for (uint64_t i = r0 + threadIdx.x; i < r1; i += HJS_THREADS) {
+    const uint32_t k = __ldcs(p.bkey + i), v = __ldcs(p.bpay + i);
+    const unsigned long long e = ((unsigned long long)v << 32) | k;
+    if (e == HJ_EMPTY) {
+      atomicAdd(s_side, 1u);
+      continue;
+    }
+    uint32_t s = hjs_slot(k, p.part_bits);
+    for (uint32_t t = 0; t < HJS_SLOTS; ++t) {
+      const unsigned long long old = atomicCAS(tab + s, HJ_EMPTY, e);
+      if (old == HJ_EMPTY) break;
+      if ((uint32_t)old == k) *s_dup = 1;
+      s = (s + 1) & (HJS_SLOTS - 1);
+    }
+  }
+  __syncthreads();
+}
+
+// Matches of key in the table (the walk ends at a free slot, or at the first
+// match when no key occurs twice); *first gets the first match's payload.
+__device__ __forceinline__ uint32_t hjs_find(const unsigned long long *tab, uint32_t key,
+                                             uint32_t part_bits, bool stop_first, uint32_t *first) {
+  uint32_t s = hjs_slot(key, part_bits), c = 0;
+  for (uint32_t t = 0; t < HJS_SLOTS; ++t) {
+    const unsigned long long e = tab[s];
+    if (e == HJ_EMPTY) break;
+    if ((uint32_t)e == key) {
+      if (c == 0) *first = (uint32_t)(e >> 32);
+      ++c;
+      if (stop_first) break;
+    }
+    s = (s + 1) & (HJS_SLOTS - 1);
+  }
+  return c;
+}
+
+// Writes every match of key (then `side` all-ones payloads for the all-ones
+// key) from output position w on; returns the next position.
+__device__ uint64_t hjs_emit(const unsigned long long *tab, const JoinSmemParams &p, uint32_t key,
+                             uint32_t row, uint32_t side, uint64_t w, bool *overflow) {
+  uint32_t s = hjs_slot(key, p.part_bits);
+  for (uint32_t t = 0; t < HJS_SLOTS; ++t) {
+    const unsigned long long e = tab[s];
+    if (e == HJ_EMPTY) break;
+    if ((uint32_t)e == key) {
+      if (w < p.cap) { p.out_pay[w] = (uint32_t)(e >> 32); p.out_row[w] = row; } else *overflow = true;
+      ++w;
+    }
+    s = (s + 1) & (HJS_SLOTS - 1);
+  }
+  if (key == 0xFFFFFFFFu) {
+    for (uint32_t m = 0; m < side; ++m, ++w) {
+      if (w < p.cap) { p.out_pay[w] = 0xFFFFFFFFu; p.out_row[w] = row; } else *overflow = true;
+    }
+  }
+  return w;
+}
+
+// One tile of a partition's probe rows [t0, min(t0 + HJS_THREADS * ITEMS,
+// r1)): warp w takes rows t0 + w * 32 * ITEMS + 32k + lane.  COUNT: returns
+// the thread's match total.  Otherwise writes the tile's pairs in probe order
+// from output position *base on (the same in every thread) and advances
+// *base past them.
+template <bool COUNT, int ITEMS>
+__device__ __forceinline__ uint32_t hjs_tile(const unsigned long long *tab, const JoinSmemParams &p,
+                                             uint64_t t0, uint64_t r1, uint32_t side, bool stop_first,
+                                             uint64_t *base, uint32_t *s_warp, bool *overflow) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint64_t wb = t0 + (uint64_t)warp * (32 * ITEMS);
+  uint32_t key[ITEMS], row[COUNT ? 1 : ITEMS];
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    const uint64_t r = wb + 32 * k + lane;
+    // the counting pass leaves the keys in L2 for the writing pass
+    key[k] = r < r1 ? (COUNT ? __ldcg(p.pkey + r) : __ldcs(p.pkey + r)) : 0u;
+    if (!COUNT) row[k] = r < r1 ? __ldcs(p.prow + r) : 0u;
+  }
+  uint32_t c[ITEMS], f[ITEMS], mine = 0;
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    c[k] = 0;
+    f[k] = 0;
+    if (wb + 32 * k + lane < r1) {
+      const bool ones = key[k] == 0xFFFFFFFFu;
+      c[k] = hjs_find(tab, key[k], p.part_bits, stop_first && !ones, &f[k]) + (ones ? side : 0u);
+    }
+    mine += c[k];
+  }
+  if (COUNT) return mine;
+
+  uint32_t wtot = mine;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) wtot += __shfl_xor_sync(0xffffffffu, wtot, o);
+  if (lane == 0) s_warp[warp] = wtot;
+  __syncthreads();
+  uint64_t w = *base;
+  uint32_t total = 0;
+#pragma unroll
+  for (int i = 0; i < HJS_WARPS; ++i) {
+    const uint32_t x = s_warp[i];
+    if (i < warp) w += x;
+    total += x;
+  }
+  __syncthreads();  // s_warp is written again by the next tile
+  *base += total;
+  const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int k = 0; k < ITEMS; ++k) {
+    // one table match (not the all-ones key, whose side rows need the walk)
+    const bool one = c[k] == 1 && key[k] != 0xFFFFFFFFu;
+    if (__all_sync(0xffffffffu, c[k] == 0 || one)) {
+      const unsigned m = __ballot_sync(0xffffffffu, one);
+      if (one) {
+        const uint64_t pos = w + __popc(m & lt);
+        if (pos < p.cap) { p.out_pay[pos] = f[k]; p.out_row[pos] = row[k]; } else *overflow = true;
+      }
+      w += __popc(m);
+    } else {
+      uint32_t ci = c[k];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, ci, o);
+        if (lane >= o) ci += t;
+      }
+      const uint64_t pos = w + ci - c[k];
+      if (one) {
+        if (pos < p.cap) { p.out_pay[pos] = f[k]; p.out_row[pos] = row[k]; } else *overflow = true;
+      } else if (c[k]) {
+        hjs_emit(tab, p, key[k], row[k], side, pos, overflow);
+      }
+      w += __shfl_sync(0xffffffffu, ci, 31);
+    }
+  }
+  return mine;
+}
+
+__device__ __forceinline__ uint64_t hjs_block_sum(uint64_t v, unsigned long long *s_red) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (threadIdx.x == 0) *s_red = 0;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) atomicAdd(s_red, (unsigned long long)v);
+  __syncthreads();
+  return *s_red;
+}
+
+// Persistent: one CTA per SM claims partitions in order.
+__global__ void __launch_bounds__(HJS_THREADS, 1) k_hjs_join(JoinSmemParams p) {
+  extern __shared__ __align__(16) unsigned long long hjs_tab[];
+  __shared__ uint32_t s_warp[HJS_WARPS];
+  __shared__ uint32_t s_side, s_dup, s_part;
+  __shared__ unsigned long long s_red;
+  __shared__ uint64_t s_prefix;
+  const int tid = threadIdx.x;
+  bool overflow = false;
+  while (true) {
+    __syncthreads();  // s_part and s_red of the previous partition have been read
+    if (tid == 0) {
+      const uint32_t q = atomicAdd(p.claim, 1u);
+      if (q >= p.parts && atomicAdd(p.claim + 1, 1u) == gridDim.x - 1) {
+        p.claim[0] = 0;  // last claimer of the launch resets the counters
+        p.claim[1] = 0;
+      }
+      s_part = q;
+    }
+    __syncthreads();
+    const uint32_t q = s_part;
+    if (q >= p.parts) break;
+    const uint64_t b0 = p.boff[q], b1 = p.boff[q + 1], r0 = p.poff[q], r1 = p.poff[q + 1];
+    const uint32_t chunks = b1 > b0 ? (uint32_t)pd_ceil_div(b1 - b0, HJS_CHUNK) : 0u;
+    // 1. count the partition's matches (over every chunk of its build rows)
+    uint64_t mine = 0;
+    for (uint32_t ch = 0; ch < chunks; ++ch) {
+      hjs_fill(hjs_tab, p, b0 + (uint64_t)ch * HJS_CHUNK, min(b1, b0 + (uint64_t)(ch + 1) * HJS_CHUNK),
+               &s_side, &s_dup);
+      const uint32_t side = s_side;
+      const bool stop_first = s_dup == 0;
+      for (uint64_t t0 = r0; t0 < r1; t0 += HJS_THREADS * HJS_CITEMS)
+        mine += hjs_tile<true, HJS_CITEMS>(hjs_tab, p, t0, r1, side, stop_first, nullptr, s_warp,
+                                           &overflow);
+    }
+    const uint64_t total = hjs_block_sum(mine, &s_red);
+    // 2. the partition's output offset
+    if (tid < 32) {
+      uint64_t pre = 0;
+      if (q == 0) {
+        if (tid == 0) pd_store_relaxed_u64(p.status, pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, total));
+      } else {
+        if (tid == 0)
+          pd_store_relaxed_u64(p.status + q, pd_pack_status(p.epoch, PD_FLAG_AGGREGATE, total));
+        pre = pd_lookback_warp(p.status, (int64_t)q, p.epoch, p.d_error);
+        if (tid == 0)
+          pd_store_relaxed_u64(p.status + q, pd_pack_status(p.epoch, PD_FLAG_INCLUSIVE, pre + total));
+      }
+      if (tid == 0) {
+        s_prefix = pre;
+        if (q == p.parts - 1) *p.d_count = pre + total;
+      }
+    }
+    __syncthreads();
+    // 3. write the pairs (a single chunk is still in the table)
+    uint64_t base = s_prefix;
+    for (uint32_t ch = 0; ch < chunks; ++ch) {
+      if (chunks > 1)
+        hjs_fill(hjs_tab, p, b0 + (uint64_t)ch * HJS_CHUNK, min(b1, b0 + (uint64_t)(ch + 1) * HJS_CHUNK),
+                 &s_side, &s_dup);
+      const uint32_t side = s_side;
+      const bool stop_first = s_dup == 0;
+      for (uint64_t t0 = r0; t0 < r1; t0 += HJS_THREADS * HJS_ITEMS)
+        hjs_tile<false, HJS_ITEMS>(hjs_tab, p, t0, r1, side, stop_first, &base, s_warp, &overflow);
+    }
+  }
+  if (overflow) atomicOr(p.d_error, PD_DEVERR_CAPACITY);
+}
+
 #ifndef PD_HJ_ONE_TABLE
 #define PD_HJ_ONE_TABLE 1
 #endif
 
 struct HjLayout {
   uint32_t bits, part_bits;
+  bool smem;  // shared-memory partitions (k_hjs_join)
   size_t table, side, boff, poff, tilebase, bk, bp, pk, pr, sort_ws, total;
 };
 
+// Shared-memory partitions: partitioned copies of both relations, their
+// partition offsets and the partition passes' workspace.
+bool hjs_layout(const pimdal_hash_join_arguments_t *a, HjLayout *l) {
+  const uint32_t pb = a->partition_bits;
+  l->smem = true;
+  l->part_bits = pb;
+  l->bits = 0;
+  const size_t offs = pd_align_up(4 * ((1ull << pb) + 1), 256);
+  size_t o = 0;
+  l->table = l->side = l->tilebase = 0;
+  l->boff = o; o += offs;
+  l->poff = o; o += offs;
+  l->bk = o; o += pd_align_up(4 * a->size_build, 256);
+  l->bp = o; o += pd_align_up(4 * a->size_build, 256);
+  l->pk = o; o += pd_align_up(4 * a->size_probe, 256);
+  l->pr = o; o += pd_align_up(4 * a->size_probe, 256);
+  pimdal_sort_arguments_t sa{};
+  sa.key_dtype = PIMDAL_U32;
+  sa.layout = PIMDAL_LAYOUT_COLUMNS;
+  sa.nr_elements = std::max(a->size_build, a->size_probe);
+  sa.begin_bit = 32 - pb;
+  sa.end_bit = 32;
+  const size_t w = pd_partition_workspace(&sa, false);
+  if (!w) return false;
+  l->sort_ws = o; o += w;
+  l->total = o;
+  return true;
+}
+
 bool hj_layout(const pimdal_hash_join_arguments_t *a, HjLayout *l) {
+  if (a->partition_bits >= HJS_MIN_BITS && a->partition_bits <= HJS_MAX_BITS) return hjs_layout(a, l);
+  l->smem = false;
   const uint32_t load_pct = a->load_factor_pct ? a->load_factor_pct : 50;
   if (load_pct > 90) return false;
   const uint32_t bits = pd_hj_table_bits(a->size_build, load_pct);
@@ -672,6 +1005,15 @@ std::vector<pimdal_hash_join_arguments_t> hj_candidates(const pimdal_hash_join_a
       if (hj_layout(&t, &m)) c.push_back(t);
     }
   }
+  // shared-memory partitions of about a half and a quarter of a table's slots
+  uint32_t sb = HJS_MIN_BITS;
+  while (sb < HJS_MAX_BITS && (a->size_build >> sb) > HJS_SLOTS / 2) ++sb;
+  for (uint32_t pb = sb; pb <= std::min(sb + 1, HJS_MAX_BITS); ++pb) {
+    t.partition_bits = pb;
+    t.load_factor_pct = 0;
+    HjLayout m;
+    if (hj_layout(&t, &m)) c.push_back(t);
+  }
   return c;
 }
 
@@ -681,6 +1023,63 @@ std::vector<uint64_t> hj_shape(const pimdal_hash_join_arguments_t *a) {
 
 bool hj_auto(const pimdal_hash_join_arguments_t *a) {
   return a->partition_bits == 0 && a->load_factor_pct == 0;
+}
+
+// The join over shared-memory partitions: both relations partitioned by the
+// top part_bits of the multiplicative hash (stable passes of at most 6 bits,
+// row ids made in the first pass when a relation has no payload column),
+// their partition offsets found by binary search, then k_hjs_join.
+int hjs_run(pimdal_ctx *ctx, const pimdal_hash_join_arguments_t *a, const HjLayout &l, char *ws,
+            pimdal_merge_results_t *d_result, cudaStream_t s) {
+  const uint32_t pb = l.part_bits, parts = 1u << pb;
+  int st;
+  JoinSmemParams p{};
+  p.part_bits = pb;
+  p.parts = parts;
+  p.out_pay = a->out_build_payload;
+  p.out_row = a->out_probe_ptr;
+  p.cap = a->out_capacity;
+  p.status = ctx->d_status;
+  p.claim = ctx->d_counters + PD_COUNTER_PROBE;
+  p.d_error = ctx->d_error;
+  p.d_count = &d_result->t_count;
+  p.epoch = pd_next_epoch(ctx, s, &st);
+  if (st) return st;
+  pimdal_sort_arguments_t sa{};
+  sa.key_dtype = PIMDAL_U32;
+  sa.layout = PIMDAL_LAYOUT_COLUMNS;
+  sa.begin_bit = 32 - pb;
+  sa.end_bit = 32;
+  sa.nr_elements = a->size_build;
+  sa.in = a->build_key;
+  sa.in_ptr = a->build_payload;
+  sa.out = ws + l.bk;
+  sa.out_ptr = (uint32_t *)(ws + l.bp);
+  if ((st = pd_partition(ctx, &sa, PD_KEY_MULHASH, ws + l.sort_ws, s, nullptr, nullptr))) return st;
+  sa.nr_elements = a->size_probe;
+  sa.in = a->probe_key;
+  sa.in_ptr = a->probe_ptr;
+  sa.out = ws + l.pk;
+  sa.out_ptr = (uint32_t *)(ws + l.pr);
+  if ((st = pd_partition(ctx, &sa, PD_KEY_MULHASH, ws + l.sort_ws, s, nullptr, nullptr))) return st;
+  p.bkey = (const uint32_t *)(ws + l.bk);
+  p.bpay = (const uint32_t *)(ws + l.bp);
+  p.pkey = (const uint32_t *)(ws + l.pk);
+  p.prow = (const uint32_t *)(ws + l.pr);
+  p.boff = (const uint32_t *)(ws + l.boff);
+  p.poff = (const uint32_t *)(ws + l.poff);
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_OTHER, s);
+    const unsigned g = (unsigned)pd_ceil_div(parts + 1, 256);
+    k_hjs_bounds<<<g, 256, 0, s>>>(p.bkey, a->size_build, pb, parts, (uint32_t *)(ws + l.boff));
+    k_hjs_bounds<<<g, 256, 0, s>>>(p.pkey, a->size_probe, pb, parts, (uint32_t *)(ws + l.poff));
+  }
+  PD_CHECK_CUDA(cudaFuncSetAttribute(k_hjs_join, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)HJS_SMEM));
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_HJ_PROBE, s);
+    k_hjs_join<<<ctx->sm_count, HJS_THREADS, HJS_SMEM, s>>>(p);
+  }
+  return pd_launch_status(ctx);
 }
 }  // namespace
 
@@ -724,6 +1123,7 @@ extern "C" int pimdal_hash_join(pimdal_ctx_t *ctx, const pimdal_hash_join_argume
   int st;
   char *ws = (char *)pd_workspace(ctx, l.total, s, &st);
   if (!ws) return st;
+  if (l.smem) return hjs_run(ctx, a, l, ws, d_result, s);
   const uint32_t parts = 1u << l.part_bits;
   const uint64_t total_tiles_direct = pd_ceil_div(a->size_probe, HJ_TILE);
   if (total_tiles_direct + parts > PD_STATUS_WORDS) return PIMDAL_ERR_ARG;

@@ -59,6 +59,25 @@ def test_hash_join_partitioned(ctx, bits):
     check_join(ctx, bk, bp, pk, partition_bits=bits)
 
 
+@pytest.mark.parametrize("bits,zipf", [(9, None), (10, 0.75), (16, None)])
+def test_hash_join_shared_memory_partitions(ctx, bits, zipf):
+    bk, bp, pk = inputs(1 << 16, (1 << 20) + 5, 47, zipf=zipf)
+    gp, gr = check_join(ctx, bk, bp, pk, partition_bits=bits)
+    # partitions in order, probe order within each
+    h = pk[gr].astype(np.uint32).astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15)
+    part = (h >> np.uint64(64 - bits)).astype(np.int64)
+    assert np.all(np.diff(part * 2**32 + gr.astype(np.int64)) > 0)
+
+
+def test_hash_join_shared_memory_partition_in_chunks(ctx):
+    # 20000 build rows of one key fill one partition past a table's capacity:
+    # the partition is joined one chunk of build rows at a time
+    bk = np.concatenate([np.full(20000, 77, np.int32), np.arange(1000, 3000, dtype=np.int32)])
+    bp = np.arange(bk.size, dtype=np.int32)
+    pk = np.array([77, 5, 1500, 77, -1, 2999, 77], np.int32)
+    check_join(ctx, bk, bp, pk, partition_bits=9, capacity=70000)
+
+
 def test_hash_join_auto_partition_small_budget(ctx):
     bk, bp, pk = inputs(1 << 17, 1 << 20, 43, zipf=0.75)
     check_join(ctx, bk, bp, pk, l2_budget_bytes=1 << 18)
@@ -70,6 +89,22 @@ def test_hash_join_duplicate_build_keys_and_sentinel(ctx):
     bp = np.array([1, 2, 3, -1, 4, 5, 6], np.int32)
     pk = np.array([5, -1, 8, 7, 5, 9, -1], np.int32)
     res, pay, row = ops.hash_join(ctx, cuda_i32(bk), cuda_i32(bp), cuda_i32(pk), capacity=64)
+    ctx.sync()
+    c = int(res.item())
+    got = sorted(zip(u32(row[:c]).tolist(), u32(pay[:c]).tolist()))
+    exp = sorted((i, int(np.uint32(bp[j]))) for i, k in enumerate(pk) for j, b in enumerate(bk) if b == k)
+    assert got == exp
+
+
+@pytest.mark.parametrize("partition_bits", [0xFFFFFFFF, 3, 9])
+def test_hash_join_sentinel_row_alone(ctx, partition_bits):
+    # the all-ones key/payload row is the only build match of an all-ones probe
+    # key: one match, whose payload is all ones
+    bk = np.array([5, -1, 7, 9], np.int32)
+    bp = np.array([1, -1, 3, 5], np.int32)
+    pk = np.array([5, -1, 8, 7, -1, 9], np.int32)
+    res, pay, row = ops.hash_join(ctx, cuda_i32(bk), cuda_i32(bp), cuda_i32(pk), capacity=64,
+                                  partition_bits=partition_bits)
     ctx.sync()
     c = int(res.item())
     got = sorted(zip(u32(row[:c]).tolist(), u32(pay[:c]).tolist()))
