@@ -933,13 +933,28 @@ __global__ void __launch_bounds__(256) k_vrange(const long long *v, uint64_t n, 
   const uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   uint64_t done = 0;
   if (((uintptr_t)v & 15u) == 0) {
+    // four 16-byte loads of a thread in flight together (one at a time left
+    // the read latency-bound)
+    constexpr int U = 4;
     const longlong2 *v2 = reinterpret_cast<const longlong2 *>(v);
-    for (uint64_t i = i0; i < n / 2; i += stride) {
+    const uint64_t n2 = n / 2;
+    uint64_t i = i0;
+    for (; i + (U - 1) * stride < n2; i += U * stride) {
+      longlong2 x[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) x[u] = __ldcs(v2 + i + u * stride);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        lo = min(lo, min(x[u].x, x[u].y));
+        hi = max(hi, max(x[u].x, x[u].y));
+      }
+    }
+    for (; i < n2; i += stride) {
       const longlong2 x = __ldcs(v2 + i);
       lo = min(lo, min(x.x, x.y));
       hi = max(hi, max(x.x, x.y));
     }
-    done = n / 2 * 2;
+    done = n2 * 2;
   }
   for (uint64_t i = done + i0; i < n; i += stride) {
     const long long x = v[i];

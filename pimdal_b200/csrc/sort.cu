@@ -143,11 +143,27 @@ __global__ void __launch_bounds__(RS_THREADS) k_sort_hist(SortParams p) {
   const bool vec = !p.pairs && ((uintptr_t)p.in & 15u) == 0;
   const uint64_t n = sort_n(p);
   uint64_t done = 0;
+  // U loads of a thread are in flight together (one 16-byte load
+  // at a time left the read latency-bound at about 2.4 TB/s)
+  constexpr int U = 4;
   if (vec) {
     const uint4 *in4 = reinterpret_cast<const uint4 *>(p.in);
     const uint64_t n4 = n / 4;
-    for (uint64_t i = (uint64_t)blockIdx.x * RS_THREADS + tid; i < n4; i += stride) {
-      uint4 v = __ldcs(in4 + i);
+    uint64_t i = (uint64_t)blockIdx.x * RS_THREADS + tid;
+    for (; i + (U - 1) * stride < n4; i += U * stride) {
+      uint4 v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) v[u] = __ldcs(in4 + i + u * stride);
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        add(v[u].x);
+        add(v[u].y);
+        add(v[u].z);
+        add(v[u].w);
+      }
+    }
+    for (; i < n4; i += stride) {
+      const uint4 v = __ldcs(in4 + i);
       add(v.x);
       add(v.y);
       add(v.z);
@@ -155,8 +171,15 @@ __global__ void __launch_bounds__(RS_THREADS) k_sort_hist(SortParams p) {
     }
     done = n4 * 4;
   }
-  for (uint64_t i = done + (uint64_t)blockIdx.x * RS_THREADS + tid; i < n; i += stride)
-    add(load_key_in(p, i));
+  uint64_t i = done + (uint64_t)blockIdx.x * RS_THREADS + tid;
+  for (; i + (U - 1) * stride < n; i += U * stride) {
+    uint32_t k[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) k[u] = load_key_in(p, i + u * stride);
+#pragma unroll
+    for (int u = 0; u < U; ++u) add(k[u]);
+  }
+  for (; i < n; i += stride) add(load_key_in(p, i));
   __syncthreads();
   for (uint32_t q = 0; q < p.npasses; ++q) {
     uint32_t s = 0;
