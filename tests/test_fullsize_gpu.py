@@ -2,7 +2,8 @@
 library itself):
 
   * config 3 hash join: build 2^25 unique int32 keys + payloads, probe 2^28
-    keys at a 50% match rate, uniform and Zipf(0.75) probes -- the full
+    keys at a 50% match rate, uniform and Zipf(0.75) probes, and the
+    uniform probe over 4096 shared-memory partitions -- the full
     multiset of (build payload, probe row id) equals the oracle's
     (reference/db_operators/hash_join.cpp:57-157 restated);
   * config 3 group-by: 2^28 rows at 16, 2^12 and 2^22 groups, hash and sort
@@ -52,8 +53,9 @@ def assert_join_equal(gpay, grow, epay, erow, n_probe):
     assert np.array_equal(by_g, by_e)
 
 
-@pytest.mark.parametrize("zipf", [False, True], ids=["uniform", "zipf0.75"])
-def test_hash_join_config3_matches_oracle(ctx, zipf):
+@pytest.mark.parametrize("zipf,partition_bits", [(False, 0), (True, 0), (False, 12)],
+                         ids=["uniform", "zipf0.75", "uniform-shared-memory-partitions"])
+def test_hash_join_config3_matches_oracle(ctx, zipf, partition_bits):
     nb, npr = 1 << 25, 1 << 28
     s = 0xB200 + 2
     g = lambda spec, n: ops.gen_column(ctx, spec, n)
@@ -62,7 +64,7 @@ def test_hash_join_config3_matches_oracle(ctx, zipf):
     pk = g(gen.Spec(L.GEN_PROBE, L.I32, seed=s, stream_id=3 if zipf else 2, lo=nb,
                     perm_domain=2 * nb, match_permille=500,
                     cdf=gen.zipf_cdf(nb, 0.75) if zipf else None), npr)
-    res, pay, row = ops.hash_join(ctx, bk, bp, pk, capacity=npr)
+    res, pay, row = ops.hash_join(ctx, bk, bp, pk, capacity=npr, partition_bits=partition_bits)
     ctx.sync()
     m = int(res.item())
     hb, hp, hk = u32(bk), u32(bp), u32(pk)
