@@ -38,13 +38,16 @@ namespace {
 constexpr int BF_THREADS = 256;
 constexpr int BF_WARPS = BF_THREADS / 32;
 #ifndef PD_BF_ITEMS
-#define PD_BF_ITEMS 8  // rows per thread of a match / filter tile (measured best with 6 CTAs per SM)
+#define PD_BF_ITEMS 8  // rows per thread of a match / filter tile (measured best; 4 was slower)
 #endif
 #ifndef PD_BF_RANGES
 #define PD_BF_RANGES 1  // 1: tile partition ranges from a pre-pass (0: searched by each tile)
 #endif
 #ifndef PD_BF_MATCH_CTAS
-#define PD_BF_MATCH_CTAS 6  // match CTAs per SM the kernel is compiled for
+// match CTAs per SM the kernel is compiled for: 8 (32 registers, a 44-byte
+// spill) hide the per-tile barriers better than 6 (40 registers): 2.31 ->
+// 1.99 ms for 2^28 probe rows at 5% match
+#define PD_BF_MATCH_CTAS 8
 #endif
 constexpr int BF_ITEMS = PD_BF_ITEMS;
 static_assert(BF_ITEMS <= 32, "one hit bit per row of a thread");
