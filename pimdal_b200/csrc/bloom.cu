@@ -11,7 +11,11 @@
 // hash_steps.c:163-185) and counts the kept rows of every partition.
 //
 // B200 design (HBM-bound streaming; the filters, 2 KB each, live in L2):
-//  * k_filter_build: CTAs stride over 2048-row tiles.  A tile spanning at
+//  * k_filter_parts: one CTA per partition of at most 16384 rows (the
+//    usual size) builds its filter in shared memory and stores it whole,
+//    no global atomics.
+//  * k_filter_build, for the rows of larger partitions only (skipped
+//    entirely when there are none): CTAs stride over 2048-row tiles.  A tile spanning at
 //    most 8 partitions builds their filters in shared memory (shared
 //    atomics) and ORs the non-zero words into the global filters, at most
 //    512 global atomics per partition; a tile spanning more partitions ORs
@@ -142,12 +146,58 @@ __device__ __forceinline__ uint32_t key_at(const void *in, int pairs, uint64_t r
   return pairs ? reinterpret_cast<const uint2 *>(in)[r].x : reinterpret_cast<const uint32_t *>(in)[r];
 }
 
-__global__ void __launch_bounds__(BF_THREADS) k_filter_build(FilterParams p) {
+// Partitions of at most BF_PART_ROWS rows: one CTA per partition in turn
+// assembles its filter in shared memory (eight key loads of a thread in
+// flight together) and stores it whole -- no other CTA writes that filter, so
+// no atomics reach global memory.  A larger partition (or a decreasing
+// part_sizes entry) sets *large and is left to k_filter_build.
+constexpr uint64_t BF_PART_ROWS = 16384;
+
+__device__ __forceinline__ bool small_part(const uint64_t *ps, int64_t q) {
+  const uint64_t a = ps[q], b = ps[q + 1];
+  return b > a && b - a <= BF_PART_ROWS;
+}
+
+__global__ void __launch_bounds__(BF_THREADS) k_filter_parts(FilterParams p, uint32_t *large) {
+  __shared__ __align__(16) uint32_t s_f[BF_WORDS];
+  const int tid = threadIdx.x;
+  for (uint32_t q = blockIdx.x; q < p.part_n; q += gridDim.x) {
+    const uint64_t a = p.ps[q], b = p.ps[q + 1];
+    if (b <= a) {
+      if (b < a && tid == 0) *large = 1;
+      continue;
+    }
+    if (b - a > BF_PART_ROWS) {
+      if (tid == 0) *large = 1;
+      continue;
+    }
+    for (uint32_t i = tid; i < BF_WORDS; i += BF_THREADS) s_f[i] = 0;
+    __syncthreads();
+    for (uint64_t r0 = a; r0 < b; r0 += 8 * BF_THREADS) {
+      uint32_t k[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const uint64_t r = r0 + (uint64_t)j * BF_THREADS + tid;
+        k[j] = r < b ? key_at(p.in, p.pairs, r) : 0u;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        if (r0 + (uint64_t)j * BF_THREADS + tid < b) set_bits(s_f, k[j]);
+    }
+    __syncthreads();
+    uint4 *g = reinterpret_cast<uint4 *>(p.filter + (uint64_t)q * BF_WORDS);
+    for (uint32_t i = tid; i < BF_WORDS / 4; i += BF_THREADS) g[i] = reinterpret_cast<const uint4 *>(s_f)[i];
+    __syncthreads();  // s_f is cleared again for the next partition
+  }
+}
+
+// The rows of the partitions k_filter_parts left (when *large is set).
+__global__ void __launch_bounds__(BF_THREADS) k_filter_build(FilterParams p, const uint32_t *large) {
   __shared__ __align__(16) uint32_t s_f[BF_SMEM_PARTS * BF_WORDS];
   __shared__ int64_t s_pa, s_pb;
   const int tid = threadIdx.x;
   const uint64_t begin = p.ps[0], end = p.ps[p.part_n];
-  if (end <= begin) return;
+  if (*large == 0 || end <= begin) return;
   const uint64_t tiles = pd_ceil_div(end - begin, BF_TILE);
   for (uint64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
     const uint64_t a = begin + t * BF_TILE, b = min(a + (uint64_t)BF_TILE, end);
@@ -163,6 +213,7 @@ __global__ void __launch_bounds__(BF_THREADS) k_filter_build(FilterParams p) {
       for (uint64_t r = a + tid; r < b; r += BF_THREADS) {
         const int64_t q = np == 1 ? pa : part_of(p.ps, pa, pb, r);
         if (q < pa) continue;  // only with a decreasing part_sizes
+        if (small_part(p.ps, q)) continue;  // stored whole by k_filter_parts
         set_bits(s_f + (q - pa) * BF_WORDS, key_at(p.in, p.pairs, r));
       }
       __syncthreads();
@@ -174,6 +225,7 @@ __global__ void __launch_bounds__(BF_THREADS) k_filter_build(FilterParams p) {
       for (uint64_t r = a + tid; r < b; r += BF_THREADS) {
         const int64_t q = part_of(p.ps, pa < 0 ? 0 : pa, pb < 0 ? -1 : pb, r);
         if (q < 0 || q >= (int64_t)p.part_n) continue;  // only with a decreasing part_sizes
+        if (small_part(p.ps, q)) continue;  // stored whole by k_filter_parts
         set_bits(p.filter + (uint64_t)q * BF_WORDS, key_at(p.in, p.pairs, r));
       }
     }
@@ -405,9 +457,15 @@ extern "C" int pimdal_filter_kernel(pimdal_ctx_t *ctx, const pimdal_filter_argum
   p.ps = a->part_sizes;
   p.part_n = a->part_n;
   p.pairs = a->layout == PIMDAL_LAYOUT_PAIRS;
+  uint32_t *large = ctx->d_counters + PD_COUNTER_FILTER;
+  PD_CHECK_CUDA(cudaMemsetAsync(large, 0, sizeof(uint32_t), s));
   {
     pd_launch_scope sc(ctx, PIMDAL_KERNEL_FILTER, s);
-    k_filter_build<<<ctx->sm_count * 8, BF_THREADS, 0, s>>>(p);
+    k_filter_parts<<<ctx->sm_count * 8, BF_THREADS, 0, s>>>(p, large);
+  }
+  {
+    pd_launch_scope sc(ctx, PIMDAL_KERNEL_FILTER, s);
+    k_filter_build<<<ctx->sm_count * 8, BF_THREADS, 0, s>>>(p, large);
   }
   return pd_launch_status(ctx);
 }

@@ -31,7 +31,8 @@ enum : uint32_t {
 
 // Slots of pimdal_ctx::d_counters (two words each: claim counter, CTAs done).
 enum : uint32_t { PD_COUNTER_SELECT = 0, PD_COUNTER_PARTITION = 2, PD_COUNTER_GROUP = 4,
-                  PD_COUNTER_PROBE = 6, PD_COUNTER_MERGE = 8, PD_COUNTER_MATCH = 10 };
+                  PD_COUNTER_PROBE = 6, PD_COUNTER_MERGE = 8, PD_COUNTER_MATCH = 10,
+                  PD_COUNTER_FILTER = 12 };
 
 // Lookback status word: [epoch:16][flag:2][value:46].
 enum : uint32_t { PD_FLAG_INVALID = 0, PD_FLAG_AGGREGATE = 1, PD_FLAG_INCLUSIVE = 2 };

@@ -107,6 +107,21 @@ def test_bloom_large_partitions_and_rows_outside(ctx):
     check(ctx, bk, bps, pk, pps, ptr=ptr)
 
 
+@pytest.mark.parametrize("pairs", [False, True])
+def test_bloom_partitions_above_and_below_the_shared_memory_size(ctx, pairs):
+    # build partitions of 20000 and 30000 rows (the tile path) between small
+    # ones (stored whole by one CTA each), one empty
+    bsz = np.array([100, 20000, 0, 50, 30000, 7, 16384, 16385, 3000], np.uint64)
+    bps = np.concatenate([[0], np.cumsum(bsz)]).astype(np.uint64)
+    bk = gen.generate_cpu(gen.Spec(L.GEN_UNIFORM, L.U32, seed=44, lo=0, hi=2**32 - 1), int(bps[-1]))
+    psz = np.array([500, 3000, 10, 700, 4000, 0, 2000, 2000, 900], np.uint64)
+    pps = np.concatenate([[0], np.cumsum(psz)]).astype(np.uint64)
+    n = int(pps[-1])
+    pk = gen.generate_cpu(gen.Spec(L.GEN_UNIFORM, L.U32, seed=45, lo=0, hi=2**32 - 1), n)
+    pk[::4] = bk[np.arange(0, n, 4) % bk.size]
+    check(ctx, bk, bps, pk, pps, pairs=pairs)
+
+
 def test_bloom_every_build_key_passes(ctx):
     # partition both sides with part_kernel (hash0 bits), then the filter of a
     # build partition must keep every probe row whose key it holds
