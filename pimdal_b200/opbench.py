@@ -8,6 +8,10 @@
     python -m pimdal_b200.opbench bloom     --rows 268435456 --parts 16384 --match-permille 50
                                              (build = rows / 8; both sides partitioned first,
                                               untimed; times filter + match)
+    python -m pimdal_b200.opbench served    [--orders 15000000]      (one fused request of the
+                                             served form over the whole lineitem table: dates
+                                             in a quarter of the range, joined to the part
+                                             attribute, revenue summed per attribute)
     python -m pimdal_b200.opbench tpch      --query q6|q1|q4|q3|q5 [--orders 15000000]
                                              (q6, q1: the fused pass over the lineitem-shaped
                                               table of the served form, about 4 rows per order;
@@ -73,6 +77,9 @@ def _inputs(ctx: ops.Context, a) -> tuple:
         from . import serve, tpch
         li = tpch.Lineitem(ctx, serve.Tables(ctx, orders=a.orders))
         return (li, tpch.Schema(ctx, li) if a.query in ("q3", "q4", "q5") else None)
+    if a.op == "served":
+        from . import serve
+        return (serve.Tables(ctx, orders=a.orders),)
     if a.op == "group":
         keys = g(gen.Spec(L.GEN_PERM_UNIFORM, L.I32, seed=a.seed, stream_id=10, lo=0,
                           hi=a.card - 1, perm_domain=0), n)
@@ -117,6 +124,16 @@ def _runner(ctx: ops.Context, a, inp):
             ops.match_kernel(ctx, filt, opk, pps, oprow, out=ok, out_row=orow, result=res)
         bloom.result = res
         return bloom
+    if a.op == "served":
+        from . import serve
+        t = inp[0]
+        a.rows = t.l_date.numel()
+        col, table, tsize, _, _ = t.dim(0)
+        res = torch.empty(1, dtype=torch.int64, device=dev)
+        d0 = serve.DAYS // 8
+        return lambda: ops.select_join_aggregate(ctx, t.l_date, d0, d0 + serve.DAYS // 4, col, table,
+                                                 tsize, t.l_price, t.l_discount,
+                                                 key_space=t.n_attr(0), result=res)
     if a.op == "tpch":
         from . import tpch
         li, schema = inp
@@ -144,7 +161,8 @@ def _runner(ctx: ops.Context, a, inp):
 
 def main(argv=None) -> None:
     p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    p.add_argument("op", choices=["select", "sort", "smj", "hash_join", "group", "bloom", "tpch"])
+    p.add_argument("op", choices=["select", "sort", "smj", "hash_join", "group", "bloom", "tpch",
+                                  "served"])
     p.add_argument("--rows", type=int, default=1 << 24)
     p.add_argument("--iters", type=int, default=10)
     p.add_argument("--warmup", type=int, default=2)
@@ -159,7 +177,7 @@ def main(argv=None) -> None:
     p.add_argument("--match-permille", type=int, default=50, help="bloom: probe match rate")
     p.add_argument("--query", default="q6", choices=["q6", "q1", "q4", "q3", "q5"],
                    help="tpch: the query")
-    p.add_argument("--orders", type=int, default=15_000_000, help="tpch: orders of the table")
+    p.add_argument("--orders", type=int, default=15_000_000, help="tpch, served: orders of the table")
     p.add_argument("--device", type=int, default=0)
     p.add_argument("--kernels", action="store_true",
                    help="also print the mean time of each library kernel class")
