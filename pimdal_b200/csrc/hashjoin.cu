@@ -40,7 +40,10 @@ namespace {
 
 constexpr uint64_t HJ_EMPTY = ~0ull;
 constexpr int HJ_THREADS = 256;
-constexpr int HJ_ITEMS = 16;
+#ifndef PD_HJ_ITEMS
+#define PD_HJ_ITEMS 16  // probe rows per thread of a tile (at most 16: 4 count bits each in 64)
+#endif
+constexpr int HJ_ITEMS = PD_HJ_ITEMS;
 constexpr int HJ_TILE = HJ_THREADS * HJ_ITEMS;  // 4096 probe rows per tile
 #ifndef PD_HJ_BATCH
 #define PD_HJ_BATCH 2  // probe rows of a thread whose bucket loads are in flight together
@@ -52,6 +55,7 @@ constexpr int HJ_TILE = HJ_THREADS * HJ_ITEMS;  // 4096 probe rows per tile
 #define PD_HJ_MIN_CTAS 3  // probe CTAs per SM (register budget)
 #endif
 constexpr int HJ_BATCH = PD_HJ_BATCH;
+static_assert(HJ_ITEMS <= 16 && HJ_ITEMS % HJ_BATCH == 0, "probe tile shape");
 constexpr uint32_t HJ_MIN_BITS = 10;
 
 }  // namespace
