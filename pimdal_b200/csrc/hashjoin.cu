@@ -538,7 +538,7 @@ __global__ void __launch_bounds__(256) k_hjb_build(pd_hj_batch b) {
   }
 }
 
-__global__ void __launch_bounds__(HJ_THREADS, 3) k_hjb_probe(pd_hj_batch b) {
+__global__ void __launch_bounds__(HJ_THREADS, PD_HJ_MIN_CTAS) k_hjb_probe(pd_hj_batch b) {
   __shared__ uint64_t s_tile;
   const int tid = threadIdx.x;
   const uint32_t epoch = *b.epoch;
